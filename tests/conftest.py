@@ -1,0 +1,9 @@
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+
+def pytest_configure(config):
+  config.addinivalue_line(
+      'markers', 'gpu: needs a CUDA device (sm_100a) and the built libdino_b200.so')
