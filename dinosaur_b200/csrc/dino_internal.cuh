@@ -1,0 +1,148 @@
+// Internal declarations shared by the dino_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/dino_b200.h"
+
+namespace dino {
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+
+void set_error(const std::string& msg);
+
+struct Status {
+  int code = DINO_OK;
+};
+
+#define DINO_CHECK_CUDA(expr)                                             \
+  do {                                                                    \
+    cudaError_t err_ = (expr);                                            \
+    if (err_ != cudaSuccess) {                                            \
+      ::dino::set_error(std::string(#expr) + ": " +                       \
+                        cudaGetErrorString(err_));                        \
+      return DINO_ERR_CUDA;                                               \
+    }                                                                     \
+  } while (0)
+
+#define DINO_REQUIRE(cond, code, msg)        \
+  do {                                       \
+    if (!(cond)) {                           \
+      ::dino::set_error(msg);                \
+      return (code);                         \
+    }                                        \
+  } while (0)
+
+#define DINO_TRY(expr)          \
+  do {                          \
+    int rc_ = (expr);           \
+    if (rc_ != DINO_OK) return rc_; \
+  } while (0)
+
+// Checks the launch status of the last kernel (does not synchronize).
+int check_launch(const char* what);
+
+// ---------------------------------------------------------------------------
+// Field segments: a batch of fields gathered from up to kMaxSegs contiguous
+// runs of [M][L] (or [I][J]) planes.
+// ---------------------------------------------------------------------------
+
+constexpr int kMaxSegs = 4;
+
+struct Segs {
+  const float* ptr[kMaxSegs];
+  int start[kMaxSegs + 1];
+  int n;
+};
+
+inline Segs one_seg(const float* p, int count) {
+  Segs s{};
+  s.ptr[0] = p;
+  s.start[0] = 0;
+  s.start[1] = count;
+  s.n = 1;
+  return s;
+}
+
+__device__ __forceinline__ const float* seg_field(const Segs& s, int b,
+                                                  size_t stride) {
+  int i = 0;
+  while (i + 1 < s.n && b >= s.start[i + 1]) ++i;
+  return s.ptr[i] + (size_t)(b - s.start[i]) * stride;
+}
+
+Segs seg_offset(const Segs& s, int first, int count, size_t stride);
+
+// ---------------------------------------------------------------------------
+// Transform plan
+// ---------------------------------------------------------------------------
+
+struct TcTables;  // tensor-core operand tables (legendre_tc.cu)
+
+}  // namespace dino
+
+struct dino_plan {
+  // Shapes.
+  int lw = 0, L = 0, I = 0, J = 0, M = 0, Jh = 0, N = 0;
+  int spacing = 0, precision = 0, max_fields = 0, device = 0;
+  double radius = 1.0;
+  bool fft_pow2 = false;
+  // FP64 nodes and weights (device and host copies).
+  double* d_x64 = nullptr;
+  double* d_w64 = nullptr;
+  std::vector<double> h_x64, h_w64;
+  // FP32 tables.
+  float* d_wq = nullptr;       // J: Gauss weight * 2pi / I
+  float* d_ptab = nullptr;     // folded Legendre table, [m][l-m][Jh]
+  int64_t* d_ptab_off = nullptr;  // lw + 1 offsets into d_ptab
+  std::vector<int64_t> h_ptab_off;
+  float* d_fbasis = nullptr;   // [I][M] real Fourier basis (generic DFT path)
+  float2* d_tw_n = nullptr;    // N twiddles exp(+2 pi i k / N)
+  float2* d_tw_i = nullptr;    // N twiddles exp(+2 pi i k / I)
+  float* d_deriv = nullptr;    // 4 tables [lw][L]: (l+1)a, -l b, (l-1)a, -(l+2)b
+  float* d_lap = nullptr;      // L: -l(l+1)/r^2
+  float* d_invlap = nullptr;   // L: inverse, 0 at l = 0
+  // Workspace: intermediate Fourier coefficients [max_fields][M][J].
+  float* d_work = nullptr;
+  dino::TcTables* tc = nullptr;
+};
+
+namespace dino {
+
+// sht.cu
+int sht_inverse_segs(dino_plan* p, const Segs& in, float* out_nodal, int nfields,
+                     float* work, int work_fields, cudaStream_t st);
+int sht_forward_to(dino_plan* p, const float* nodal, float* out_modal,
+                   int nfields, float* work, int work_fields, cudaStream_t st);
+int legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
+                     int nfields, cudaStream_t st);
+int legendre_forward(dino_plan* p, const float* fourier, float* out_modal,
+                     int nfields, cudaStream_t st);
+int fourier_inverse(dino_plan* p, const float* fourier, float* nodal,
+                    int nfields, bool weighted_adjoint, cudaStream_t st);
+int fourier_forward(dino_plan* p, const float* nodal, float* fourier,
+                    int nfields, bool weighted, cudaStream_t st);
+int modal_op(dino_plan* p, int op, const float* in, float* out, int nfields,
+             int arg, cudaStream_t st);
+// Sets kernel attributes ahead of stream capture.
+int sht_prepare(dino_plan* p);
+
+// legendre_tc.cu
+int tc_tables_build(dino_plan* p);
+void tc_tables_free(dino_plan* p);
+int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
+                        int nfields, cudaStream_t st);
+int tc_legendre_forward(dino_plan* p, const float* fourier, float* out_modal,
+                        int nfields, cudaStream_t st);
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace dino

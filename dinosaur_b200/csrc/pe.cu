@@ -1,0 +1,1441 @@
+// Primitive equations on sigma levels: explicit tendencies, implicit terms,
+// implicit inverse and the imex_rk_sil3 step with a per-l step filter.
+//
+// Follows PrimitiveEquationsSigma (dinosaur/primitive_equations.py:835-1458),
+// compute_diagnostic_state_sigma (:168-225), HeldSuarezForcingSigma
+// (dinosaur/held_suarez.py:47-167), imex_runge_kutta / imex_rk_sil3
+// (dinosaur/time_integration.py:329-405) and the exponential step filter
+// (:427-455).  Data stays in HBM in the packed, kind-major state layout
+// described in include/dino_b200.h; one explicit evaluation is
+//   modal pre-pass -> inverse SHT -> fused nodal column kernel ->
+//   forward SHT -> modal post-pass,
+// and each RK stage is one fused kernel (combine, per-l implicit solve,
+// implicit terms of the solution, final combination and filter).
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dino_internal.cuh"
+
+namespace dino {
+
+constexpr int kMaxTracers = 4;
+
+// ---------------------------------------------------------------------------
+// Object
+// ---------------------------------------------------------------------------
+
+struct InvCacheEntry {
+  double eta;
+  float* d_inv;  // [L][N][NP] padded FP32 inverse matrices
+};
+
+struct FilterCacheEntry {
+  std::vector<double> host;
+  float* d_filter;
+};
+
+struct GraphEntry {
+  float* state = nullptr;
+  double dt = 0;
+  float* filter = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace dino
+
+struct dino_pe {
+  dino_plan* plan = nullptr;
+  int K = 0, mem = 0, nT = 0, hum = -1, vadv = 1, hs = 0, tref_varies = 0;
+  int KM = 0;  // padded level count for the per-l solves
+  int M = 0, L = 0, I = 0, J = 0;
+  size_t ML = 0, IJ = 0;
+  double R = 0, Rv = 0, Cpv = 0, kappa = 0, g = 0, Omega = 0;
+  double hs_p0 = 0, hs_sigma_b = 0, hs_kf = 0, hs_ka = 0, hs_ks = 0,
+         hs_minT = 0, hs_maxT = 0, hs_dTy = 0, hs_dThz = 0;
+  // Host copies (FP64).
+  std::vector<double> dsig, c2c, alpha, tref, sumsig, sigma, G, H;
+  // Device constants.
+  float* d_lev = nullptr;   // per-level constants (see LevOff)
+  float* d_lat = nullptr;   // per-latitude constants: sec2, f, sin2, cos2
+  float* d_mat = nullptr;   // padded G and H (KM x KM each)
+  float* d_orog = nullptr;  // modal orography [M][L]
+  // Field bookkeeping (planes).
+  int n_state = 0, n_inv = 0, n_fwd = 0, n_aux = 0;
+  // Plane bases inside the nodal buffer / forward buffers.
+  int p_u = 0, p_v = 0, p_gqx = 0, p_gqy = 0, p_gx = 0, p_gy = 0,
+      p_laplnps = 0, p_lnps = 0;
+  int o_Au = 0, o_Av = 0, o_KE = 0, o_uT = 0, o_vT = 0, o_Tn = 0, o_tr = 0,
+      o_vh = 0, o_gh = 0, o_dh = 0, o_hsT = 0, o_lnps = 0;
+  // Work buffers.
+  float* d_aux = nullptr;
+  float* d_nodal = nullptr;
+  float* d_fwd_in = nullptr;
+  float* d_fwd_out = nullptr;
+  float* d_work = nullptr;
+  int work_fields = 0;
+  float* d_f[3] = {nullptr, nullptr, nullptr};
+  float* d_g[2] = {nullptr, nullptr};
+  float* d_Y = nullptr;
+  int* d_flag = nullptr;
+  std::vector<dino::InvCacheEntry> inv_cache;
+  std::vector<dino::FilterCacheEntry> filter_cache;
+  dino::GraphEntry graph;
+};
+
+namespace dino {
+
+// Offsets into d_lev (floats); every array has K entries (c2ci has K-1).
+struct LevOff {
+  int dsig, c2ci, alpha, tref, sumsig, sigma, kv, trefdiff;
+  int total;
+};
+
+static LevOff lev_offsets(int K) {
+  LevOff o;
+  o.dsig = 0;
+  o.c2ci = K;
+  o.alpha = 2 * K;
+  o.tref = 3 * K;
+  o.sumsig = 4 * K;
+  o.sigma = 5 * K;
+  o.kv = 6 * K;
+  o.trefdiff = 7 * K;  // (Tref[k+1]-Tref[k]) * c2ci[k]
+  o.total = 8 * K;
+  return o;
+}
+
+// Plane index helpers: kind base p, member mb, level k.
+__device__ __forceinline__ size_t pl(int p, int mb, int K, int k) {
+  return (size_t)p + (size_t)mb * K + k;
+}
+
+// ---------------------------------------------------------------------------
+// Modal pre-pass: u cos, v cos, cos grad ln ps (+ humidity gradient, lap ln ps)
+// (get_cos_lat_vector, spherical_harmonic.py:1164-1178; cos_lat_grad :1104-1111;
+//  primitive_equations.py:168-225, :861-963)
+// ---------------------------------------------------------------------------
+
+struct PrepArgs {
+  const float* state;
+  float* aux;
+  int K, mem, nT, hum;
+  int M, L, lw;
+  int p_div, p_vort, p_lnps, p_hum;  // state planes
+  int a_u, a_v, a_gqx, a_gqy, a_gx, a_gy, a_laplnps;  // aux planes (-1 = unused)
+  const float* deriv;
+  const float* lap;
+  const float* invlap;
+  float inv_radius;
+};
+
+__device__ __forceinline__ float d_dlon_at(const float* x, int row, int l,
+                                           int L) {
+  if (row == 0) return 0.f;
+  int m = (row + 1) >> 1;
+  return (row & 1) ? m * x[(size_t)(row + 1) * L + l]
+                   : -m * x[(size_t)(row - 1) * L + l];
+}
+
+// cos_lat_d_dlat (tab = 0) or sec_lat_d_dlat_cos2 (tab = 2) at (row, l) of a
+// plane x scaled elementwise by s[l] (s = nullptr: no scaling).
+__device__ __forceinline__ float dlat_at(const float* x, const float* s,
+                                         int row, int l, int L, int lw,
+                                         const float* deriv, int tab) {
+  int m = (row + 1) >> 1;
+  const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
+  const float* tb = ta + (size_t)lw * L;
+  const float* xr = x + (size_t)row * L;
+  float v = 0.f;
+  if (l + 1 < L) v += ta[l + 1] * (s ? s[l + 1] * xr[l + 1] : xr[l + 1]);
+  if (l >= 1) v += tb[l - 1] * (s ? s[l - 1] * xr[l - 1] : xr[l - 1]);
+  return v;
+}
+
+__global__ void pe_prep_kernel(PrepArgs a) {
+  const size_t ML = (size_t)a.M * a.L;
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ML) return;
+  const int l = idx % a.L, row = idx / a.L;
+  const int mb = blockIdx.y;
+  for (int k = 0; k < a.K; ++k) {
+    const float* vort = a.state + pl(a.p_vort, mb, a.K, k) * ML;
+    const float* div = a.state + pl(a.p_div, mb, a.K, k) * ML;
+    // psi = lap^-1 vort, chi = lap^-1 div (l = 0 -> 0)
+    float dchi = d_dlon_at(div, row, l, a.L) * a.invlap[l];
+    float dpsi = d_dlon_at(vort, row, l, a.L) * a.invlap[l];
+    float cchi = dlat_at(div, a.invlap, row, l, a.L, a.lw, a.deriv, 0);
+    float cpsi = dlat_at(vort, a.invlap, row, l, a.L, a.lw, a.deriv, 0);
+    a.aux[pl(a.a_u, mb, a.K, k) * ML + idx] = (dchi - cpsi) * a.inv_radius;
+    a.aux[pl(a.a_v, mb, a.K, k) * ML + idx] = (cchi + dpsi) * a.inv_radius;
+    if (a.hum >= 0) {
+      const float* q = a.state + pl(a.p_hum, mb, a.K, k) * ML;
+      a.aux[pl(a.a_gqx, mb, a.K, k) * ML + idx] =
+          d_dlon_at(q, row, l, a.L) * a.inv_radius;
+      a.aux[pl(a.a_gqy, mb, a.K, k) * ML + idx] =
+          dlat_at(q, nullptr, row, l, a.L, a.lw, a.deriv, 0) * a.inv_radius;
+    }
+  }
+  const float* lnps = a.state + ((size_t)a.p_lnps + mb) * ML;
+  a.aux[((size_t)a.a_gx + mb) * ML + idx] = d_dlon_at(lnps, row, l, a.L) * a.inv_radius;
+  a.aux[((size_t)a.a_gy + mb) * ML + idx] =
+      dlat_at(lnps, nullptr, row, l, a.L, a.lw, a.deriv, 0) * a.inv_radius;
+  if (a.hum >= 0)
+    a.aux[((size_t)a.a_laplnps + mb) * ML + idx] = lnps[idx] * a.lap[l];
+}
+
+// ---------------------------------------------------------------------------
+// Fused nodal column kernel (all explicit nodal products of one evaluation)
+// ---------------------------------------------------------------------------
+
+struct NodalArgs {
+  const float* nod;
+  float* fwd;
+  int K, mem, nT, hum, vadv, hs, tref_varies;
+  int I, J;
+  int p_vort, p_div, p_temp, p_tr, p_u, p_v, p_gqx, p_gqy, p_gx, p_gy,
+      p_laplnps, p_lnps;
+  int o_Au, o_Av, o_KE, o_uT, o_vT, o_Tn, o_tr, o_vh, o_gh, o_dh, o_hsT,
+      o_lnps;
+  const float* lev;
+  LevOff lo;
+  const float* lat;  // [4][J]: sec2, coriolis, sin^2, cos^2
+  float R, kappa, Rv_over_R, Cpv_over_Cp, Rv_minus_R;
+  float hs_p0, hs_ka, hs_ks, hs_sigma_b, hs_minT, hs_maxT, hs_dTy, hs_dThz;
+};
+
+__global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
+  const size_t IJ = (size_t)a.I * a.J;
+  size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= IJ) return;
+  const int mb = blockIdx.y;
+  const int K = a.K;
+  const int j = col % a.J;
+  const float sec2 = a.lat[j];
+  const float fcor = a.lat[a.J + j];
+  const float* dsig = a.lev + a.lo.dsig;
+  const float* c2ci = a.lev + a.lo.c2ci;
+  const float* alpha = a.lev + a.lo.alpha;
+  const float* tref = a.lev + a.lo.tref;
+  const float* sumsig = a.lev + a.lo.sumsig;
+  const float* nod = a.nod;
+  float* fwd = a.fwd;
+#define NOD(p, k) nod[pl(p, mb, K, k) * IJ + col]
+#define FWD(p, k) fwd[pl(p, mb, K, k) * IJ + col]
+  const float gx = nod[((size_t)a.p_gx + mb) * IJ + col];
+  const float gy = nod[((size_t)a.p_gy + mb) * IJ + col];
+
+  // Pass 1: column totals of u.grad(ln ps) and of (div + u.grad ln ps), both
+  // weighted by the layer thickness (cumulative_sigma_integral, last level).
+  float Fe = 0.f, Ff = 0.f;
+  for (int k = 0; k < K; ++k) {
+    float u = NOD(a.p_u, k), v = NOD(a.p_v, k), d = NOD(a.p_div, k);
+    float ugl = (u * gx + v * gy) * sec2;
+    Fe += ugl * dsig[k];
+    Ff += (d + ugl) * dsig[k];
+  }
+
+  // Moist: geopotential of the virtual-temperature difference, G @ td with
+  // G[k][h] = R alpha_k (h = k), R (alpha_h + alpha_{h-1}) (h > k): a suffix
+  // sum evaluated bottom-up (get_geopotential_weights_sigma, :306-338).
+  if (a.hum >= 0) {
+    float suffix = 0.f;
+    const int ph = a.p_tr + a.hum * a.mem * K;
+    for (int k = K - 1; k >= 0; --k) {
+      float q = NOD(ph, k), T = NOD(a.p_temp, k);
+      float td = q * (T + tref[k]) * (a.Rv_over_R - 1.f);
+      FWD(a.o_gh, k) = a.R * (alpha[k] * td + suffix);
+      if (k > 0) suffix += (alpha[k] + alpha[k - 1]) * td;
+    }
+  }
+
+  // Pass 2: everything else, streaming over levels top-down with a window
+  // of (k-1, k, k+1) for the vertically advected fields.
+  float u_p = 0.f, v_p = 0.f, T_p = 0.f;
+  float u_c = NOD(a.p_u, 0), v_c = NOD(a.p_v, 0), T_c = NOD(a.p_temp, 0);
+  float q_p[kMaxTracers], q_c[kMaxTracers], q_n[kMaxTracers];
+#pragma unroll
+  for (int t = 0; t < kMaxTracers; ++t) {
+    q_p[t] = 0.f;
+    q_c[t] = (t < a.nT) ? NOD(a.p_tr + t * a.mem * K, 0) : 0.f;
+    q_n[t] = 0.f;
+  }
+  float fe = 0.f, ff = 0.f, fe_prev = 0.f, ff_prev = 0.f;
+  float sd_up_f = 0.f, sd_up_e = 0.f;  // sigma-dot at k - 1/2
+  float hs_ps = 0.f, sin2 = 0.f, cos2 = 0.f, lnps_n = 0.f;
+  if (a.hs) {
+    lnps_n = nod[((size_t)a.p_lnps + mb) * IJ + col];
+    hs_ps = expf(lnps_n);
+    sin2 = a.lat[2 * a.J + j];
+    cos2 = a.lat[3 * a.J + j];
+  }
+  float gqx = 0.f, gqy = 0.f, laplnps = 0.f;
+  if (a.hum >= 0) laplnps = nod[((size_t)a.p_laplnps + mb) * IJ + col];
+
+  for (int k = 0; k < K; ++k) {
+    const bool has_next = k + 1 < K;
+    float u_n = 0.f, v_n = 0.f, T_n = 0.f;
+    if (has_next) {
+      u_n = NOD(a.p_u, k + 1);
+      v_n = NOD(a.p_v, k + 1);
+      T_n = NOD(a.p_temp, k + 1);
+    }
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t)
+      if (t < a.nT) q_n[t] = has_next ? NOD(a.p_tr + t * a.mem * K, k + 1) : 0.f;
+    const float zeta = NOD(a.p_vort, k);
+    const float div = NOD(a.p_div, k);
+    const float ugl = (u_c * gx + v_c * gy) * sec2;
+    fe += ugl * dsig[k];
+    ff += (div + ugl) * dsig[k];
+    float sd_dn_f = 0.f, sd_dn_e = 0.f;  // sigma-dot at k + 1/2
+    if (has_next) {
+      sd_dn_f = sumsig[k] * Ff - ff;
+      sd_dn_e = sumsig[k] * Fe - fe;
+    }
+    const float ci_dn = has_next ? c2ci[k] : 0.f;
+    const float ci_up = (k > 0) ? c2ci[k - 1] : 0.f;
+    // centered_vertical_advection(w, x)[k] = -0.5 (w_{k+1/2} dx_{k+1/2} +
+    // w_{k-1/2} dx_{k-1/2}) (sigma_coordinates.py:344-405).
+    auto vadv = [&](float xp, float xc, float xn, float wdn, float wup) {
+      float pd = has_next ? wdn * ((xn - xc) * ci_dn) : 0.f;
+      float pu = (k > 0) ? wup * ((xc - xp) * ci_up) : 0.f;
+      return -0.5f * (pd + pu);
+    };
+    float q_h = 0.f;
+    if (a.hum >= 0) {
+#pragma unroll
+      for (int t = 0; t < kMaxTracers; ++t)
+        if (t == a.hum) q_h = q_c[t];
+    }
+    // curl_and_div_tendencies (:1001-1059)
+    const float adj = (a.hum >= 0) ? 1.f + (a.Rv_over_R - 1.f) * q_h : 1.f;
+    const float rt = a.R * T_c * adj;
+    float sdu = 0.f, sdv = 0.f;
+    if (a.vadv) {
+      sdu = -vadv(u_p, u_c, u_n, sd_dn_f, sd_up_f);
+      sdv = -vadv(v_p, v_c, v_n, sd_dn_f, sd_up_f);
+    }
+    const float tv = zeta + fcor;
+    float Au = -v_c * tv * sec2 + (sdu + rt * gx) * sec2;
+    float Av = u_c * tv * sec2 + (sdv + rt * gy) * sec2;
+    if (a.hs) {
+      // Rayleigh drag folded in: curl/div of -(-kv u / cos^2).
+      const float kv = a.lev[a.lo.kv + k];
+      Au += kv * u_c * sec2;
+      Av += kv * v_c * sec2;
+    }
+    FWD(a.o_Au, k) = Au;
+    FWD(a.o_Av, k) = Av;
+    FWD(a.o_KE, k) = (u_c * u_c + v_c * v_c) * sec2 * 0.5f;
+    FWD(a.o_uT, k) = u_c * T_c * sec2;
+    FWD(a.o_vT, k) = v_c * T_c * sec2;
+    // Temperature: horizontal nodal term, vertical advection, adiabatic.
+    float Tn = T_c * div;
+    if (a.vadv) Tn += vadv(T_p, T_c, T_n, sd_dn_f, sd_up_f);
+    if (a.tref_varies) {
+      const float* trd = a.lev + a.lo.trefdiff;
+      float pd = has_next ? sd_dn_e * trd[k] : 0.f;
+      float pu = (k > 0) ? sd_up_e * trd[k - 1] : 0.f;
+      Tn += -0.5f * (pd + pu);
+    }
+    const float inv_ds = 1.f / dsig[k];
+    const float ge = (alpha[k] * fe + (k > 0 ? alpha[k - 1] * fe_prev : 0.f)) * inv_ds;
+    const float gf = (alpha[k] * ff + (k > 0 ? alpha[k - 1] * ff_prev : 0.f)) * inv_ds;
+    const float mean_part = tref[k] * (ugl - ge);
+    float var_part;
+    if (a.hum < 0) {
+      var_part = T_c * (ugl - gf);
+    } else {
+      const float den = 1.f + (a.Cpv_over_Cp - 1.f) * q_h;
+      const float tv_var = T_c * ((1.f + (a.Rv_over_R - 1.f) * q_h) / den);
+      const float tv_ref = tref[k] * (((a.Rv_over_R - a.Cpv_over_Cp) * q_h) / den);
+      var_part = (tv_var + tv_ref) * (ugl - gf);
+    }
+    Tn += a.kappa * (mean_part + var_part);
+    FWD(a.o_Tn, k) = Tn;
+    // Tracers: u q, v q (times sec^2) and q div + vertical advection.
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t) {
+      if (t >= a.nT) break;
+      const int ob = a.o_tr + 3 * t * a.mem * K;
+      FWD(ob, k) = u_c * q_c[t] * sec2;
+      FWD(ob + a.mem * K, k) = v_c * q_c[t] * sec2;
+      float qn = q_c[t] * div;
+      if (a.vadv) qn += vadv(q_p[t], q_c[t], q_n[t], sd_dn_f, sd_up_f);
+      FWD(ob + 2 * a.mem * K, k) = qn;
+    }
+    if (a.hum >= 0) {
+      gqx = NOD(a.p_gqx, k);
+      gqy = NOD(a.p_gqy, k);
+      const float coef = tref[k] * a.Rv_minus_R;
+      FWD(a.o_vh, k) = coef * sec2 * (gx * gqy - gy * gqx);
+      FWD(a.o_dh, k) = coef * sec2 * (gqx * gx + gqy * gy) +
+                       q_h * laplnps * tref[k] * a.Rv_minus_R;
+    }
+    if (a.hs) {
+      // held_suarez.py:105-120, :138-151
+      const float sig = a.lev[a.lo.sigma + k];
+      const float cutoff = fmaxf(0.f, (sig - a.hs_sigma_b) / (1.f - a.hs_sigma_b));
+      const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (cutoff * cos2 * cos2);
+      const float pp0 = sig * hs_ps / a.hs_p0;
+      float teq = powf(pp0, a.kappa) *
+                  (a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * logf(pp0) * cos2);
+      teq = fmaxf(a.hs_minT, teq);
+      FWD(a.o_hsT, k) = -kt * (tref[k] + T_c - teq);
+    }
+    // Advance the window.
+    fe_prev = fe;
+    ff_prev = ff;
+    sd_up_f = sd_dn_f;
+    sd_up_e = sd_dn_e;
+    u_p = u_c; v_p = v_c; T_p = T_c;
+    u_c = u_n; v_c = v_n; T_c = T_n;
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t) {
+      q_p[t] = q_c[t];
+      q_c[t] = q_n[t];
+    }
+  }
+  fwd[((size_t)a.o_lnps + mb) * IJ + col] = -Fe;
+#undef NOD
+#undef FWD
+}
+
+// ---------------------------------------------------------------------------
+// Modal post-pass: curl/div, Laplacians, horizontal advection divergence,
+// orography, humidity corrections, clip of the top wavenumber.
+// ---------------------------------------------------------------------------
+
+struct PostArgs {
+  const float* fm;  // forward outputs (modal)
+  float* tend;      // packed state layout
+  const float* orog;
+  int K, mem, nT, hum, hs;
+  int M, L, lw;
+  int o_Au, o_Av, o_KE, o_uT, o_vT, o_Tn, o_tr, o_vh, o_gh, o_dh, o_hsT,
+      o_lnps;
+  int p_vort, p_div, p_temp, p_tr, p_lnps;
+  const float* deriv;
+  const float* lap;
+  float inv_radius, gravity;
+};
+
+__global__ void pe_post_kernel(PostArgs a) {
+  const size_t ML = (size_t)a.M * a.L;
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ML) return;
+  const int l = idx % a.L, row = idx / a.L;
+  const int mb = blockIdx.y;
+  const int K = a.K;
+  const bool clip = (l == a.L - 1);
+  const float lam = a.lap[l];
+#define FM(p, k) (a.fm + pl(p, mb, K, k) * ML)
+#define OUT(p, k) a.tend[pl(p, mb, K, k) * ML + idx]
+  for (int k = 0; k < K; ++k) {
+    const float* Au = FM(a.o_Au, k);
+    const float* Av = FM(a.o_Av, k);
+    float vort = -(d_dlon_at(Av, row, l, a.L) -
+                   dlat_at(Au, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
+    float div = -(d_dlon_at(Au, row, l, a.L) +
+                  dlat_at(Av, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
+    div += -lam * FM(a.o_KE, k)[idx] - a.gravity * lam * a.orog[idx];
+    if (a.hum >= 0) {
+      vort += FM(a.o_vh, k)[idx];
+      div += -lam * FM(a.o_gh, k)[idx] - FM(a.o_dh, k)[idx];
+    }
+    const float* uT = FM(a.o_uT, k);
+    const float* vT = FM(a.o_vT, k);
+    float temp = FM(a.o_Tn, k)[idx] -
+                 (d_dlon_at(uT, row, l, a.L) +
+                  dlat_at(vT, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
+    if (clip) {
+      vort = 0.f;
+      div = 0.f;
+      temp = 0.f;
+    }
+    if (a.hs) temp += FM(a.o_hsT, k)[idx];
+    OUT(a.p_vort, k) = vort;
+    OUT(a.p_div, k) = div;
+    OUT(a.p_temp, k) = temp;
+    for (int t = 0; t < a.nT; ++t) {
+      const int ob = a.o_tr + 3 * t * a.mem * K;
+      const float* uq = FM(ob, k);
+      const float* vq = FM(ob + a.mem * K, k);
+      float q = FM(ob + 2 * a.mem * K, k)[idx] -
+                (d_dlon_at(uq, row, l, a.L) +
+                 dlat_at(vq, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
+      OUT(a.p_tr + t * a.mem * K, k) = clip ? 0.f : q;
+    }
+  }
+  float lnps = a.fm[((size_t)a.o_lnps + mb) * ML + idx];
+  a.tend[((size_t)a.p_lnps + mb) * ML + idx] = clip ? 0.f : lnps;
+#undef FM
+#undef OUT
+}
+
+// ---------------------------------------------------------------------------
+// Per-l implicit matrices (FP64 on the GPU): build (I - eta L_l) as in
+// _get_implicit_term_matrix_sigma (:544-598) and invert with Gauss-Jordan
+// elimination with partial pivoting; store FP32 in the padded layout.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int pad_index(int i, int K, int KM) {
+  return i < K ? i : (i < 2 * K ? KM + (i - K) : 2 * KM);
+}
+
+__global__ void implicit_inverse_build_kernel(
+    int K, int KM, int L, double eta, double R, const double* __restrict__ G,
+    const double* __restrict__ H, const double* __restrict__ tref,
+    const double* __restrict__ dsig, const double* __restrict__ lam,
+    float* __restrict__ out, int* __restrict__ flag) {
+  extern __shared__ double aug[];  // n x 2n
+  const int l = blockIdx.x;
+  const int n = 2 * K + 1, n2 = 2 * n;
+  const int N = 2 * KM + 1, NP = (N + 3) & ~3;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  __shared__ double factor[2 * 64 + 1];
+  __shared__ int piv;
+  const double lm = lam[l];
+  for (int e = tid; e < n * n2; e += nt) {
+    int r = e / n2, c = e % n2;
+    double v = 0.0;
+    if (c >= n) {
+      v = (c - n == r) ? 1.0 : 0.0;
+    } else if (r < K) {
+      if (c < K) v = (r == c) ? 1.0 : 0.0;
+      else if (c < 2 * K) v = eta * lm * G[r * K + (c - K)];
+      else v = eta * R * lm * tref[r];
+    } else if (r < 2 * K) {
+      if (c < K) v = eta * H[(r - K) * K + c];
+      else if (c < 2 * K) v = (r == c) ? 1.0 : 0.0;
+      else v = 0.0;
+    } else {
+      if (c < K) v = eta * dsig[c];
+      else if (c < 2 * K) v = 0.0;
+      else v = 1.0;
+    }
+    aug[e] = v;
+  }
+  __syncthreads();
+  for (int col = 0; col < n; ++col) {
+    if (tid == 0) {
+      int best = col;
+      double bv = fabs(aug[col * n2 + col]);
+      for (int r = col + 1; r < n; ++r) {
+        double v = fabs(aug[r * n2 + col]);
+        if (v > bv) {
+          bv = v;
+          best = r;
+        }
+      }
+      piv = best;
+      if (!(bv > 0.0)) atomicExch(flag, 1);
+    }
+    __syncthreads();
+    if (piv != col) {
+      for (int c = tid; c < n2; c += nt) {
+        double t = aug[col * n2 + c];
+        aug[col * n2 + c] = aug[piv * n2 + c];
+        aug[piv * n2 + c] = t;
+      }
+    }
+    __syncthreads();
+    const double inv_p = 1.0 / aug[col * n2 + col];
+    __syncthreads();
+    for (int c = tid; c < n2; c += nt) aug[col * n2 + c] *= inv_p;
+    for (int r = tid; r < n; r += nt) factor[r] = aug[r * n2 + col];
+    __syncthreads();
+    for (int e = tid; e < n * n2; e += nt) {
+      int r = e / n2, c = e % n2;
+      if (r != col) aug[e] -= factor[r] * aug[col * n2 + c];
+    }
+    __syncthreads();
+  }
+  float* o = out + (size_t)l * N * NP;
+  for (int e = tid; e < N * NP; e += nt) o[e] = 0.f;
+  __syncthreads();
+  for (int e = tid; e < n * n; e += nt) {
+    int r = e / n, c = e % n;
+    double v = aug[r * n2 + n + c];
+    if (!isfinite(v)) atomicExch(flag, 2);
+    o[pad_index(r, K, KM) * NP + pad_index(c, K, KM)] = (float)v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// IMEX stage kernel
+// ---------------------------------------------------------------------------
+
+struct StageArgs {
+  const float* y0;
+  const float* f[3];
+  float fc[3];
+  int nf;
+  const float* g[2];
+  float gc[2];
+  int ng;
+  float* g0_out;    // if set: G(y0) is written here and added with g0c
+  float g0c;
+  const float* inv; // [L][N][NP] or null (no solve)
+  float* g_out;     // if set: G(Y) written here
+  float final_c;    // if use_final: out = Y* + final_c G(Y)
+  int use_final;
+  int mode;         // 0: stage, 1: implicit terms of y0
+  const float* filter;  // per-l scaling or null
+  float* out;
+  int K, mem, nT, M, L;
+  int p_vort, p_div, p_temp, p_tr, p_lnps;
+  const float* mat;  // padded G then H (KM x KM each)
+  const float* lev;  // level constants (tref at lo_tref, dsig at 0)
+  int lo_tref;
+  const float* lap;
+  float R;
+  int LT;            // l values per CTA
+};
+
+template <int KM>
+__device__ __forceinline__ void apply_implicit(const float* Gs, const float* Hs,
+                                               const float* trs,
+                                               const float* dss, float lam,
+                                               float R, const float* v,
+                                               float* o) {
+  constexpr int N = 2 * KM + 1;
+  (void)N;
+#pragma unroll
+  for (int k = 0; k < KM; ++k) {
+    float s = R * trs[k] * v[2 * KM];
+    float h = 0.f;
+#pragma unroll
+    for (int c = 0; c < KM; ++c) {
+      s = fmaf(Gs[k * KM + c], v[KM + c], s);
+      h = fmaf(Hs[k * KM + c], v[c], h);
+    }
+    o[k] = -lam * s;
+    o[KM + k] = -h;
+  }
+  float p = 0.f;
+#pragma unroll
+  for (int c = 0; c < KM; ++c) p = fmaf(dss[c], v[c], p);
+  o[2 * KM] = -p;
+}
+
+template <int KM>
+__global__ void __launch_bounds__(256) pe_stage_kernel(StageArgs a) {
+  constexpr int N = 2 * KM + 1;
+  constexpr int NP = (N + 3) & ~3;
+  extern __shared__ __align__(16) float smem[];
+  float* Ms = smem;                               // LT * N * NP
+  float* Gs = Ms + (size_t)a.LT * N * NP;         // KM*KM
+  float* Hs = Gs + KM * KM;                       // KM*KM
+  float* trs = Hs + KM * KM;                      // KM
+  float* dss = trs + KM;                          // KM
+  const int tid = threadIdx.x;
+  const int l0 = blockIdx.x * a.LT;
+  const int rows_per = blockDim.x / a.LT;
+  const int K = a.K;
+  // Stage constants in shared memory.
+  if (a.inv) {
+    for (int lo = 0; lo < a.LT; ++lo) {
+      int l = l0 + lo;
+      if (l >= a.L) break;
+      const float4* src = reinterpret_cast<const float4*>(a.inv + (size_t)l * N * NP);
+      float4* dst = reinterpret_cast<float4*>(Ms + (size_t)lo * N * NP);
+      for (int e = tid; e < N * NP / 4; e += blockDim.x) dst[e] = src[e];
+    }
+  }
+  for (int e = tid; e < 2 * KM * KM; e += blockDim.x) Gs[e] = a.mat[e];
+  for (int e = tid; e < KM; e += blockDim.x) {
+    trs[e] = e < K ? a.lev[a.lo_tref + e] : 0.f;
+    dss[e] = e < K ? a.lev[e] : 0.f;
+  }
+  __syncthreads();
+  const int lo = tid % a.LT;
+  const int l = l0 + lo;
+  const int row = blockIdx.y * rows_per + tid / a.LT;
+  const int mb = blockIdx.z;
+  if (l >= a.L || row >= a.M) return;
+  const size_t ML = (size_t)a.M * a.L;
+  const size_t off = (size_t)row * a.L + l;
+  const float lam = a.lap[l];
+  const float filt = a.filter ? a.filter[l] : 1.f;
+
+  // Gather the (div, temp, ln ps) column and form Y*.
+  float ys[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) ys[i] = 0.f;
+  auto plane_of = [&](int i) -> size_t {
+    // padded index -> packed plane
+    if (i < KM) return pl(a.p_div, mb, K, i);
+    if (i < 2 * KM) return pl(a.p_temp, mb, K, i - KM);
+    return (size_t)a.p_lnps + mb;
+  };
+  auto valid = [&](int i) { return (i < KM) ? i < K : (i < 2 * KM ? i - KM < K : true); };
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    if (!valid(i)) continue;
+    size_t p = plane_of(i) * ML + off;
+    float v = a.y0[p];
+    if (a.mode == 0) {
+      for (int t = 0; t < a.nf; ++t) v = fmaf(a.fc[t], a.f[t][p], v);
+      for (int t = 0; t < a.ng; ++t) v = fmaf(a.gc[t], a.g[t][p], v);
+    }
+    ys[i] = v;
+  }
+  if (a.mode == 1) {
+    float gv[N];
+    apply_implicit<KM>(Gs, Hs, trs, dss, lam, a.R, ys, gv);
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      if (valid(i)) a.out[plane_of(i) * ML + off] = gv[i];
+  } else {
+    if (a.g0_out) {
+      // G(y0) needs the bare y0 column.
+      float y0v[N], gv[N];
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        y0v[i] = valid(i) ? a.y0[plane_of(i) * ML + off] : 0.f;
+      apply_implicit<KM>(Gs, Hs, trs, dss, lam, a.R, y0v, gv);
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        if (!valid(i)) continue;
+        a.g0_out[plane_of(i) * ML + off] = gv[i];
+        ys[i] = fmaf(a.g0c, gv[i], ys[i]);
+      }
+    }
+    float y[N];
+    if (a.inv) {
+      const float* Mt = Ms + (size_t)lo * N * NP;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        float acc = 0.f;
+        const float4* mrow = reinterpret_cast<const float4*>(Mt + i * NP);
+#pragma unroll
+        for (int c4 = 0; c4 < NP / 4; ++c4) {
+          float4 mv = mrow[c4];
+          if (4 * c4 + 0 < N) acc = fmaf(mv.x, ys[4 * c4 + 0], acc);
+          if (4 * c4 + 1 < N) acc = fmaf(mv.y, ys[4 * c4 + 1], acc);
+          if (4 * c4 + 2 < N) acc = fmaf(mv.z, ys[4 * c4 + 2], acc);
+          if (4 * c4 + 3 < N) acc = fmaf(mv.w, ys[4 * c4 + 3], acc);
+        }
+        y[i] = acc;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < N; ++i) y[i] = ys[i];
+    }
+    if (a.g_out || a.use_final) {
+      float gy[N];
+      apply_implicit<KM>(Gs, Hs, trs, dss, lam, a.R, y, gy);
+      if (a.g_out) {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+          if (valid(i)) a.g_out[plane_of(i) * ML + off] = gy[i];
+      }
+      if (a.use_final) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) y[i] = fmaf(a.final_c, gy[i], ys[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      if (valid(i)) a.out[plane_of(i) * ML + off] = y[i] * filt;
+  }
+  // Vorticity and tracers: no implicit part.
+  const int nkind = 1 + a.nT;
+  for (int kd = 0; kd < nkind; ++kd) {
+    const int pb = (kd == 0) ? a.p_vort : a.p_tr + (kd - 1) * a.mem * K;
+    for (int k = 0; k < K; ++k) {
+      size_t p = pl(pb, mb, K, k) * ML + off;
+      float v;
+      if (a.mode == 1) {
+        v = 0.f;
+      } else {
+        v = a.y0[p];
+        for (int t = 0; t < a.nf; ++t) v = fmaf(a.fc[t], a.f[t][p], v);
+        v *= filt;
+      }
+      a.out[p] = v;
+    }
+  }
+}
+
+template <int KM>
+static int launch_stage_km(dino_pe* pe, StageArgs a, cudaStream_t st) {
+  constexpr int N = 2 * KM + 1;
+  constexpr int NP = (N + 3) & ~3;
+  const size_t per_l = sizeof(float) * N * NP;
+  int LT = (int)((64 * 1024) / per_l);
+  if (LT < 1) LT = 1;
+  if (LT > 16) LT = 16;
+  int p2 = 1;
+  while (p2 * 2 <= LT) p2 *= 2;
+  LT = p2;
+  a.LT = LT;
+  const int threads = 256;
+  // The matrix area is reserved even when no solve runs: the kernel places
+  // G, H and the level constants after it unconditionally.
+  const size_t smem = per_l * LT + sizeof(float) * (2 * KM * KM + 2 * KM);
+  static bool configured = false;
+  if (!configured) {
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_stage_kernel<KM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024));
+    configured = true;
+  }
+  if (!pe) return DINO_OK;  // attribute set-up only
+  dim3 grid(ceil_div(pe->L, LT), ceil_div(pe->M, threads / LT), pe->mem);
+  pe_stage_kernel<KM><<<grid, threads, smem, st>>>(a);
+  return check_launch("pe_stage");
+}
+
+static int launch_stage_n(int km, dino_pe* pe, StageArgs a, cudaStream_t st) {
+  switch (km) {
+    case 8: return launch_stage_km<8>(pe, a, st);
+    case 16: return launch_stage_km<16>(pe, a, st);
+    case 24: return launch_stage_km<24>(pe, a, st);
+    case 32: return launch_stage_km<32>(pe, a, st);
+    case 48: return launch_stage_km<48>(pe, a, st);
+  }
+  set_error("internal: unsupported padded level count");
+  return DINO_ERR_UNSUPPORTED;
+}
+
+static int launch_stage(dino_pe* pe, StageArgs a, cudaStream_t st) {
+  return launch_stage_n(pe->KM, pe, a, st);
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration
+// ---------------------------------------------------------------------------
+
+static StageArgs base_stage(dino_pe* pe) {
+  StageArgs a{};
+  a.K = pe->K;
+  a.mem = pe->mem;
+  a.nT = pe->nT;
+  a.M = pe->M;
+  a.L = pe->L;
+  a.p_vort = 0;
+  a.p_div = pe->mem * pe->K;
+  a.p_temp = 2 * pe->mem * pe->K;
+  a.p_tr = 3 * pe->mem * pe->K;
+  a.p_lnps = (3 + pe->nT) * pe->mem * pe->K;
+  a.mat = pe->d_mat;
+  a.lev = pe->d_lev;
+  a.lo_tref = lev_offsets(pe->K).tref;
+  a.lap = pe->plan->d_lap;
+  a.R = (float)pe->R;
+  return a;
+}
+
+static int get_inverse(dino_pe* pe, double eta, const float** out) {
+  for (auto& e : pe->inv_cache) {
+    if (e.eta == eta) {
+      *out = e.d_inv;
+      return DINO_OK;
+    }
+  }
+  const int K = pe->K, KM = pe->KM, L = pe->L;
+  const int N = 2 * KM + 1, NP = (N + 3) & ~3;
+  const int n = 2 * K + 1;
+  DINO_REQUIRE(K <= 64, DINO_ERR_UNSUPPORTED, "implicit inverse supports up to 64 levels");
+  double *dG, *dH, *dT, *dS, *dL;
+  std::vector<double> lam(L);
+  for (int l = 0; l < L; ++l)
+    lam[l] = -(double)l * (l + 1) / (pe->plan->radius * pe->plan->radius);
+  DINO_CHECK_CUDA(cudaMalloc(&dG, sizeof(double) * K * K));
+  DINO_CHECK_CUDA(cudaMalloc(&dH, sizeof(double) * K * K));
+  DINO_CHECK_CUDA(cudaMalloc(&dT, sizeof(double) * K));
+  DINO_CHECK_CUDA(cudaMalloc(&dS, sizeof(double) * K));
+  DINO_CHECK_CUDA(cudaMalloc(&dL, sizeof(double) * L));
+  DINO_CHECK_CUDA(cudaMemcpy(dG, pe->G.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
+  DINO_CHECK_CUDA(cudaMemcpy(dH, pe->H.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
+  DINO_CHECK_CUDA(cudaMemcpy(dT, pe->tref.data(), sizeof(double) * K, cudaMemcpyHostToDevice));
+  DINO_CHECK_CUDA(cudaMemcpy(dS, pe->dsig.data(), sizeof(double) * K, cudaMemcpyHostToDevice));
+  DINO_CHECK_CUDA(cudaMemcpy(dL, lam.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
+  float* d_inv;
+  DINO_CHECK_CUDA(cudaMalloc(&d_inv, sizeof(float) * (size_t)L * N * NP));
+  DINO_CHECK_CUDA(cudaMemset(pe->d_flag, 0, sizeof(int)));
+  size_t smem = sizeof(double) * n * 2 * n;
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(implicit_inverse_build_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+  implicit_inverse_build_kernel<<<L, 256, smem>>>(K, KM, L, eta, pe->R, dG, dH, dT,
+                                                  dS, dL, d_inv, pe->d_flag);
+  DINO_TRY(check_launch("implicit_inverse_build"));
+  int flag = 0;
+  DINO_CHECK_CUDA(cudaMemcpy(&flag, pe->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(dG);
+  cudaFree(dH);
+  cudaFree(dT);
+  cudaFree(dS);
+  cudaFree(dL);
+  if (flag) {
+    cudaFree(d_inv);
+    set_error("implicit matrix is singular or its inverse is not finite");
+    return DINO_ERR_NAN;
+  }
+  pe->inv_cache.push_back({eta, d_inv});
+  *out = d_inv;
+  return DINO_OK;
+}
+
+static int get_filter(dino_pe* pe, const double* host, float** out) {
+  *out = nullptr;
+  if (!host) return DINO_OK;
+  for (auto& e : pe->filter_cache) {
+    if (std::memcmp(e.host.data(), host, sizeof(double) * pe->L) == 0) {
+      *out = e.d_filter;
+      return DINO_OK;
+    }
+  }
+  std::vector<float> f(pe->L);
+  for (int l = 0; l < pe->L; ++l) f[l] = (float)host[l];
+  float* d;
+  DINO_CHECK_CUDA(cudaMalloc(&d, sizeof(float) * pe->L));
+  DINO_CHECK_CUDA(cudaMemcpy(d, f.data(), sizeof(float) * pe->L, cudaMemcpyHostToDevice));
+  pe->filter_cache.push_back({std::vector<double>(host, host + pe->L), d});
+  *out = d;
+  return DINO_OK;
+}
+
+static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
+                            cudaStream_t st) {
+  dino_plan* p = pe->plan;
+  const int K = pe->K, mem = pe->mem;
+  const int mK = mem * K;
+  // 1. modal pre-pass
+  {
+    PrepArgs a{};
+    a.state = state;
+    a.aux = pe->d_aux;
+    a.K = K;
+    a.mem = mem;
+    a.nT = pe->nT;
+    a.hum = pe->hum;
+    a.M = pe->M;
+    a.L = pe->L;
+    a.lw = p->lw;
+    a.p_vort = 0;
+    a.p_div = mK;
+    a.p_lnps = (3 + pe->nT) * mK;
+    a.p_hum = pe->hum >= 0 ? (3 + pe->hum) * mK : 0;
+    int q = 0;
+    a.a_u = q; q += mK;
+    a.a_v = q; q += mK;
+    if (pe->hum >= 0) {
+      a.a_gqx = q; q += mK;
+      a.a_gqy = q; q += mK;
+    }
+    a.a_gx = q; q += mem;
+    a.a_gy = q; q += mem;
+    if (pe->hum >= 0) {
+      a.a_laplnps = q; q += mem;
+    }
+    a.deriv = p->d_deriv;
+    a.lap = p->d_lap;
+    a.invlap = p->d_invlap;
+    a.inv_radius = (float)(1.0 / p->radius);
+    dim3 grid(ceil_div((int)pe->ML, 256), mem);
+    pe_prep_kernel<<<grid, 256, 0, st>>>(a);
+    DINO_TRY(check_launch("pe_prep"));
+  }
+  // 2. inverse SHT of [state kinds][aux][ln ps (Held-Suarez)]
+  {
+    Segs s{};
+    s.n = 0;
+    s.start[0] = 0;
+    int acc = 0;
+    s.ptr[s.n] = state;
+    acc += (3 + pe->nT) * mK;
+    s.start[++s.n] = acc;
+    s.ptr[s.n] = pe->d_aux;
+    acc += pe->n_aux;
+    s.start[++s.n] = acc;
+    if (pe->hs) {
+      s.ptr[s.n] = state + (size_t)(3 + pe->nT) * mK * pe->ML;
+      acc += mem;
+      s.start[++s.n] = acc;
+    }
+    DINO_TRY(sht_inverse_segs(p, s, pe->d_nodal, pe->n_inv, pe->d_work,
+                              pe->work_fields, st));
+  }
+  // 3. fused nodal column kernel
+  {
+    NodalArgs a{};
+    a.nod = pe->d_nodal;
+    a.fwd = pe->d_fwd_in;
+    a.K = K;
+    a.mem = mem;
+    a.nT = pe->nT;
+    a.hum = pe->hum;
+    a.vadv = pe->vadv;
+    a.hs = pe->hs;
+    a.tref_varies = pe->tref_varies;
+    a.I = pe->I;
+    a.J = pe->J;
+    a.p_vort = 0;
+    a.p_div = mK;
+    a.p_temp = 2 * mK;
+    a.p_tr = 3 * mK;
+    a.p_u = pe->p_u;
+    a.p_v = pe->p_v;
+    a.p_gqx = pe->p_gqx;
+    a.p_gqy = pe->p_gqy;
+    a.p_gx = pe->p_gx;
+    a.p_gy = pe->p_gy;
+    a.p_laplnps = pe->p_laplnps;
+    a.p_lnps = pe->p_lnps;
+    a.o_Au = pe->o_Au;
+    a.o_Av = pe->o_Av;
+    a.o_KE = pe->o_KE;
+    a.o_uT = pe->o_uT;
+    a.o_vT = pe->o_vT;
+    a.o_Tn = pe->o_Tn;
+    a.o_tr = pe->o_tr;
+    a.o_vh = pe->o_vh;
+    a.o_gh = pe->o_gh;
+    a.o_dh = pe->o_dh;
+    a.o_hsT = pe->o_hsT;
+    a.o_lnps = pe->o_lnps;
+    a.lev = pe->d_lev;
+    a.lo = lev_offsets(K);
+    a.lat = pe->d_lat;
+    a.R = (float)pe->R;
+    a.kappa = (float)pe->kappa;
+    a.Rv_over_R = (float)(pe->Rv / pe->R);
+    a.Cpv_over_Cp = (float)(pe->Cpv / (pe->R / pe->kappa));
+    a.Rv_minus_R = (float)(pe->Rv - pe->R);
+    a.hs_p0 = (float)pe->hs_p0;
+    a.hs_ka = (float)pe->hs_ka;
+    a.hs_ks = (float)pe->hs_ks;
+    a.hs_sigma_b = (float)pe->hs_sigma_b;
+    a.hs_minT = (float)pe->hs_minT;
+    a.hs_maxT = (float)pe->hs_maxT;
+    a.hs_dTy = (float)pe->hs_dTy;
+    a.hs_dThz = (float)pe->hs_dThz;
+    dim3 grid(ceil_div((int)pe->IJ, 128), mem);
+    pe_nodal_kernel<<<grid, 128, 0, st>>>(a);
+    DINO_TRY(check_launch("pe_nodal"));
+  }
+  // 4. forward SHT
+  DINO_TRY(sht_forward_to(p, pe->d_fwd_in, pe->d_fwd_out, pe->n_fwd, pe->d_work,
+                          pe->work_fields, st));
+  // 5. modal post-pass
+  {
+    PostArgs a{};
+    a.fm = pe->d_fwd_out;
+    a.tend = tend;
+    a.orog = pe->d_orog;
+    a.K = K;
+    a.mem = mem;
+    a.nT = pe->nT;
+    a.hum = pe->hum;
+    a.hs = pe->hs;
+    a.M = pe->M;
+    a.L = pe->L;
+    a.lw = p->lw;
+    a.o_Au = pe->o_Au;
+    a.o_Av = pe->o_Av;
+    a.o_KE = pe->o_KE;
+    a.o_uT = pe->o_uT;
+    a.o_vT = pe->o_vT;
+    a.o_Tn = pe->o_Tn;
+    a.o_tr = pe->o_tr;
+    a.o_vh = pe->o_vh;
+    a.o_gh = pe->o_gh;
+    a.o_dh = pe->o_dh;
+    a.o_hsT = pe->o_hsT;
+    a.o_lnps = pe->o_lnps;
+    a.p_vort = 0;
+    a.p_div = mK;
+    a.p_temp = 2 * mK;
+    a.p_tr = 3 * mK;
+    a.p_lnps = (3 + pe->nT) * mK;
+    a.deriv = p->d_deriv;
+    a.lap = p->d_lap;
+    a.inv_radius = (float)(1.0 / p->radius);
+    a.gravity = (float)pe->g;
+    dim3 grid(ceil_div((int)pe->ML, 256), mem);
+    pe_post_kernel<<<grid, 256, 0, st>>>(a);
+    DINO_TRY(check_launch("pe_post"));
+  }
+  return DINO_OK;
+}
+
+// One filtered imex_rk_sil3 step in place (time_integration.py:329-405 with
+// the SIL3 tableau; see the launch sequence in the file header).
+static int pe_step_once(dino_pe* pe, float* y, double dt, const float* filt,
+                        const float* inv1, const float* inv2, const float* inv3,
+                        cudaStream_t st) {
+  const float fdt = (float)dt;
+  DINO_TRY(pe_explicit_impl(pe, y, pe->d_f[0], st));
+  {
+    StageArgs a = base_stage(pe);
+    a.y0 = y;
+    a.f[0] = pe->d_f[0];
+    a.fc[0] = (float)(dt * (1.0 / 3.0));
+    a.nf = 1;
+    a.ng = 0;
+    a.g0_out = pe->d_g[0];
+    a.g0c = (float)(dt * (1.0 / 6.0));
+    a.inv = inv1;
+    a.out = pe->d_Y;
+    DINO_TRY(launch_stage(pe, a, st));
+  }
+  DINO_TRY(pe_explicit_impl(pe, pe->d_Y, pe->d_f[1], st));
+  {
+    StageArgs a = base_stage(pe);
+    a.y0 = y;
+    a.f[0] = pe->d_f[0];
+    a.f[1] = pe->d_f[1];
+    a.fc[0] = (float)(dt * (1.0 / 6.0));
+    a.fc[1] = (float)(dt * 0.5);
+    a.nf = 2;
+    a.g[0] = pe->d_g[0];
+    a.gc[0] = (float)(dt * (1.0 / 3.0));
+    a.ng = 1;
+    a.inv = inv2;
+    a.g_out = pe->d_g[1];
+    a.out = pe->d_Y;
+    DINO_TRY(launch_stage(pe, a, st));
+  }
+  DINO_TRY(pe_explicit_impl(pe, pe->d_Y, pe->d_f[2], st));
+  {
+    StageArgs a = base_stage(pe);
+    a.y0 = y;
+    a.f[0] = pe->d_f[0];
+    a.f[1] = pe->d_f[1];
+    a.f[2] = pe->d_f[2];
+    a.fc[0] = (float)(dt * 0.5);
+    a.fc[1] = (float)(dt * -0.5);
+    a.fc[2] = fdt;
+    a.nf = 3;
+    a.g[0] = pe->d_g[0];
+    a.g[1] = pe->d_g[1];
+    a.gc[0] = (float)(dt * 0.375);
+    a.gc[1] = (float)(dt * 0.375);
+    a.ng = 2;
+    a.inv = inv3;
+    a.use_final = 1;
+    a.final_c = (float)(dt * 0.25);
+    a.filter = filt;
+    a.out = y;
+    DINO_TRY(launch_stage(pe, a, st));
+  }
+  return DINO_OK;
+}
+
+template <typename T>
+static int upload_vec(T** dst, const std::vector<T>& v) {
+  DINO_CHECK_CUDA(cudaMalloc((void**)dst, sizeof(T) * (v.empty() ? 1 : v.size())));
+  if (!v.empty())
+    DINO_CHECK_CUDA(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return DINO_OK;
+}
+
+static void pe_free(dino_pe* pe) {
+  if (!pe) return;
+  if (pe->graph.exec) cudaGraphExecDestroy(pe->graph.exec);
+  if (pe->graph.graph) cudaGraphDestroy(pe->graph.graph);
+  for (auto& e : pe->inv_cache) cudaFree(e.d_inv);
+  for (auto& e : pe->filter_cache) cudaFree(e.d_filter);
+  cudaFree(pe->d_lev);
+  cudaFree(pe->d_lat);
+  cudaFree(pe->d_mat);
+  cudaFree(pe->d_orog);
+  cudaFree(pe->d_aux);
+  cudaFree(pe->d_nodal);
+  cudaFree(pe->d_fwd_in);
+  cudaFree(pe->d_fwd_out);
+  cudaFree(pe->d_work);
+  for (auto* f : pe->d_f) cudaFree(f);
+  for (auto* g : pe->d_g) cudaFree(g);
+  cudaFree(pe->d_Y);
+  cudaFree(pe->d_flag);
+  delete pe;
+}
+
+static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
+  dino_plan* p = pe->plan;
+  const int K = pe->K, mem = pe->mem, nT = pe->nT, J = pe->J;
+  const int mK = mem * K;
+  pe->dsig.assign(d->layer_thickness, d->layer_thickness + K);
+  pe->c2c.assign(d->inv_center_to_center, d->inv_center_to_center + (K > 1 ? K - 1 : 0));
+  pe->alpha.assign(d->sigma_ratios, d->sigma_ratios + K);
+  pe->tref.assign(d->reference_temperature, d->reference_temperature + K);
+  pe->sigma.assign(d->sigma_centers, d->sigma_centers + K);
+  pe->G.assign(d->geopotential_weights, d->geopotential_weights + K * K);
+  pe->H.assign(d->temperature_weights, d->temperature_weights + K * K);
+  pe->sumsig.resize(K);
+  double acc = 0.0;
+  for (int k = 0; k < K; ++k) {
+    acc += pe->dsig[k];
+    pe->sumsig[k] = acc;
+  }
+  pe->tref_varies = 0;
+  for (int k = 1; k < K; ++k)
+    if (pe->tref[k] != pe->tref[0]) pe->tref_varies = 1;
+
+  // Level constants.
+  LevOff lo = lev_offsets(K);
+  std::vector<float> lev(lo.total, 0.f);
+  for (int k = 0; k < K; ++k) {
+    lev[lo.dsig + k] = (float)pe->dsig[k];
+    lev[lo.alpha + k] = (float)pe->alpha[k];
+    lev[lo.tref + k] = (float)pe->tref[k];
+    lev[lo.sumsig + k] = (float)pe->sumsig[k];
+    lev[lo.sigma + k] = (float)pe->sigma[k];
+    double cut = (pe->sigma[k] - pe->hs_sigma_b) / (1.0 - pe->hs_sigma_b);
+    lev[lo.kv + k] = (float)(pe->hs_kf * (cut > 0 ? cut : 0.0));
+    if (k + 1 < K) {
+      // center_to_center arrives already as the reference's 1/x operand.
+      lev[lo.c2ci + k] = (float)pe->c2c[k];
+      lev[lo.trefdiff + k] = (float)((pe->tref[k + 1] - pe->tref[k]) * pe->c2c[k]);
+    }
+  }
+  DINO_TRY(upload_vec(&pe->d_lev, lev));
+  // Latitude constants: sec^2, Coriolis 2 Omega sin, sin^2, cos^2.
+  std::vector<float> lat(4 * J);
+  for (int j = 0; j < J; ++j) {
+    double s = p->h_x64[j];
+    lat[j] = (float)(1.0 / (1.0 - s * s));
+    lat[J + j] = (float)(2.0 * pe->Omega * s);
+    double latr = std::asin(s);
+    lat[2 * J + j] = (float)(std::sin(latr) * std::sin(latr));
+    lat[3 * J + j] = (float)(std::cos(latr) * std::cos(latr));
+  }
+  DINO_TRY(upload_vec(&pe->d_lat, lat));
+  // Padded G and H.
+  std::vector<float> mat(2 * pe->KM * pe->KM, 0.f);
+  for (int r = 0; r < K; ++r)
+    for (int c = 0; c < K; ++c) {
+      mat[r * pe->KM + c] = (float)pe->G[r * K + c];
+      mat[pe->KM * pe->KM + r * pe->KM + c] = (float)pe->H[r * K + c];
+    }
+  DINO_TRY(upload_vec(&pe->d_mat, mat));
+  {
+    std::vector<float> orog(pe->ML, 0.f);
+    if (d->orography_modal) std::memcpy(orog.data(), d->orography_modal, sizeof(float) * pe->ML);
+    DINO_TRY(upload_vec(&pe->d_orog, orog));
+  }
+
+  // Field bookkeeping.
+  const bool moist = pe->hum >= 0;
+  pe->n_state = (3 + nT) * mK + mem;
+  pe->n_aux = 2 * mK + (moist ? 2 * mK : 0) + 2 * mem + (moist ? mem : 0);
+  pe->n_inv = (3 + nT) * mK + pe->n_aux + (pe->hs ? mem : 0);
+  {
+    int q = (3 + nT) * mK;  // nodal planes follow the inverse field order
+    pe->p_u = q; q += mK;
+    pe->p_v = q; q += mK;
+    if (moist) {
+      pe->p_gqx = q; q += mK;
+      pe->p_gqy = q; q += mK;
+    }
+    pe->p_gx = q; q += mem;
+    pe->p_gy = q; q += mem;
+    if (moist) {
+      pe->p_laplnps = q; q += mem;
+    }
+    if (pe->hs) {
+      pe->p_lnps = q; q += mem;
+    }
+  }
+  {
+    int q = 0;
+    pe->o_Au = q; q += mK;
+    pe->o_Av = q; q += mK;
+    pe->o_KE = q; q += mK;
+    pe->o_uT = q; q += mK;
+    pe->o_vT = q; q += mK;
+    pe->o_Tn = q; q += mK;
+    pe->o_tr = q; q += 3 * nT * mK;
+    if (moist) {
+      pe->o_vh = q; q += mK;
+      pe->o_gh = q; q += mK;
+      pe->o_dh = q; q += mK;
+    }
+    if (pe->hs) {
+      pe->o_hsT = q; q += mK;
+    }
+    pe->o_lnps = q; q += mem;
+    pe->n_fwd = q;
+  }
+  const size_t ML = pe->ML, IJ = pe->IJ;
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_aux, sizeof(float) * pe->n_aux * ML));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_nodal, sizeof(float) * pe->n_inv * IJ));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_fwd_in, sizeof(float) * pe->n_fwd * IJ));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_fwd_out, sizeof(float) * pe->n_fwd * ML));
+  pe->work_fields = pe->n_inv > pe->n_fwd ? pe->n_inv : pe->n_fwd;
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_work, sizeof(float) * (size_t)pe->work_fields * p->M * p->J));
+  for (auto*& f : pe->d_f) DINO_CHECK_CUDA(cudaMalloc(&f, sizeof(float) * pe->n_state * ML));
+  for (auto*& g : pe->d_g) DINO_CHECK_CUDA(cudaMalloc(&g, sizeof(float) * pe->n_state * ML));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_Y, sizeof(float) * pe->n_state * ML));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_flag, sizeof(int)));
+  DINO_CHECK_CUDA(cudaDeviceSynchronize());
+  return DINO_OK;
+}
+
+}  // namespace dino
+
+using namespace dino;
+
+extern "C" {
+
+int dino_pe_create(dino_plan* plan, const dino_pe_desc* d, dino_pe** out) {
+  DINO_REQUIRE(plan && d && out, DINO_ERR_ARG, "dino_pe_create: null argument");
+  *out = nullptr;
+  DINO_REQUIRE(d->layers >= 1 && d->layers <= 48, DINO_ERR_UNSUPPORTED,
+               "layers must be in [1, 48]");
+  DINO_REQUIRE(d->members >= 1, DINO_ERR_ARG, "members must be >= 1");
+  DINO_REQUIRE(d->n_tracers >= 0 && d->n_tracers <= kMaxTracers,
+               DINO_ERR_UNSUPPORTED, "at most 4 tracers are supported");
+  DINO_REQUIRE(d->humidity_tracer >= -1 && d->humidity_tracer < d->n_tracers,
+               DINO_ERR_ARG, "humidity_tracer out of range");
+  DINO_REQUIRE(d->layer_thickness && d->inv_center_to_center && d->sigma_ratios &&
+                   d->reference_temperature && d->geopotential_weights &&
+                   d->temperature_weights && d->sigma_centers,
+               DINO_ERR_ARG, "dino_pe_create: missing vertical arrays");
+  DINO_REQUIRE(!(d->held_suarez && d->n_tracers > 0), DINO_ERR_UNSUPPORTED,
+               "Held-Suarez forcing composes with tracer-free states only");
+  dino_pe* pe = new dino_pe();
+  pe->plan = plan;
+  pe->K = d->layers;
+  pe->mem = d->members;
+  pe->nT = d->n_tracers;
+  pe->hum = d->humidity_tracer;
+  pe->vadv = d->include_vertical_advection ? 1 : 0;
+  pe->hs = d->held_suarez ? 1 : 0;
+  pe->KM = pe->K <= 8 ? 8 : pe->K <= 16 ? 16 : pe->K <= 24 ? 24 : pe->K <= 32 ? 32 : 48;
+  pe->M = plan->M;
+  pe->L = plan->L;
+  pe->I = plan->I;
+  pe->J = plan->J;
+  pe->ML = (size_t)pe->M * pe->L;
+  pe->IJ = (size_t)pe->I * pe->J;
+  pe->R = d->R;
+  pe->Rv = d->R_vapor;
+  pe->Cpv = d->Cp_vapor;
+  pe->kappa = d->kappa;
+  pe->g = d->gravity;
+  pe->Omega = d->angular_velocity;
+  pe->hs_p0 = d->hs_p0;
+  pe->hs_sigma_b = d->hs_sigma_b;
+  pe->hs_kf = d->hs_kf;
+  pe->hs_ka = d->hs_ka;
+  pe->hs_ks = d->hs_ks;
+  pe->hs_minT = d->hs_minT;
+  pe->hs_maxT = d->hs_maxT;
+  pe->hs_dTy = d->hs_dTy;
+  pe->hs_dThz = d->hs_dThz;
+  int rc = pe_build(pe, d);
+  if (rc != DINO_OK) {
+    pe_free(pe);
+    return rc;
+  }
+  *out = pe;
+  return DINO_OK;
+}
+
+int dino_pe_destroy(dino_pe* pe) {
+  pe_free(pe);
+  return DINO_OK;
+}
+
+int64_t dino_pe_state_size(const dino_pe* pe) {
+  if (!pe) return -1;
+  return (int64_t)pe->n_state * (int64_t)pe->ML;
+}
+
+int dino_pe_explicit(dino_pe* pe, const float* state, float* tend, void* stream) {
+  DINO_REQUIRE(pe && state && tend, DINO_ERR_ARG, "dino_pe_explicit: null argument");
+  DINO_REQUIRE(state != tend, DINO_ERR_ARG, "dino_pe_explicit: in and out must differ");
+  return pe_explicit_impl(pe, state, tend, (cudaStream_t)stream);
+}
+
+int dino_pe_implicit(dino_pe* pe, const float* state, float* out, void* stream) {
+  DINO_REQUIRE(pe && state && out, DINO_ERR_ARG, "dino_pe_implicit: null argument");
+  DINO_REQUIRE(state != out, DINO_ERR_ARG, "dino_pe_implicit: in and out must differ");
+  StageArgs a = base_stage(pe);
+  a.y0 = state;
+  a.mode = 1;
+  a.out = out;
+  return launch_stage(pe, a, (cudaStream_t)stream);
+}
+
+int dino_pe_implicit_inverse(dino_pe* pe, const float* state, float* out,
+                             double eta, void* stream) {
+  DINO_REQUIRE(pe && state && out, DINO_ERR_ARG, "dino_pe_implicit_inverse: null argument");
+  DINO_REQUIRE(std::isfinite(eta), DINO_ERR_ARG, "step_size must be finite");
+  const float* inv = nullptr;
+  DINO_TRY(get_inverse(pe, eta, &inv));
+  StageArgs a = base_stage(pe);
+  a.y0 = state;
+  a.inv = inv;
+  a.out = out;
+  return launch_stage(pe, a, (cudaStream_t)stream);
+}
+
+int dino_pe_step(dino_pe* pe, float* state, double dt, const double* host_filter,
+                 int32_t n_steps, void* stream) {
+  DINO_REQUIRE(pe && state, DINO_ERR_ARG, "dino_pe_step: null argument");
+  DINO_REQUIRE(n_steps >= 0, DINO_ERR_ARG, "n_steps must be >= 0");
+  const float *i1, *i2, *i3;
+  DINO_TRY(get_inverse(pe, dt / 6.0, &i1));
+  DINO_TRY(get_inverse(pe, dt / 3.0, &i2));
+  DINO_TRY(get_inverse(pe, dt / 4.0, &i3));
+  float* filt = nullptr;
+  DINO_TRY(get_filter(pe, host_filter, &filt));
+  for (int s = 0; s < n_steps; ++s)
+    DINO_TRY(pe_step_once(pe, state, dt, filt, i1, i2, i3, (cudaStream_t)stream));
+  return DINO_OK;
+}
+
+int dino_pe_step_graph(dino_pe* pe, float* state, double dt,
+                       const double* host_filter, int32_t n_steps,
+                       void* stream) {
+  DINO_REQUIRE(pe && state, DINO_ERR_ARG, "dino_pe_step_graph: null argument");
+  DINO_REQUIRE(n_steps >= 0, DINO_ERR_ARG, "n_steps must be >= 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  const float *i1, *i2, *i3;
+  DINO_TRY(get_inverse(pe, dt / 6.0, &i1));
+  DINO_TRY(get_inverse(pe, dt / 3.0, &i2));
+  DINO_TRY(get_inverse(pe, dt / 4.0, &i3));
+  float* filt = nullptr;
+  DINO_TRY(get_filter(pe, host_filter, &filt));
+  GraphEntry& g = pe->graph;
+  if (!(g.exec && g.state == state && g.dt == dt && g.filter == filt)) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = GraphEntry{};
+    DINO_TRY(sht_prepare(pe->plan));
+    DINO_TRY(launch_stage_n(pe->KM, nullptr, StageArgs{}, st));
+    // Capture on a private stream so that the caller's stream (possibly the
+    // legacy default stream) is never put in capture mode.
+    cudaStream_t cap;
+    DINO_CHECK_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    DINO_CHECK_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int rc = pe_step_once(pe, state, dt, filt, i1, i2, i3, cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    if (rc != DINO_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    DINO_CHECK_CUDA(ce);
+    DINO_CHECK_CUDA(cudaGraphInstantiate(&g.exec, graph, 0));
+    g.graph = graph;
+    g.state = state;
+    g.dt = dt;
+    g.filter = filt;
+  }
+  for (int s = 0; s < n_steps; ++s) DINO_CHECK_CUDA(cudaGraphLaunch(g.exec, st));
+  return DINO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,744 @@
+// Spherical-harmonic transform pair on one B200: per-m Legendre contraction
+// over Gaussian latitude (N/S folded, FP32 SIMT form here; tensor-core form in
+// legendre_tc.cu) and a real FFT over longitude in shared memory.
+//
+// Semantics follow RealSphericalHarmonics.inverse_transform / transform
+// (dinosaur/spherical_harmonic.py:262-280):
+//   inverse:  px[b,m,j] = sum_l p[m,j,l] x[b,m,l];  out[b,i,j] = sum_m f[i,m] px[b,m,j]
+//   forward:  fwx[b,m,j] = sum_i f[i,m] w[j] z[b,i,j];  out[b,m,l] = sum_j p[m,j,l] fwx[b,m,j]
+// with f the unit-norm real Fourier basis (fourier.py:24-60) and p the
+// normalised associated Legendre functions duplicated over +-m rows.
+//
+// Folding: Gauss nodes are mirror symmetric and p[m, J-1-j, l] =
+// (-1)^(l-m) p[m, j, l], so each contraction splits into even and odd (l-m)
+// halves over Jh = ceil(J/2) latitudes, halving the arithmetic.
+
+#include <cmath>
+
+#include "dino_internal.cuh"
+
+namespace dino {
+
+// ---------------------------------------------------------------------------
+// Legendre contraction, FP32 SIMT
+// ---------------------------------------------------------------------------
+
+constexpr int kLegTB = 128;  // (field, cos/sin) rows per CTA
+constexpr int kLegTN = 32;   // latitudes (inverse) or l values (forward) per CTA
+constexpr int kLegKC = 16;   // contraction chunk
+constexpr int kLegThreads = 128;
+
+// Row r of the m-slice: m == 0 has one row per field (cos), m > 0 has two.
+__device__ __forceinline__ void row_map(int m, int r, int& b, int& row) {
+  if (m == 0) {
+    b = r;
+    row = 0;
+  } else {
+    b = r >> 1;
+    row = 2 * m - 1 + (r & 1);
+  }
+}
+
+// out_fourier[b][row][j] for all j from modal rows (inverse contraction).
+__global__ void __launch_bounds__(kLegThreads)
+legendre_inverse_simt(Segs in, float* __restrict__ out, int B, int M, int L,
+                      int J, int Jh, const float* __restrict__ ptab,
+                      const int64_t* __restrict__ ptab_off) {
+  const int m = blockIdx.z;
+  const int rows = (m == 0) ? B : 2 * B;
+  const int r0 = blockIdx.y * kLegTB;
+  if (r0 >= rows) return;
+  const int j0 = blockIdx.x * kLegTN;
+  const int Lm = L - m;
+  const float* P = ptab + ptab_off[m];
+
+  __shared__ __align__(16) float Xs[kLegKC][kLegTB + 4];
+  __shared__ __align__(16) float Ps[kLegKC][kLegTN];
+
+  const int tid = threadIdx.x;
+  const int tx = tid & 7;   // 8 groups of 4 latitudes
+  const int ty = tid >> 3;  // 16 groups of 8 rows
+
+  float accE[8][4], accO[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) accE[i][t] = accO[i][t] = 0.f;
+
+  for (int kc = 0; kc < Lm; kc += kLegKC) {
+    // Stage X chunk: rows r0.., l = m + kc + kk (contiguous in global).
+    for (int idx = tid; idx < kLegTB * kLegKC; idx += kLegThreads) {
+      int kk = idx % kLegKC, rl = idx / kLegKC;
+      int r = r0 + rl, k = kc + kk;
+      float v = 0.f;
+      if (r < rows && k < Lm) {
+        int b, row;
+        row_map(m, r, b, row);
+        v = seg_field(in, b, (size_t)M * L)[(size_t)row * L + m + k];
+      }
+      Xs[kk][rl] = v;
+    }
+    for (int idx = tid; idx < kLegKC * kLegTN; idx += kLegThreads) {
+      int jj = idx % kLegTN, kk = idx / kLegTN;
+      int j = j0 + jj, k = kc + kk;
+      Ps[kk][jj] = (j < Jh && k < Lm) ? P[(size_t)k * Jh + j] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kLegKC; kk += 2) {
+      float4 xa = *reinterpret_cast<const float4*>(&Xs[kk][ty * 8]);
+      float4 xb = *reinterpret_cast<const float4*>(&Xs[kk][ty * 8 + 4]);
+      float4 pp = *reinterpret_cast<const float4*>(&Ps[kk][tx * 4]);
+      float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+      float pv[4] = {pp.x, pp.y, pp.z, pp.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) accE[i][t] = fmaf(xv[i], pv[t], accE[i][t]);
+      xa = *reinterpret_cast<const float4*>(&Xs[kk + 1][ty * 8]);
+      xb = *reinterpret_cast<const float4*>(&Xs[kk + 1][ty * 8 + 4]);
+      pp = *reinterpret_cast<const float4*>(&Ps[kk + 1][tx * 4]);
+      float xw[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+      float pw[4] = {pp.x, pp.y, pp.z, pp.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) accO[i][t] = fmaf(xw[i], pw[t], accO[i][t]);
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int r = r0 + ty * 8 + i;
+    if (r >= rows) continue;
+    int b, row;
+    row_map(m, r, b, row);
+    float* o = out + ((size_t)b * M + row) * J;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      int j = j0 + tx * 4 + t;
+      if (j >= Jh) continue;
+      o[j] = accE[i][t] + accO[i][t];
+      int jm = J - 1 - j;
+      if (jm != j) o[jm] = accE[i][t] - accO[i][t];
+    }
+  }
+}
+
+// out_modal[b][row][l] = sum_j p[m,j,l] G[b][row][j] (forward contraction);
+// writes zeros for l < m.
+__global__ void __launch_bounds__(kLegThreads)
+legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
+                      int B, int M, int L, int J, int Jh,
+                      const float* __restrict__ ptab,
+                      const int64_t* __restrict__ ptab_off) {
+  const int m = blockIdx.z;
+  const int rows = (m == 0) ? B : 2 * B;
+  const int r0 = blockIdx.y * kLegTB;
+  if (r0 >= rows) return;
+  const int Lm = L - m;
+  const int k0 = blockIdx.x * kLegTN;  // l - m offset of this tile
+  const int tid = threadIdx.x;
+  const int tx = tid & 7;
+  const int ty = tid >> 3;
+
+  if (blockIdx.x == 0 && m > 0) {
+    // Structural zeros l < m of the rows handled by this CTA.
+    for (int idx = tid; idx < kLegTB * m; idx += kLegThreads) {
+      int rl = idx / m, l = idx % m;
+      int r = r0 + rl;
+      if (r < rows) {
+        int b, row;
+        row_map(m, r, b, row);
+        out[((size_t)b * M + row) * L + l] = 0.f;
+      }
+    }
+  }
+  if (k0 >= Lm) return;
+  const float* P = ptab + ptab_off[m];
+
+  __shared__ __align__(16) float Ss[kLegKC][kLegTB + 4];
+  __shared__ __align__(16) float Ds[kLegKC][kLegTB + 4];
+  __shared__ float Ps[kLegKC][kLegTN + 1];
+
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) acc[i][t] = 0.f;
+
+  for (int jc = 0; jc < Jh; jc += kLegKC) {
+    for (int idx = tid; idx < kLegTB * kLegKC; idx += kLegThreads) {
+      int jj = idx % kLegKC, rl = idx / kLegKC;
+      int r = r0 + rl, j = jc + jj;
+      float s = 0.f, d = 0.f;
+      if (r < rows && j < Jh) {
+        int b, row;
+        row_map(m, r, b, row);
+        const float* g = G + ((size_t)b * M + row) * J;
+        float g1 = g[j];
+        int jm = J - 1 - j;
+        float g2 = (jm != j) ? g[jm] : 0.f;
+        s = g1 + g2;
+        d = g1 - g2;
+      }
+      Ss[jj][rl] = s;
+      Ds[jj][rl] = d;
+    }
+    for (int idx = tid; idx < kLegKC * kLegTN; idx += kLegThreads) {
+      int jj = idx % kLegKC, kk = idx / kLegKC;
+      int j = jc + jj, k = k0 + kk;
+      Ps[jj][kk] = (j < Jh && k < Lm) ? P[(size_t)k * Jh + j] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < kLegKC; ++jj) {
+      float4 sa = *reinterpret_cast<const float4*>(&Ss[jj][ty * 8]);
+      float4 sb = *reinterpret_cast<const float4*>(&Ss[jj][ty * 8 + 4]);
+      float4 da = *reinterpret_cast<const float4*>(&Ds[jj][ty * 8]);
+      float4 db = *reinterpret_cast<const float4*>(&Ds[jj][ty * 8 + 4]);
+      float sv[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
+      float dv[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+      float pv[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) pv[t] = Ps[jj][tx * 4 + t];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        acc[i][0] = fmaf(sv[i], pv[0], acc[i][0]);
+        acc[i][1] = fmaf(dv[i], pv[1], acc[i][1]);
+        acc[i][2] = fmaf(sv[i], pv[2], acc[i][2]);
+        acc[i][3] = fmaf(dv[i], pv[3], acc[i][3]);
+      }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int r = r0 + ty * 8 + i;
+    if (r >= rows) continue;
+    int b, row;
+    row_map(m, r, b, row);
+    float* o = out + ((size_t)b * M + row) * L + m;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      int k = k0 + tx * 4 + t;
+      if (k < Lm) o[k] = acc[i][t];
+    }
+  }
+}
+
+int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
+                     cudaStream_t st) {
+  if (p->precision == DINO_PREC_BF16X3)
+    return tc_legendre_inverse(p, in, out, nf, st);
+  dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
+  legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
+      in, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
+  return check_launch("legendre_inverse_simt");
+}
+
+int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
+                     cudaStream_t st) {
+  if (p->precision == DINO_PREC_BF16X3)
+    return tc_legendre_forward(p, G, out, nf, st);
+  dim3 grid(ceil_div(p->L, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
+  legendre_forward_simt<<<grid, kLegThreads, 0, st>>>(
+      G, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
+  return check_launch("legendre_forward_simt");
+}
+
+// ---------------------------------------------------------------------------
+// Real FFT over longitude (power-of-two I = 2N), shared-memory Stockham
+// radix-4/2 on the half-length complex sequence z[n] = x[2n] + i x[2n+1].
+// ---------------------------------------------------------------------------
+
+constexpr int kFftJS = 16;       // latitudes (columns) per CTA
+constexpr int kFftThreads = 256;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return make_float2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// Multiply by +i (kSign = +1) or -i (kSign = -1).
+template <int kSign>
+__device__ __forceinline__ float2 cmul_i(float2 a) {
+  return kSign > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// Stockham passes over N points for kFftJS columns; data[n * JS + c].
+// kSign = +1: sum_k Z[k] e^{+2 pi i k n / N}; -1: e^{-...}.  Returns the
+// buffer holding the result.
+template <int N, int kSign>
+__device__ float2* stockham(float2* a, float2* b, const float2* twn) {
+  const int tid = threadIdx.x;
+#pragma unroll 1
+  for (int Ns = 1; Ns < N; ) {
+    if (Ns * 4 <= N) {
+      const int quarter = N / 4;
+      const int stride = N / (Ns * 4);
+      for (int item = tid; item < quarter * kFftJS; item += kFftThreads) {
+        int c = item % kFftJS, j = item / kFftJS;
+        int k = j % Ns;
+        float2 v0 = a[(j) * kFftJS + c];
+        float2 v1 = a[(j + quarter) * kFftJS + c];
+        float2 v2 = a[(j + 2 * quarter) * kFftJS + c];
+        float2 v3 = a[(j + 3 * quarter) * kFftJS + c];
+        if (k) {
+          float2 w1 = twn[k * stride], w2 = twn[2 * k * stride],
+                 w3 = twn[3 * k * stride];
+          if (kSign < 0) {
+            w1 = cconj(w1);
+            w2 = cconj(w2);
+            w3 = cconj(w3);
+          }
+          v1 = cmul(v1, w1);
+          v2 = cmul(v2, w2);
+          v3 = cmul(v3, w3);
+        }
+        float2 s02 = cadd(v0, v2), d02 = csub(v0, v2);
+        float2 s13 = cadd(v1, v3), d13 = cmul_i<kSign>(csub(v1, v3));
+        int dst = (j / Ns) * Ns * 4 + k;
+        b[(dst) * kFftJS + c] = cadd(s02, s13);
+        b[(dst + Ns) * kFftJS + c] = cadd(d02, d13);
+        b[(dst + 2 * Ns) * kFftJS + c] = csub(s02, s13);
+        b[(dst + 3 * Ns) * kFftJS + c] = csub(d02, d13);
+      }
+      Ns *= 4;
+    } else {
+      const int half = N / 2;
+      const int stride = N / (Ns * 2);
+      for (int item = tid; item < half * kFftJS; item += kFftThreads) {
+        int c = item % kFftJS, j = item / kFftJS;
+        int k = j % Ns;
+        float2 v0 = a[j * kFftJS + c];
+        float2 v1 = a[(j + half) * kFftJS + c];
+        if (k) {
+          float2 w = twn[k * stride];
+          if (kSign < 0) w = cconj(w);
+          v1 = cmul(v1, w);
+        }
+        int dst = (j / Ns) * Ns * 2 + k;
+        b[dst * kFftJS + c] = cadd(v0, v1);
+        b[(dst + Ns) * kFftJS + c] = csub(v0, v1);
+      }
+      Ns *= 2;
+    }
+    __syncthreads();
+    float2* t = a;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Fourier coefficients F[b][row][j] -> nodal[b][i][j] (optionally scaled by
+// wq[j], which gives the adjoint of the weighted forward transform).
+template <int N>
+__global__ void __launch_bounds__(kFftThreads)
+rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
+                    int M, int lw, int J, const float2* __restrict__ tw_n,
+                    const float2* __restrict__ tw_i,
+                    const float* __restrict__ wq) {
+  extern __shared__ float2 sm[];
+  float2* A = sm;
+  float2* Bf = A + N * kFftJS;
+  float2* twn = Bf + N * kFftJS;
+  float2* twi = twn + N;
+  const int tid = threadIdx.x;
+  const int b = blockIdx.y;
+  const int j0 = blockIdx.x * kFftJS;
+  const int ncol = min(kFftJS, J - j0);
+  for (int t = tid; t < N; t += kFftThreads) {
+    twn[t] = tw_n[t];
+    twi[t] = tw_i[t];
+  }
+  // X[k]: half-weighted positive-frequency spectrum (X[0] full weight).
+  const float* Fb = F + (size_t)b * M * J + j0;
+  const float inv_sqrt_2pi = 0.3989422804014327f;
+  const float half_inv_sqrt_pi = 0.28209479177387814f;
+  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
+    int k = idx / kFftJS, c = idx % kFftJS;
+    float2 v = make_float2(0.f, 0.f);
+    if (c < ncol && k < lw) {
+      if (k == 0) {
+        v.x = Fb[c] * inv_sqrt_2pi;
+      } else {
+        v.x = Fb[(size_t)(2 * k - 1) * J + c] * half_inv_sqrt_pi;
+        v.y = -Fb[(size_t)(2 * k) * J + c] * half_inv_sqrt_pi;
+      }
+    }
+    Bf[idx] = v;
+  }
+  __syncthreads();
+  // Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]), X[N] = 0.
+  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
+    int k = idx / kFftJS, c = idx % kFftJS;
+    float2 xk = Bf[idx];
+    float2 xc = (k == 0) ? make_float2(0.f, 0.f) : cconj(Bf[(N - k) * kFftJS + c]);
+    float2 s = cadd(xk, xc);
+    float2 d = cmul_i<1>(cmul(twi[k], csub(xk, xc)));
+    A[idx] = cadd(s, d);
+  }
+  __syncthreads();
+  float2* z = stockham<N, 1>(A, Bf, twn);
+  float* ob = out + (size_t)b * (2 * N) * J + j0;
+  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
+    int n = idx / kFftJS, c = idx % kFftJS;
+    if (c >= ncol) continue;
+    float2 v = z[idx];
+    float s = wq ? wq[j0 + c] : 1.f;
+    ob[(size_t)(2 * n) * J + c] = v.x * s;
+    ob[(size_t)(2 * n + 1) * J + c] = v.y * s;
+  }
+}
+
+// nodal[b][i][j] -> F[b][row][j] (times wq[j] when given: the forward SHT's
+// quadrature weights; without: the adjoint of the inverse transform).
+template <int N>
+__global__ void __launch_bounds__(kFftThreads)
+rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
+                    int lw, int J, const float2* __restrict__ tw_n,
+                    const float2* __restrict__ tw_i,
+                    const float* __restrict__ wq) {
+  extern __shared__ float2 sm[];
+  float2* A = sm;
+  float2* Bf = A + N * kFftJS;
+  float2* twn = Bf + N * kFftJS;
+  float2* twi = twn + N;
+  const int tid = threadIdx.x;
+  const int b = blockIdx.y;
+  const int j0 = blockIdx.x * kFftJS;
+  const int ncol = min(kFftJS, J - j0);
+  for (int t = tid; t < N; t += kFftThreads) {
+    twn[t] = tw_n[t];
+    twi[t] = tw_i[t];
+  }
+  const float* xb = x + (size_t)b * (2 * N) * J + j0;
+  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
+    int n = idx / kFftJS, c = idx % kFftJS;
+    float2 v = make_float2(0.f, 0.f);
+    if (c < ncol) {
+      v.x = xb[(size_t)(2 * n) * J + c];
+      v.y = xb[(size_t)(2 * n + 1) * J + c];
+    }
+    A[idx] = v;
+  }
+  __syncthreads();
+  float2* Z = stockham<N, -1>(A, Bf, twn);
+  float* Fb = F + (size_t)b * M * J + j0;
+  const float inv_sqrt_2pi = 0.3989422804014327f;
+  const float inv_sqrt_pi = 0.5641895835477563f;
+  for (int idx = tid; idx < lw * kFftJS; idx += kFftThreads) {
+    int k = idx / kFftJS, c = idx % kFftJS;
+    if (c >= ncol) continue;
+    float2 zk = Z[(k % N) * kFftJS + c];
+    float2 zc = cconj(Z[((N - k) % N) * kFftJS + c]);
+    float2 s = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+    float2 d = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
+    // X[k] = s + e^{-2 pi i k / I} * (-i d)
+    float2 xk = cadd(s, cmul(cconj(twi[k]), cmul_i<-1>(d)));
+    float w = wq ? wq[j0 + c] : 1.f;
+    if (k == 0) {
+      Fb[c] = xk.x * w * inv_sqrt_2pi;
+    } else {
+      Fb[(size_t)(2 * k - 1) * J + c] = xk.x * w * inv_sqrt_pi;
+      Fb[(size_t)(2 * k) * J + c] = -xk.y * w * inv_sqrt_pi;
+    }
+  }
+}
+
+// Generic longitude transforms by direct summation with the FP32 real basis
+// f[i][row] (any I, any lw <= I).
+__global__ void dft_inverse_kernel(const float* __restrict__ F,
+                                   float* __restrict__ out, int M, int I, int J,
+                                   const float* __restrict__ f,
+                                   const float* __restrict__ wq) {
+  int j = blockIdx.x * 32 + threadIdx.x;
+  int i = blockIdx.y * 8 + threadIdx.y;
+  int b = blockIdx.z;
+  if (j >= J || i >= I) return;
+  const float* Fb = F + (size_t)b * M * J + j;
+  const float* fi = f + (size_t)i * M;
+  float acc = 0.f;
+  for (int r = 0; r < M; ++r) acc = fmaf(fi[r], Fb[(size_t)r * J], acc);
+  if (wq) acc *= wq[j];
+  out[((size_t)b * I + i) * J + j] = acc;
+}
+
+__global__ void dft_forward_kernel(const float* __restrict__ x,
+                                   float* __restrict__ F, int M, int I, int J,
+                                   const float* __restrict__ f,
+                                   const float* __restrict__ wq) {
+  int j = blockIdx.x * 32 + threadIdx.x;
+  int r = blockIdx.y * 8 + threadIdx.y;
+  int b = blockIdx.z;
+  if (j >= J || r >= M) return;
+  const float* xb = x + (size_t)b * I * J + j;
+  float acc = 0.f;
+  for (int i = 0; i < I; ++i) acc = fmaf(f[(size_t)i * M + r], xb[(size_t)i * J], acc);
+  if (wq) acc *= wq[j];
+  F[((size_t)b * M + r) * J + j] = acc;
+}
+
+template <int N>
+static int configure_rfft() {
+  // Kernel attributes are set once per process, outside any stream capture.
+  static bool configured = false;
+  if (configured) return DINO_OK;
+  const int smem = (int)(sizeof(float2) * (2 * (size_t)N * kFftJS + 2 * N));
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_inverse_kernel<N>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_forward_kernel<N>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  configured = true;
+  return DINO_OK;
+}
+
+template <int N>
+static int launch_rfft(dino_plan* p, const float* in, float* out, int nf,
+                       bool inverse, const float* wq, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * (2 * (size_t)N * kFftJS + 2 * N);
+  if (!p) return configure_rfft<N>();
+  DINO_TRY(configure_rfft<N>());
+  dim3 grid(ceil_div(p->J, kFftJS), nf);
+  if (inverse) {
+    rfft_inverse_kernel<N><<<grid, kFftThreads, smem, st>>>(
+        in, out, p->M, p->lw, p->J, p->d_tw_n, p->d_tw_i, wq);
+    return check_launch("rfft_inverse");
+  }
+  rfft_forward_kernel<N><<<grid, kFftThreads, smem, st>>>(
+      in, out, p->M, p->lw, p->J, p->d_tw_n, p->d_tw_i, wq);
+  return check_launch("rfft_forward");
+}
+
+static int rfft_dispatch_n(int n, dino_plan* p, const float* in, float* out,
+                           int nf, bool inverse, const float* wq,
+                           cudaStream_t st) {
+  switch (n) {
+    case 8: return launch_rfft<8>(p, in, out, nf, inverse, wq, st);
+    case 16: return launch_rfft<16>(p, in, out, nf, inverse, wq, st);
+    case 32: return launch_rfft<32>(p, in, out, nf, inverse, wq, st);
+    case 64: return launch_rfft<64>(p, in, out, nf, inverse, wq, st);
+    case 128: return launch_rfft<128>(p, in, out, nf, inverse, wq, st);
+    case 256: return launch_rfft<256>(p, in, out, nf, inverse, wq, st);
+    case 512: return launch_rfft<512>(p, in, out, nf, inverse, wq, st);
+  }
+  set_error("internal: unsupported FFT length");
+  return DINO_ERR_UNSUPPORTED;
+}
+
+static int rfft_dispatch(dino_plan* p, const float* in, float* out, int nf,
+                         bool inverse, const float* wq, cudaStream_t st) {
+  return rfft_dispatch_n(p->N, p, in, out, nf, inverse, wq, st);
+}
+
+int sht_prepare(dino_plan* p) {
+  if (!p->fft_pow2) return DINO_OK;
+  return rfft_dispatch_n(p->N, nullptr, nullptr, nullptr, 0, true, nullptr, 0);
+}
+
+int fourier_inverse(dino_plan* p, const float* F, float* nodal, int nf,
+                    bool weighted_adjoint, cudaStream_t st) {
+  const float* wq = weighted_adjoint ? p->d_wq : nullptr;
+  if (p->fft_pow2) return rfft_dispatch(p, F, nodal, nf, true, wq, st);
+  dim3 grid(ceil_div(p->J, 32), ceil_div(p->I, 8), nf);
+  dft_inverse_kernel<<<grid, dim3(32, 8), 0, st>>>(F, nodal, p->M, p->I, p->J,
+                                                    p->d_fbasis, wq);
+  return check_launch("dft_inverse");
+}
+
+int fourier_forward(dino_plan* p, const float* nodal, float* F, int nf,
+                    bool weighted, cudaStream_t st) {
+  const float* wq = weighted ? p->d_wq : nullptr;
+  if (p->fft_pow2) return rfft_dispatch(p, nodal, F, nf, false, wq, st);
+  dim3 grid(ceil_div(p->J, 32), ceil_div(p->M, 8), nf);
+  dft_forward_kernel<<<grid, dim3(32, 8), 0, st>>>(nodal, F, p->M, p->I, p->J,
+                                                    p->d_fbasis, wq);
+  return check_launch("dft_forward");
+}
+
+// ---------------------------------------------------------------------------
+// Transform drivers (chunked by workspace capacity)
+// ---------------------------------------------------------------------------
+
+int sht_inverse_segs(dino_plan* p, const Segs& in, float* out, int nf,
+                     float* work, int work_fields, cudaStream_t st) {
+  const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
+  for (int f0 = 0; f0 < nf; f0 += work_fields) {
+    int n = nf - f0 < work_fields ? nf - f0 : work_fields;
+    Segs sub = seg_offset(in, f0, n, ms);
+    DINO_TRY(legendre_inverse(p, sub, work, n, st));
+    DINO_TRY(fourier_inverse(p, work, out + f0 * ns, n, false, st));
+  }
+  return DINO_OK;
+}
+
+int sht_forward_to(dino_plan* p, const float* nodal, float* out, int nf,
+                   float* work, int work_fields, cudaStream_t st) {
+  const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
+  for (int f0 = 0; f0 < nf; f0 += work_fields) {
+    int n = nf - f0 < work_fields ? nf - f0 : work_fields;
+    DINO_TRY(fourier_forward(p, nodal + f0 * ns, work, n, true, st));
+    DINO_TRY(legendre_forward(p, work, out + f0 * ms, n, st));
+  }
+  return DINO_OK;
+}
+
+// Adjoint of the inverse transform: unweighted forward Fourier, then the
+// forward contraction.  Adjoint of the forward transform: the inverse
+// contraction, then the inverse Fourier synthesis scaled by w[j].
+static int sht_inverse_adjoint(dino_plan* p, const float* nodal_ct,
+                               float* modal_ct, int nf, cudaStream_t st) {
+  const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
+  for (int f0 = 0; f0 < nf; f0 += p->max_fields) {
+    int n = nf - f0 < p->max_fields ? nf - f0 : p->max_fields;
+    DINO_TRY(fourier_forward(p, nodal_ct + f0 * ns, p->d_work, n, false, st));
+    DINO_TRY(legendre_forward(p, p->d_work, modal_ct + f0 * ms, n, st));
+  }
+  return DINO_OK;
+}
+
+static int sht_forward_adjoint(dino_plan* p, const float* modal_ct,
+                               float* nodal_ct, int nf, cudaStream_t st) {
+  const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
+  for (int f0 = 0; f0 < nf; f0 += p->max_fields) {
+    int n = nf - f0 < p->max_fields ? nf - f0 : p->max_fields;
+    DINO_TRY(legendre_inverse(p, one_seg(modal_ct + f0 * ms, n), p->d_work, n, st));
+    DINO_TRY(fourier_inverse(p, p->d_work, nodal_ct + f0 * ns, n, true, st));
+  }
+  return DINO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Spectral operators (spherical_harmonic.py:1033-1102)
+// ---------------------------------------------------------------------------
+
+// Spectral operators; `transpose` applies the transposed (adjoint) map.
+// cos_lat_d_dlat: out[l] = ta[l+1] x[l+1] + tb[l-1] x[l-1]
+//   transpose:    out[l] = ta[l] x[l-1] + tb[l] x[l+1]
+// d_dlon is antisymmetric; the Laplacians and the clip are diagonal.
+__global__ void modal_op_kernel(int op, int transpose,
+                                const float* __restrict__ in,
+                                float* __restrict__ out, int nf, int M, int L,
+                                int lw, const float* __restrict__ deriv,
+                                const float* __restrict__ lap,
+                                const float* __restrict__ invlap, int clip_n) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t total = (size_t)nf * M * L;
+  if (idx >= total) return;
+  int l = idx % L;
+  int row = (idx / L) % M;
+  size_t base = idx - l - (size_t)row * L;  // start of this field
+  int m = (row + 1) / 2;
+  const float* x = in + base;
+  float v = 0.f;
+  switch (op) {
+    case DINO_OP_D_DLON: {
+      float s = transpose ? -1.f : 1.f;
+      if (row == 0) v = 0.f;
+      else if (row & 1) v = s * m * x[(size_t)(row + 1) * L + l];
+      else v = -s * m * x[(size_t)(row - 1) * L + l];
+      break;
+    }
+    case DINO_OP_COS_LAT_D_DLAT:
+    case DINO_OP_SEC_LAT_D_DLAT_COS2: {
+      const float* ta = deriv + (op == DINO_OP_COS_LAT_D_DLAT ? 0 : 2) * (size_t)lw * L;
+      const float* tb = ta + (size_t)lw * L;
+      const float* xr = x + (size_t)row * L;
+      const float* tam = ta + (size_t)m * L;
+      const float* tbm = tb + (size_t)m * L;
+      if (!transpose) {
+        if (l + 1 < L) v += tam[l + 1] * xr[l + 1];
+        if (l >= 1) v += tbm[l - 1] * xr[l - 1];
+      } else {
+        if (l >= 1) v += tam[l] * xr[l - 1];
+        if (l + 1 < L) v += tbm[l] * xr[l + 1];
+      }
+      break;
+    }
+    case DINO_OP_LAPLACIAN:
+      v = x[(size_t)row * L + l] * lap[l];
+      break;
+    case DINO_OP_INVERSE_LAPLACIAN:
+      v = x[(size_t)row * L + l] * invlap[l];
+      break;
+    case DINO_OP_CLIP:
+      v = (l < L - clip_n) ? x[(size_t)row * L + l] : 0.f;
+      break;
+  }
+  out[idx] = v;
+}
+
+int modal_op(dino_plan* p, int op, const float* in, float* out, int nf, int arg,
+             cudaStream_t st) {
+  const int transpose = (op & 8) ? 1 : 0;
+  op &= 7;
+  DINO_REQUIRE(op >= DINO_OP_D_DLON && op <= DINO_OP_CLIP, DINO_ERR_ARG,
+               "unknown modal operator");
+  DINO_REQUIRE(op != DINO_OP_CLIP || arg > 0, DINO_ERR_ARG,
+               "`n` must be >= 0");
+  DINO_REQUIRE(in != out, DINO_ERR_ARG, "modal_op: in and out must differ");
+  size_t total = (size_t)nf * p->M * p->L;
+  if (total == 0) return DINO_OK;
+  modal_op_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+      op, transpose, in, out, nf, p->M, p->L, p->lw, p->d_deriv, p->d_lap,
+      p->d_invlap, arg);
+  return check_launch("modal_op");
+}
+
+}  // namespace dino
+
+using namespace dino;
+
+extern "C" {
+
+int dino_sht_inverse(dino_plan* p, const float* modal, float* nodal, int32_t nf,
+                     void* stream) {
+  DINO_REQUIRE(p && modal && nodal, DINO_ERR_ARG, "dino_sht_inverse: null argument");
+  DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  if (nf == 0) return DINO_OK;
+  return sht_inverse_segs(p, one_seg(modal, nf), nodal, nf, p->d_work,
+                          p->max_fields, (cudaStream_t)stream);
+}
+
+int dino_sht_forward(dino_plan* p, const float* nodal, float* modal, int32_t nf,
+                     void* stream) {
+  DINO_REQUIRE(p && modal && nodal, DINO_ERR_ARG, "dino_sht_forward: null argument");
+  DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  if (nf == 0) return DINO_OK;
+  return sht_forward_to(p, nodal, modal, nf, p->d_work, p->max_fields,
+                        (cudaStream_t)stream);
+}
+
+int dino_sht_inverse_adjoint(dino_plan* p, const float* nodal_ct,
+                             float* modal_ct, int32_t nf, void* stream) {
+  DINO_REQUIRE(p && nodal_ct && modal_ct, DINO_ERR_ARG, "null argument");
+  DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  if (nf == 0) return DINO_OK;
+  return sht_inverse_adjoint(p, nodal_ct, modal_ct, nf, (cudaStream_t)stream);
+}
+
+int dino_sht_forward_adjoint(dino_plan* p, const float* modal_ct,
+                             float* nodal_ct, int32_t nf, void* stream) {
+  DINO_REQUIRE(p && nodal_ct && modal_ct, DINO_ERR_ARG, "null argument");
+  DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  if (nf == 0) return DINO_OK;
+  return sht_forward_adjoint(p, modal_ct, nodal_ct, nf, (cudaStream_t)stream);
+}
+
+int dino_modal_op(dino_plan* p, int32_t op, const float* in, float* out,
+                  int32_t nf, int32_t arg, void* stream) {
+  DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_modal_op: null argument");
+  DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  return modal_op(p, op, in, out, nf, arg, (cudaStream_t)stream);
+}
+
+}  // extern "C"

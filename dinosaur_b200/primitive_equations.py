@@ -1,0 +1,419 @@
+"""Primitive equations on sigma levels with CUDA explicit/implicit terms.
+
+Mirrors the sigma-coordinate part of ``dinosaur/primitive_equations.py``
+(reference v1.3.6): ``State`` (:61-84), ``validate_state_shape`` (:87-120),
+the vertical weight matrices (:283-541, FP64 on the host exactly as the
+reference builds them), ``truncated_modal_orography`` (:626-636) and
+``PrimitiveEquationsSigma`` (:835-1458) with ``explicit_terms``,
+``implicit_terms`` and ``implicit_inverse`` ('split' method).  The terms run
+in ``libdino_b200`` on a packed state; ensemble members may be stacked on a
+leading axis of every field.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import functools
+from typing import Any, Mapping
+
+import numpy as np
+import torch
+
+from dinosaur_b200 import _lib
+from dinosaur_b200 import coordinate_systems
+from dinosaur_b200 import pytree
+from dinosaur_b200 import sigma_coordinates
+from dinosaur_b200 import spherical_harmonic as sh
+from dinosaur_b200 import time_integration
+from dinosaur_b200 import units
+
+Array = Any
+
+
+# ---------------------------------------------------------------------------
+# State
+# ---------------------------------------------------------------------------
+
+
+def _binary(op):
+  def f(self, other):
+    if isinstance(other, State):
+      return pytree.tree_map(lambda a, b: op(a, b) if a is not None else None,
+                             self, other)
+    return pytree.tree_map(lambda a: op(a, other) if a is not None else None,
+                           self)
+  return f
+
+
+@dataclasses.dataclass
+class State:
+  """State of the primitive equations (primitive_equations.py:61-84)."""
+
+  vorticity: Array
+  divergence: Array
+  temperature_variation: Array
+  log_surface_pressure: Array
+  tracers: Mapping[str, Array] = dataclasses.field(default_factory=dict)
+  sim_time: float | None = None
+
+  __add__ = _binary(lambda a, b: a + b)
+  __sub__ = _binary(lambda a, b: a - b)
+  __mul__ = _binary(lambda a, b: a * b)
+  __rmul__ = _binary(lambda a, b: b * a)
+  __truediv__ = _binary(lambda a, b: a / b)
+
+  def __neg__(self):
+    return pytree.tree_map(lambda a: -a, self)
+
+  @property
+  def fields(self):
+    return dataclasses.fields(self)
+
+  def asdict(self):
+    return {f.name: getattr(self, f.name) for f in dataclasses.fields(self)
+            if f.name != 'sim_time' or self.sim_time is not None}
+
+
+class StateShapeError(Exception):
+  """Exceptions for unexpected state shapes."""
+
+
+def validate_state_shape(state: State,
+                         coords: coordinate_systems.CoordinateSystem):
+  """primitive_equations.py:87-120 (a leading member axis is allowed)."""
+  def check(name, arr, expected):
+    shape = tuple(arr.shape)
+    if shape[-len(expected):] != tuple(expected) or len(shape) > len(expected) + 1:
+      raise StateShapeError(f'Expected {name} shape {expected}; got shape {shape}.')
+  check('vorticity', state.vorticity, coords.modal_shape)
+  check('divergence', state.divergence, coords.modal_shape)
+  check('temperature_variation', state.temperature_variation, coords.modal_shape)
+  check('log_surface_pressure', state.log_surface_pressure,
+        coords.surface_modal_shape)
+  for name, arr in state.tracers.items():
+    if tuple(arr.shape[-3:]) != tuple(coords.modal_shape):
+      raise StateShapeError(f'Expected tracer {name} shape {coords.modal_shape}; '
+                            f'got shape {tuple(arr.shape)}.')
+
+
+# ---------------------------------------------------------------------------
+# Vertical weights (host, FP64 with the reference's dtype behaviour)
+# ---------------------------------------------------------------------------
+
+
+def get_sigma_ratios(coordinates: sigma_coordinates.SigmaCoordinates):
+  """primitive_equations.py:283-303."""
+  alpha = np.diff(np.log(coordinates.centers), append=0) / 2
+  alpha[-1] = -np.log(coordinates.centers[-1])
+  return alpha
+
+
+def get_geopotential_weights_sigma(coordinates, ideal_gas_constant):
+  """G (primitive_equations.py:306-338)."""
+  alpha = get_sigma_ratios(coordinates)
+  k = coordinates.layers
+  weights = np.zeros([k, k])
+  for j in range(k):
+    weights[j, j] = alpha[j]
+    for kk in range(j + 1, k):
+      weights[j, kk] = alpha[kk] + alpha[kk - 1]
+  return ideal_gas_constant * weights
+
+
+def get_temperature_implicit_weights_sigma(coordinates, reference_temperature,
+                                           kappa):
+  """H (primitive_equations.py:419-502)."""
+  reference_temperature = np.asarray(reference_temperature)
+  if (reference_temperature.ndim != 1
+      or reference_temperature.shape[-1] != coordinates.layers):
+    raise ValueError(
+        '`reference_temp` must be a vector of length `coordinates.layers`; '
+        f'got shape {reference_temperature.shape} and '
+        f'{coordinates.layers} layers.')
+  k = coordinates.layers
+  p = np.tril(np.ones([k, k]))
+  alpha = get_sigma_ratios(coordinates)[..., None]
+  p_alpha = p * alpha
+  p_alpha_shifted = np.roll(p_alpha, 1, axis=0)
+  p_alpha_shifted[0] = 0
+  h0 = (kappa * reference_temperature[..., None] * (p_alpha + p_alpha_shifted)
+        / coordinates.layer_thickness[..., None])
+  temp_diff = np.diff(reference_temperature)
+  thickness_sum = coordinates.layer_thickness[:-1] + coordinates.layer_thickness[1:]
+  k0 = np.concatenate((temp_diff / thickness_sum, [0]), axis=0)[..., None]
+  thickness_cumulative = np.cumsum(coordinates.layer_thickness)[..., None]
+  k1 = p - thickness_cumulative
+  kk = k0 * k1
+  k_shifted = np.roll(kk, 1, axis=0)
+  k_shifted[0] = 0
+  return (h0 - kk - k_shifted) * coordinates.layer_thickness
+
+
+def truncated_modal_orography(orography, coords, wavenumbers_to_clip: int = 1):
+  """primitive_equations.py:626-636."""
+  grid = coords.horizontal
+  if tuple(np.shape(orography)) != tuple(grid.nodal_shape):
+    raise ValueError(f'Expected nodal orography with shape={grid.nodal_shape}')
+  return grid.clip_wavenumbers(grid.to_modal(orography), n=wavenumbers_to_clip)
+
+
+# ---------------------------------------------------------------------------
+# Packed-state engine
+# ---------------------------------------------------------------------------
+
+
+class _Engine:
+  """A ``dino_pe`` for one (members, tracer names) combination."""
+
+  def __init__(self, eq: PrimitiveEquationsSigma, members: int,
+               tracer_names: tuple[str, ...]):
+    grid = eq.coords.horizontal
+    vert = eq.coords.vertical
+    ps = eq.physics_specs
+    self.grid = grid
+    self.members = members
+    self.tracer_names = tracer_names
+    self.K = vert.layers
+    self.M, self.L = grid.modal_shape
+    hum = -1
+    if eq.humidity_key is not None:
+      if eq.humidity_key not in tracer_names:
+        raise ValueError(f'`{eq.humidity_key}` is not found in tracers: '
+                         f'{tracer_names}.')
+      hum = tracer_names.index(eq.humidity_key)
+    K = self.K
+    # Host constants, kept alive for the duration of the create call.
+    self._arrays = dict(
+        bounds=np.ascontiguousarray(vert.boundaries, np.float64),
+        centers=np.ascontiguousarray(vert.centers, np.float64),
+        thick=np.ascontiguousarray(vert.layer_thickness, np.float64),
+        inv_c2c=np.ascontiguousarray(
+            (1 / vert.center_to_center) if K > 1 else np.zeros(1), np.float64),
+        tref=np.ascontiguousarray(eq.reference_temperature, np.float64),
+        G=np.ascontiguousarray(get_geopotential_weights_sigma(vert, ps.R),
+                               np.float64),
+        H=np.ascontiguousarray(get_temperature_implicit_weights_sigma(
+            vert, eq.reference_temperature, ps.kappa), np.float64),
+        alpha=np.ascontiguousarray(get_sigma_ratios(vert), np.float64),
+    )
+    orog = eq.orography
+    if isinstance(orog, torch.Tensor):
+      orog = orog.detach().cpu().numpy()
+    self._orog = np.ascontiguousarray(np.asarray(orog, np.float32).reshape(
+        self.M, self.L))
+    a = self._arrays
+    hs = eq.held_suarez
+    desc = _lib.PEDesc(
+        layers=K, members=members, n_tracers=len(tracer_names),
+        humidity_tracer=hum,
+        include_vertical_advection=int(eq.include_vertical_advection),
+        held_suarez=int(hs is not None),
+        sigma_boundaries=_lib.dptr(a['bounds']),
+        sigma_centers=_lib.dptr(a['centers']),
+        layer_thickness=_lib.dptr(a['thick']),
+        inv_center_to_center=_lib.dptr(a['inv_c2c']),
+        reference_temperature=_lib.dptr(a['tref']),
+        geopotential_weights=_lib.dptr(a['G']),
+        temperature_weights=_lib.dptr(a['H']),
+        sigma_ratios=_lib.dptr(a['alpha']),
+        orography_modal=self._orog.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        angular_velocity=ps.angular_velocity, gravity=ps.g, R=ps.R,
+        R_vapor=ps.R_vapor, Cp_vapor=ps.Cp_vapor, kappa=ps.kappa)
+    if hs is not None:
+      desc.hs_p0 = hs.p0
+      desc.hs_sigma_b = hs.sigma_b
+      desc.hs_kf = hs.kf
+      desc.hs_ka = hs.ka
+      desc.hs_ks = hs.ks
+      desc.hs_minT = hs.minT
+      desc.hs_maxT = hs.maxT
+      desc.hs_dTy = hs.dTy
+      desc.hs_dThz = hs.dThz
+    plan = grid.plan
+    self.plan = plan  # keep the plan alive while the engine lives
+    handle = ctypes.c_void_p()
+    _lib.check(_lib.lib().dino_pe_create(plan.handle, ctypes.byref(desc),
+                                         ctypes.byref(handle)), 'dino_pe_create')
+    self.handle = handle
+    self.size = int(_lib.lib().dino_pe_state_size(handle))
+    self.plane = self.M * self.L
+
+  def __del__(self):
+    h = getattr(self, 'handle', None)
+    if h is not None and h.value:
+      try:
+        _lib.lib().dino_pe_destroy(h)
+      except Exception:
+        pass
+
+  # -- packing -------------------------------------------------------------
+  def pack(self, state: State) -> torch.Tensor:
+    mK = self.members * self.K
+    parts = [sh.as_device_tensor(state.vorticity).reshape(mK, self.M, self.L),
+             sh.as_device_tensor(state.divergence).reshape(mK, self.M, self.L),
+             sh.as_device_tensor(state.temperature_variation).reshape(
+                 mK, self.M, self.L)]
+    for name in self.tracer_names:
+      parts.append(sh.as_device_tensor(state.tracers[name]).reshape(
+          mK, self.M, self.L))
+    parts.append(sh.as_device_tensor(state.log_surface_pressure).reshape(
+        self.members, self.M, self.L))
+    buf = torch.cat(parts).reshape(-1).contiguous()
+    assert buf.numel() == self.size
+    return buf
+
+  def unpack(self, buf: torch.Tensor, like: State, sim_time=None) -> State:
+    mK = self.members * self.K
+    planes = buf.view(-1, self.M, self.L)
+    shape3 = tuple(like.vorticity.shape)
+    lshape = tuple(like.log_surface_pressure.shape)
+    out = State(
+        vorticity=planes[0:mK].view(shape3),
+        divergence=planes[mK:2 * mK].view(shape3),
+        temperature_variation=planes[2 * mK:3 * mK].view(shape3),
+        log_surface_pressure=planes[(3 + len(self.tracer_names)) * mK:].view(
+            lshape),
+        tracers={name: planes[(3 + t) * mK:(4 + t) * mK].view(
+            tuple(like.tracers[name].shape))
+                 for t, name in enumerate(self.tracer_names)},
+        sim_time=sim_time)
+    return out
+
+  # -- calls ---------------------------------------------------------------
+  def _out(self):
+    return torch.empty(self.size, device='cuda', dtype=torch.float32)
+
+  def explicit(self, buf):
+    out = self._out()
+    _lib.check(_lib.lib().dino_pe_explicit(self.handle, sh.ptr(buf), sh.ptr(out),
+                                           sh.stream_handle()), 'explicit_terms')
+    return out
+
+  def implicit(self, buf):
+    out = self._out()
+    _lib.check(_lib.lib().dino_pe_implicit(self.handle, sh.ptr(buf), sh.ptr(out),
+                                           sh.stream_handle()), 'implicit_terms')
+    return out
+
+  def inverse(self, buf, eta):
+    out = self._out()
+    _lib.check(_lib.lib().dino_pe_implicit_inverse(
+        self.handle, sh.ptr(buf), sh.ptr(out), float(eta), sh.stream_handle()),
+               'implicit_inverse')
+    return out
+
+  def step_(self, buf, dt, filt, n_steps, graph=False):
+    fptr = None
+    if filt is not None:
+      self._filt = np.ascontiguousarray(filt, np.float64)
+      if self._filt.shape != (self.L,):
+        raise ValueError(f'filter scaling must have shape ({self.L},)')
+      fptr = _lib.dptr(self._filt)
+    fn = (_lib.lib().dino_pe_step_graph if graph else _lib.lib().dino_pe_step)
+    _lib.check(fn(self.handle, sh.ptr(buf), float(dt), fptr, int(n_steps),
+                  sh.stream_handle()), 'step')
+    return buf
+
+
+# ---------------------------------------------------------------------------
+# Equations
+# ---------------------------------------------------------------------------
+
+
+@dataclasses.dataclass(eq=False)
+class PrimitiveEquationsSigma(time_integration.ImplicitExplicitODE):
+  """Primitive equations on sigma coordinates (primitive_equations.py:835-1458).
+
+  ``implicit_inverse_method`` accepts the reference's values; all of them are
+  evaluated with the per-wavenumber dense inverse ('split'), which the
+  reference's 'stacked' and 'blockwise' methods equal up to round-off.
+  """
+
+  reference_temperature: np.ndarray
+  orography: Array
+  coords: coordinate_systems.CoordinateSystem
+  physics_specs: units.SimUnits
+  vertical_matmul_method: str | None = dataclasses.field(default=None,
+                                                          kw_only=True)
+  implicit_inverse_method: str = dataclasses.field(default='split',
+                                                   kw_only=True)
+  include_vertical_advection: bool = dataclasses.field(default=True,
+                                                       kw_only=True)
+  humidity_key: str | None = dataclasses.field(default=None, kw_only=True)
+  cloud_keys: tuple[str, ...] | None = dataclasses.field(default=None,
+                                                         kw_only=True)
+  held_suarez: Any = dataclasses.field(default=None, kw_only=True)
+
+  def __post_init__(self):
+    if not np.allclose(self.coords.horizontal.radius,
+                       self.physics_specs.radius, rtol=1e-5):
+      raise ValueError(
+          'inconsistent radius between coordinates and constants: '
+          f'{self.coords.horizontal.radius=} != {self.physics_specs.radius=}')
+    if self.cloud_keys is not None and self.humidity_key is None:
+      raise ValueError('cloud_keys requires humidity_key to be set.')
+    if self.cloud_keys is not None:
+      raise NotImplementedError('cloud_keys are not supported by this build')
+    if self.implicit_inverse_method not in ('split', 'stacked', 'blockwise'):
+      raise ValueError(
+          f'invalid implicit_inverse_method {self.implicit_inverse_method}')
+    self.reference_temperature = np.asarray(self.reference_temperature)
+    self._engines = {}
+
+  @property
+  def T_ref(self):
+    return self.reference_temperature[..., None, None]
+
+  @property
+  def coriolis_parameter(self):
+    _, sin_lat = self.coords.horizontal.nodal_mesh
+    return 2 * self.physics_specs.angular_velocity * sin_lat
+
+  def _members(self, state: State) -> int:
+    nd = state.vorticity.ndim
+    if nd == 3:
+      return 1
+    if nd == 4:
+      return int(state.vorticity.shape[0])
+    raise StateShapeError(f'unexpected vorticity rank {nd}')
+
+  def engine(self, state: State) -> _Engine:
+    validate_state_shape(state, self.coords)
+    key = (self._members(state), tuple(state.tracers.keys()))
+    eng = self._engines.get(key)
+    if eng is None:
+      eng = _Engine(self, *key)
+      self._engines[key] = eng
+    return eng
+
+  def explicit_terms(self, state: State) -> State:
+    """primitive_equations.py:1126-1194."""
+    eng = self.engine(state)
+    out = eng.explicit(eng.pack(state))
+    return eng.unpack(out, state,
+                      None if state.sim_time is None else 1.0)
+
+  def implicit_terms(self, state: State) -> State:
+    """primitive_equations.py:1196-1249."""
+    eng = self.engine(state)
+    out = eng.implicit(eng.pack(state))
+    return eng.unpack(out, state, None if state.sim_time is None else 0.0)
+
+  def implicit_inverse(self, state: State, step_size: float) -> State:
+    """(1 - step_size * implicit_terms)^-1 (primitive_equations.py:1251-1330)."""
+    if isinstance(step_size, torch.Tensor):
+      raise TypeError(
+          f'`step_size` must be concrete but a tensor was passed: {step_size}.')
+    eng = self.engine(state)
+    out = eng.inverse(eng.pack(state), float(step_size))
+    return eng.unpack(out, state, state.sim_time)
+
+
+PrimitiveEquations = PrimitiveEquationsSigma
+
+
+def MoistPrimitiveEquations(*args, **kwargs):  # pylint: disable=invalid-name
+  """Deprecated alias of the reference (primitive_equations.py:2560-2596)."""
+  kwargs.setdefault('humidity_key', 'specific_humidity')
+  return PrimitiveEquationsSigma(*args, **kwargs)

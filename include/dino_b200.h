@@ -1,0 +1,185 @@
+/*
+ * dino_b200 -- C ABI of the B200-native spectral dynamical-core step.
+ *
+ * Every entry point returns an int status (DINO_OK = 0) and never throws;
+ * dino_last_error() returns a thread-local message for the last failure.
+ * Pointers named d_* are device pointers; `stream` is a cudaStream_t passed as
+ * void* (NULL = legacy default stream).  Array layouts follow the reference:
+ *   nodal  [fields][longitude I][latitude J]  (latitude fastest, ascending sin)
+ *   modal  [fields][M = 2*lw-1][L = tw]       (rows m = 0, +1, -1, +2, -2, ...)
+ * Objects (plans, equations) are immutable after creation except for internal
+ * caches and may be shared by threads that use distinct streams; calls that
+ * share a workspace must not overlap in time (one stream per object).
+ *
+ * Reference interfaces replaced (neuralgcm/dinosaur 1.3.6, file:line):
+ *   dino_plan_create        Grid.spherical_harmonics / RealSphericalHarmonics.basis
+ *                           (dinosaur/spherical_harmonic.py:935-949, :219-260),
+ *                           associated_legendre.evaluate / gauss_legendre_nodes
+ *                           (dinosaur/associated_legendre.py:70-114)
+ *   dino_sht_inverse        Grid.to_nodal -> RealSphericalHarmonics.inverse_transform
+ *                           (dinosaur/spherical_harmonic.py:1017-1023, :262-269)
+ *   dino_sht_forward        Grid.to_modal -> RealSphericalHarmonics.transform
+ *                           (dinosaur/spherical_harmonic.py:1025-1031, :271-280)
+ *   dino_sht_*_adjoint      the VJPs JAX derives for the two einsum pairs above
+ *   dino_modal_op           Grid.d_dlon / cos_lat_d_dlat / sec_lat_d_dlat_cos2 /
+ *                           laplacian / inverse_laplacian / clip_wavenumbers
+ *                           (dinosaur/spherical_harmonic.py:1033-1102)
+ *   dino_pe_create          PrimitiveEquationsSigma.__init__ + weight matrices
+ *                           (dinosaur/primitive_equations.py:283-598, :697-724)
+ *   dino_pe_explicit        PrimitiveEquationsSigma.explicit_terms (:1126-1194)
+ *   dino_pe_implicit        PrimitiveEquationsSigma.implicit_terms (:1196-1249)
+ *   dino_pe_implicit_inverse PrimitiveEquationsSigma.implicit_inverse, 'split'
+ *                           (:1251-1330)
+ *   dino_pe_step            step_with_filters(imex_rk_sil3(eq, dt), [filter])
+ *                           repeated n times (dinosaur/time_integration.py:375-405,
+ *                           :427-455, :494-520)
+ */
+#ifndef DINO_B200_H_
+#define DINO_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DINO_API __attribute__((visibility("default")))
+#else
+#define DINO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define DINO_OK 0
+#define DINO_ERR_ARG 1         /* bad argument (null pointer, bad enum)      */
+#define DINO_ERR_SHAPE 2       /* inconsistent sizes                         */
+#define DINO_ERR_CUDA 3        /* a CUDA runtime call failed                 */
+#define DINO_ERR_TIMEOUT 4     /* a bounded device wait gave up              */
+#define DINO_ERR_NAN 5         /* non-finite value where the reference asserts */
+#define DINO_ERR_UNSUPPORTED 6 /* configuration not supported by this build  */
+
+/* Latitude spacings (spherical_harmonic.py:43-47). */
+#define DINO_SPACING_GAUSS 0
+#define DINO_SPACING_EQUIANGULAR 1
+#define DINO_SPACING_EQUIANGULAR_WITH_POLES 2
+
+/* Legendre-contraction arithmetic. */
+#define DINO_PREC_FP32 0    /* SIMT FP32 FMA (plain form)                          */
+#define DINO_PREC_BF16X3 1  /* tcgen05 kind::f16, hi*hi + hi*lo + lo*hi, FP32 accum */
+
+/* Modal operators for dino_modal_op. */
+#define DINO_OP_D_DLON 0
+#define DINO_OP_COS_LAT_D_DLAT 1
+#define DINO_OP_SEC_LAT_D_DLAT_COS2 2
+#define DINO_OP_LAPLACIAN 3
+#define DINO_OP_INVERSE_LAPLACIAN 4
+#define DINO_OP_CLIP 5
+
+typedef struct dino_grid_desc {
+  int32_t longitude_wavenumbers; /* lw: m in [0, lw)                 */
+  int32_t total_wavenumbers;     /* tw = L: l in [0, tw)             */
+  int32_t longitude_nodes;       /* I                                */
+  int32_t latitude_nodes;        /* J                                */
+  int32_t latitude_spacing;      /* DINO_SPACING_*                   */
+  int32_t reserved;
+  double radius;                 /* sphere radius (nondimensional)   */
+  /* Optional host arrays (length J) of sin(latitude) nodes and weights for
+   * non-Gauss spacings; NULL for Gauss nodes, which are built on the GPU. */
+  const double* host_nodes;
+  const double* host_weights;
+} dino_grid_desc;
+
+typedef struct dino_plan dino_plan;
+typedef struct dino_pe dino_pe;
+
+/* Copies the last error message of this thread into buf (NUL-terminated). */
+DINO_API int dino_last_error(char* buf, size_t len);
+/* Library version string, e.g. "dino_b200 0.1 sm_100a". */
+DINO_API const char* dino_version(void);
+
+/* Builds a transform plan on the current device: FP64 Gauss nodes/weights and
+ * associated-Legendre tables computed on the GPU, rounded to the working
+ * precision; a workspace for up to max_fields fields per call. */
+DINO_API int dino_plan_create(const dino_grid_desc* desc, int32_t max_fields,
+                     int32_t precision, dino_plan** out);
+DINO_API int dino_plan_destroy(dino_plan* plan);
+/* Copies the FP64 sin(latitude) nodes and quadrature weights (length J). */
+DINO_API int dino_plan_nodes(const dino_plan* plan, double* host_sin_lat,
+                    double* host_weights);
+/* Copies the FP32 Legendre table entry p[m, j, l] for one (m, l) over all j
+ * into host_out (length J); used by tests. */
+DINO_API int dino_plan_legendre_column(const dino_plan* plan, int32_t m, int32_t l,
+                              double* host_out);
+
+/* modal [nfields][M][L] -> nodal [nfields][I][J]. */
+DINO_API int dino_sht_inverse(dino_plan* plan, const float* d_modal, float* d_nodal,
+                     int32_t nfields, void* stream);
+/* nodal [nfields][I][J] -> modal [nfields][M][L]. */
+DINO_API int dino_sht_forward(dino_plan* plan, const float* d_nodal, float* d_modal,
+                     int32_t nfields, void* stream);
+/* Transposes of the two maps above: nodal cotangent -> modal cotangent and
+ * modal cotangent -> nodal cotangent. */
+DINO_API int dino_sht_inverse_adjoint(dino_plan* plan, const float* d_nodal_ct,
+                             float* d_modal_ct, int32_t nfields, void* stream);
+DINO_API int dino_sht_forward_adjoint(dino_plan* plan, const float* d_modal_ct,
+                             float* d_nodal_ct, int32_t nfields, void* stream);
+/* One spectral operator (DINO_OP_*) on modal [nfields][M][L]; `arg` is the
+ * number of wavenumbers to clip for DINO_OP_CLIP and is ignored otherwise. */
+DINO_API int dino_modal_op(dino_plan* plan, int32_t op, const float* d_in, float* d_out,
+                  int32_t nfields, int32_t arg, void* stream);
+
+/* Primitive equations on sigma levels.  Packed state layout (device, FP32),
+ * kind-major so each kind is contiguous over members and levels:
+ *   [vorticity  members*K][divergence members*K][temperature members*K]
+ *   [tracer_0 members*K]...[tracer_{n-1} members*K][log_ps members]
+ * each entry one modal [M][L] plane. */
+typedef struct dino_pe_desc {
+  int32_t layers;              /* K                                        */
+  int32_t members;             /* ensemble members in one launch           */
+  int32_t n_tracers;
+  int32_t humidity_tracer;     /* index of specific humidity, -1 if dry    */
+  int32_t include_vertical_advection;
+  int32_t held_suarez;         /* 1: add HeldSuarezForcingSigma tendencies */
+  const double* sigma_boundaries;     /* host, K+1 (the reference's dtype) */
+  const double* sigma_centers;        /* host, K                           */
+  const double* layer_thickness;      /* host, K                           */
+  const double* inv_center_to_center; /* host, K-1: 1/(sigma[k+1]-sigma[k]) as the
+                                         reference forms it (in the sigma dtype) */
+  const double* reference_temperature;/* host, K                           */
+  const double* geopotential_weights; /* host, K*K (G, includes R)         */
+  const double* temperature_weights;  /* host, K*K (H)                     */
+  const double* sigma_ratios;         /* host, K (alpha)                   */
+  const float* orography_modal;       /* host, M*L (modal orography)       */
+  double angular_velocity, gravity, R, R_vapor, Cp_vapor, kappa;
+  /* Held-Suarez constants (nondimensional), used when held_suarez = 1. */
+  double hs_p0, hs_sigma_b, hs_kf, hs_ka, hs_ks, hs_minT, hs_maxT, hs_dTy,
+      hs_dThz;
+} dino_pe_desc;
+
+DINO_API int dino_pe_create(dino_plan* plan, const dino_pe_desc* desc, dino_pe** out);
+DINO_API int dino_pe_destroy(dino_pe* pe);
+/* Size in floats of one packed state. */
+DINO_API int64_t dino_pe_state_size(const dino_pe* pe);
+DINO_API int dino_pe_explicit(dino_pe* pe, const float* d_state, float* d_tendency,
+                     void* stream);
+DINO_API int dino_pe_implicit(dino_pe* pe, const float* d_state, float* d_out,
+                     void* stream);
+DINO_API int dino_pe_implicit_inverse(dino_pe* pe, const float* d_state, float* d_out,
+                             double step_size, void* stream);
+/* Advances d_state in place by n_steps of imex_rk_sil3 with time step dt,
+ * followed each step by multiplication with the per-l filter scaling
+ * (host array of length L, e.g. the exponential step filter; NULL = none). */
+DINO_API int dino_pe_step(dino_pe* pe, float* d_state, double dt,
+                 const double* host_filter, int32_t n_steps, void* stream);
+/* Captures one filtered step into a CUDA graph (created on first use for this
+ * (dt, filter)); dino_pe_step_graph then replays it n_steps times. */
+DINO_API int dino_pe_step_graph(dino_pe* pe, float* d_state, double dt,
+                       const double* host_filter, int32_t n_steps,
+                       void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DINO_B200_H_ */
