@@ -1,0 +1,451 @@
+#!/usr/bin/env python
+"""Benchmark of the spectral-transform hot path on B200.
+
+Headline workload: the spherical-harmonic transform pair (inverse then
+forward, ``Grid.to_nodal`` / ``Grid.to_modal``) on Grid.TL255 (512 x 256
+nodes, 257 total wavenumbers) for a batch of 128 float32 fields (32 levels x
+4 variables), seeded synthetic spectral coefficients (complex Gaussians scaled
+by (l+1)^-1.5, top wavenumber zeroed).  Metric: algorithmic SHT TFLOP/s,
+counting the triangular Legendre work 2 * J * N_tri per field per direction.
+
+One JSON line is printed by rank 0.  ``--impl reference`` times the CPU
+restatement of the reference's Real spherical-harmonic transform (NumPy FP32
+einsums, all host threads) on a bounded sample of the same workload.
+Multi-GPU runs (torchrun) are independent replicas (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = dict(name='TL255', max_wavenumber=255, gaussian_nodes=128)
+FIELDS = 128
+
+
+def workload_dims():
+  lw = GRID['max_wavenumber'] + 1
+  L = GRID['max_wavenumber'] + 2
+  I, J = 4 * GRID['gaussian_nodes'], 2 * GRID['gaussian_nodes']
+  M = 2 * lw - 1
+  n_tri = L + 2 * sum(L - m for m in range(1, lw))
+  return lw, L, I, J, M, n_tri
+
+
+def sht_flops(fields):
+  _, _, _, J, _, n_tri = workload_dims()
+  return 2.0 * 2.0 * J * n_tri * fields  # 2 directions x 2 flops x J x N_tri
+
+
+def modal_input(fields, seed=0):
+  """Seeded complex Gaussians (Re -> cos row, Im -> sin row) * (l+1)^-1.5."""
+  lw, L, _, _, M, _ = workload_dims()
+  rng = np.random.default_rng(seed)
+  re = rng.standard_normal((fields, lw, L))
+  im = rng.standard_normal((fields, lw, L))
+  out = np.zeros((fields, M, L))
+  out[:, 0] = re[:, 0]
+  out[:, 1::2] = re[:, 1:]
+  out[:, 2::2] = im[:, 1:]
+  m = np.concatenate([[0], np.repeat(np.arange(1, lw), 2)])
+  l = np.arange(L)
+  mask = m[:, None] <= l[None, :]
+  out *= mask / (l + 1.0) ** 1.5
+  out[..., -1] = 0
+  return out.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+  FIELDS = ('clocks.sm,clocks.max.sm,clocks_event_reasons.active,'
+            'clocks_event_reasons.hw_slowdown,'
+            'clocks_event_reasons.hw_thermal_slowdown,'
+            'clocks_event_reasons.sw_thermal_slowdown,'
+            'clocks_event_reasons.sw_power_cap')
+
+  def __init__(self, device_index):
+    self.proc = None
+    try:
+      self.proc = subprocess.Popen(
+          ['nvidia-smi', f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
+           '-lms', '100', '-i', str(device_index)],
+          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except (OSError, FileNotFoundError):
+      self.proc = None
+
+  def stop(self):
+    if self.proc is None:
+      return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+    self.proc.terminate()
+    try:
+      out, _ = self.proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+      self.proc.kill()
+      out, _ = self.proc.communicate()
+    sm, smax, reasons = [], None, set()
+    names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+             'sw_power_cap']
+    for line in out.strip().splitlines():
+      parts = [p.strip() for p in line.split(',')]
+      if len(parts) < 7:
+        continue
+      try:
+        sm.append(float(parts[0]))
+        smax = float(parts[1])
+      except ValueError:
+        continue
+      for name, val in zip(names, parts[3:7]):
+        if val.lower().startswith('active'):
+          reasons.add(name)
+    under_load = [s for s in sm if smax and s > 0.3 * smax] or sm
+    return {'sm_mhz': statistics.median(under_load) if under_load else None,
+            'sm_max_mhz': smax, 'reasons': sorted(reasons),
+            'samples': len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (oracle port of the reference's Real SHT)
+# ---------------------------------------------------------------------------
+
+def cpu_sht_sample(fields, seconds=10.0):
+  """Times the reference's einsum SHT pair (FP32 NumPy) on `fields` fields."""
+  from oracle import sht as osht  # CPU baseline only
+  og = osht.Grid.TL255()
+  f, p, w = og.basis
+  f, p, w = f.astype(np.float32), p.astype(np.float32), w.astype(np.float32)
+  x = modal_input(fields, seed=1)
+  ft = np.ascontiguousarray(f.T)
+  pt = np.ascontiguousarray(np.swapaxes(p, -1, -2))
+
+  def pair(xx):
+    px = np.matmul(p, xx[..., None])[..., 0]            # 'mjl,...ml->...mj'
+    nodal = np.matmul(f, px)                            # 'im,...mj->...ij'
+    fwx = np.matmul(ft, w * nodal)                      # 'im,...ij->...mj'
+    return np.matmul(pt, fwx[..., None])[..., 0]        # 'mjl,...mj->...ml'
+
+  pair(x[:1])
+  times = []
+  t_end = time.perf_counter() + seconds
+  while time.perf_counter() < t_end or len(times) < 2:
+    t0 = time.perf_counter()
+    pair(x)
+    times.append(time.perf_counter() - t0)
+  return statistics.median(times), len(times)
+
+
+def cpu_baseline_entry(fields=4, seconds=10.0):
+  t, reps = cpu_sht_sample(fields, seconds)
+  return {'value': sht_flops(fields) / t / 1e12, 'unit': 'TFLOP/s',
+          'cores': os.cpu_count(), 'kind': 'port',
+          'sample': f'{fields} of {FIELDS} TL255 fields per pair, FP32 NumPy '
+                    f'einsums of the reference Real SHT, median of {reps} pairs'}
+
+
+def run_reference(args):
+  rank = int(os.environ.get('RANK', '0'))
+  if rank != 0:
+    return
+  fields = 8
+  for _ in range(args.warmup):
+    cpu_sht_sample(fields, seconds=0.0)
+  times = []
+  for _ in range(args.steps):
+    t, _ = cpu_sht_sample(fields, seconds=0.0)
+    times.append(t)
+  t = statistics.median(times)
+  value = sht_flops(fields) / t / 1e12
+  line = {
+      'metric': 'SHT TFLOP/s (TL255 fwd+inv pair, 128 fields)',
+      'value': value, 'unit': 'TFLOP/s', 'n_gpus': args.gpus,
+      'steps': args.steps, 'warmup': args.warmup,
+      'ms_per_step': t * 1e3 * FIELDS / fields,
+      'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+      'dtype': 'f32', 'data': 'synthetic',
+      'config': {'workload': 'SHT pair TL255 x 128 fields (CPU sample)',
+                 'grid': 'TL255', 'fields': FIELDS, 'sample_fields': fields},
+      'impl': 'reference',
+      'cpu_baseline': {'value': value, 'unit': 'TFLOP/s',
+                       'cores': os.cpu_count(), 'kind': 'port',
+                       'sample': f'{fields} fields per pair; NumPy FP32 '
+                                 'restatement of the reference Real SHT '
+                                 '(JAX is not installed)'},
+      'e2e': {'value': value, 'unit': 'TFLOP/s', 'h2d_bytes_per_step': 0,
+              'd2h_bytes_per_step': 0},
+  }
+  print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Multi-rank helpers (replicas: no collective on the data path)
+# ---------------------------------------------------------------------------
+
+def replica_seed(rank):
+  """Each replica transforms its own seeded batch."""
+  return 1000 + rank
+
+
+def max_over_ranks(value, device='cpu'):
+  """Max of a per-rank float over the default process group (or the value)."""
+  import torch
+  import torch.distributed as dist
+  if not (dist.is_available() and dist.is_initialized()):
+    return float(value)
+  t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+  dist.all_reduce(t, op=dist.ReduceOp.MAX)
+  return float(t.item())
+
+
+def aggregate_tflops(flops_per_rank, world, ms_max):
+  """Whole-job throughput: every rank does flops_per_rank in ms_max."""
+  return world * flops_per_rank / (ms_max * 1e-3) / 1e12
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def phase_bytes(phase, fields, precision):
+  lw, L, I, J, M, n_tri = workload_dims()
+  Jh = J // 2
+  table_elems = Jh * sum(L - m for m in range(lw))
+  table_bytes = table_elems * (4 if precision == 'fp32' else 4)  # fp32 or bf16 hi+lo
+  modal = fields * M * L * 4
+  fourier = fields * M * J * 4
+  nodal = fields * I * J * 4
+  return {'legendre_inverse': modal + fourier + table_bytes,
+          'fourier_inverse': fourier + nodal,
+          'fourier_forward': nodal + fourier,
+          'legendre_forward': fourier + modal + table_bytes}[phase]
+
+
+def run_ours(args):
+  import torch
+  import torch.distributed as dist
+  from dinosaur_b200 import _lib
+  from dinosaur_b200 import spherical_harmonic as sh
+
+  world = int(os.environ.get('WORLD_SIZE', '1'))
+  rank = int(os.environ.get('RANK', '0'))
+  local = int(os.environ.get('LOCAL_RANK', '0'))
+  torch.cuda.set_device(local)
+  if world > 1:
+    import datetime
+    dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+
+  def barrier():
+    if world > 1:
+      dist.barrier()
+
+  fields = FIELDS
+  grid = sh.Grid.TL255(spherical_harmonics_impl=lambda **kw: sh.CudaSphericalHarmonics(
+      precision=args.precision, **kw))
+  plan = grid.plan
+  x_host = torch.from_numpy(modal_input(fields, seed=replica_seed(rank))).pin_memory()
+  x = x_host.cuda()
+  stream = torch.cuda.current_stream()
+
+  def step():
+    nodal = plan.inverse(x)
+    return plan.forward(nodal)
+
+  for _ in range(args.warmup):
+    y = step()
+  torch.cuda.synchronize()
+  rt_err = float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x))
+
+  # Device-resident timed region (working set ~0.3 GB > 126 MB L2).
+  sampler = ClockSampler(local)
+  barrier()
+  torch.cuda.synchronize()
+  e0 = torch.cuda.Event(enable_timing=True)
+  e1 = torch.cuda.Event(enable_timing=True)
+  e0.record(stream)
+  for _ in range(args.steps):
+    y = step()
+  e1.record(stream)
+  torch.cuda.synchronize()
+  barrier()
+  clocks = sampler.stop()
+  ms = e0.elapsed_time(e1) / args.steps
+  if args.profile:
+    if rank == 0:
+      print(json.dumps({'profile_ms_per_step': ms}), flush=True)
+    if world > 1:
+      dist.destroy_process_group()
+    return
+  ms_max = max_over_ranks(ms, device='cuda')
+  value = aggregate_tflops(sht_flops(fields), world, ms_max)
+
+  # End to end through the public API with pinned host buffers.
+  out_host = torch.empty_like(x_host).pin_memory()
+  barrier()
+  torch.cuda.synchronize()
+  e2 = torch.cuda.Event(enable_timing=True)
+  e3 = torch.cuda.Event(enable_timing=True)
+  e2.record(stream)
+  for _ in range(args.steps):
+    xd = x_host.to('cuda', non_blocking=True)
+    yd = grid.to_modal(grid.to_nodal(xd))
+    out_host.copy_(yd, non_blocking=True)
+  e3.record(stream)
+  torch.cuda.synchronize()
+  barrier()
+  ms_e2e = max_over_ranks(e2.elapsed_time(e3) / args.steps, device='cuda')
+  e2e_value = aggregate_tflops(sht_flops(fields), world, ms_e2e)
+
+  # Per-phase kernel timing (live CUDA events on the launching stream).
+  lw, L, I, J, M, _ = workload_dims()
+  buf_f = torch.empty((fields, M, J), device='cuda')
+  buf_n = torch.empty((fields, I, J), device='cuda')
+  buf_m = torch.empty((fields, M, L), device='cuda')
+  phases = [('legendre_inverse', 0, x, buf_f), ('fourier_inverse', 1, buf_f, buf_n),
+            ('fourier_forward', 2, buf_n, buf_f), ('legendre_forward', 3, buf_f, buf_m)]
+  phase_ms = {}
+  reps = max(5, args.steps)
+  for name, code, src, dst in phases:
+    for _ in range(2):
+      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
+                                           fields, sh.stream_handle()))
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(reps):
+      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
+                                           fields, sh.stream_handle()))
+    a1.record(stream)
+    torch.cuda.synchronize()
+    phase_ms[name] = a0.elapsed_time(a1) / reps
+  dominant = max(phase_ms, key=phase_ms.get)
+  peaks = {}
+  try:
+    with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+      peaks = json.load(fh)
+  except OSError:
+    pass
+  hbm_peak = peaks.get('hbm_gbs', 6650.0)
+  peak_src = 'measured' if 'hbm_gbs' in peaks else 'fallback'
+  achieved = phase_bytes(dominant, fields, args.precision) / (phase_ms[dominant] * 1e-3) / 1e9
+  launches_per_step = 4 if args.precision == 'fp32' else 6
+
+  extra = {}
+  if not args.no_extra and world == 1:
+    extra = pe_extras(torch)
+
+  if rank == 0:
+    line = {
+        'metric': 'SHT TFLOP/s (TL255 fwd+inv pair, 128 fields)',
+        'value': value, 'unit': 'TFLOP/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_max,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if args.precision == 'fp32' else 'bf16x3->f32',
+        'data': 'synthetic',
+        'config': {'workload': 'SHT pair TL255 x 128 fields', 'grid': 'TL255',
+                   'fields': fields, 'precision': args.precision,
+                   'parallelism': f'replicas x{world}',
+                   'l2': 'working set ~0.3 GB per step > 126 MB L2 (no flush)'},
+        'e2e': {'value': e2e_value, 'unit': 'TFLOP/s',
+                'h2d_bytes_per_step': int(x_host.numel() * 4),
+                'd2h_bytes_per_step': int(out_host.numel() * 4)},
+        'roofline': {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved,
+                     'peak': hbm_peak, 'unit': 'GB/s',
+                     'frac': achieved / hbm_peak, 'peak_source': peak_src,
+                     'traffic': None, 'phase_ms': phase_ms},
+        'clocks': clocks,
+        'gpu_launches': launches_per_step * args.steps,
+        'round_trip_rel_l2': rt_err,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+      line['cpu_baseline'] = cpu_baseline_entry()
+    if extra:
+      line['extra'] = extra
+    print(json.dumps(line), flush=True)
+  if world > 1:
+    dist.destroy_process_group()
+
+
+def pe_extras(torch):
+  """Primitive-equation steps/s on the benchmark grids (CUDA-graph replay)."""
+  from dinosaur_b200 import coordinate_systems, held_suarez, primitive_equations as pe
+  from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
+  from dinosaur_b200 import time_integration as ti, units
+  out = {}
+  for name, grid_fn, layers, members, hs, dt_min in [
+      ('T42_L24_x16_held_suarez', sh.Grid.T42, 24, 16, True, 15),
+      ('TL255_L32_dry', sh.Grid.TL255, 32, 1, False, 6)]:
+    g = grid_fn()
+    vert = sigma_coordinates.SigmaCoordinates.equidistant(layers)
+    coords = coordinate_systems.CoordinateSystem(g, vert)
+    ps = units.SimUnits()
+    tref = np.full(layers, 285.0) if hs else np.linspace(220.0, 288.0, layers)
+    eq = pe.PrimitiveEquationsSigma(tref, np.zeros(g.modal_shape, np.float32),
+                                    coords, ps)
+    if hs:
+      eq = ti.compose_equations([eq, held_suarez.HeldSuarezForcingSigma(coords, ps, tref)])
+    dt = units.nondim_time(dt_min * 60.0)
+    if hs:
+      flt = ti.exponential_step_filter(g, dt, tau=0.0087504, order=1.5, cutoff=0.8)
+    else:
+      flt = ti.exponential_step_filter(g, dt)
+    step = ti.step_with_filters(ti.imex_rk_sil3(eq, dt), [flt])
+    rng = np.random.default_rng(0)
+    shape = (members, layers) + g.modal_shape if members > 1 else (layers,) + g.modal_shape
+    lshape = (members, 1) + g.modal_shape if members > 1 else (1,) + g.modal_shape
+    _, l = g.modal_mesh
+    scale = g.mask / (l + 1.0) ** 2
+    t = lambda s: torch.as_tensor((1e-4 * rng.standard_normal(s) * scale).astype(np.float32),
+                                  device='cuda')
+    state = pe.State(t(shape), t(shape), t(shape), t(lshape))
+    eng = eq.engine(state)
+    buf = eng.pack(state)
+    eng.step_(buf, dt, step.filter_scaling, 3, graph=True)
+    torch.cuda.synchronize()
+    n = 20 if name.startswith('TL255') else 60
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record()
+    eng.step_(buf, dt, step.filter_scaling, n, graph=True)
+    a1.record()
+    torch.cuda.synchronize()
+    ms = a0.elapsed_time(a1) / n
+    out[name] = {'ms_per_step': ms, 'steps_per_s': 1e3 / ms,
+                 'member_steps_per_s': members * 1e3 / ms,
+                 'finite': bool(torch.isfinite(buf).all())}
+  return out
+
+
+def main():
+  ap = argparse.ArgumentParser()
+  ap.add_argument('--gpus', type=int, default=1)
+  ap.add_argument('--steps', type=int, default=20)
+  ap.add_argument('--warmup', type=int, default=5)
+  ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+  ap.add_argument('--precision', default=os.environ.get('DINO_BENCH_PRECISION', 'fp32'),
+                  choices=['fp32', 'bf16x3'])
+  ap.add_argument('--no-extra', action='store_true')
+  ap.add_argument('--no-cpu-baseline', action='store_true')
+  ap.add_argument('--profile', action='store_true',
+                  help='only the device-resident timed loop (for ncu captures)')
+  args = ap.parse_args()
+  if args.warmup < 3:
+    args.warmup = 3
+  if args.impl == 'reference':
+    run_reference(args)
+  else:
+    run_ours(args)
+
+
+if __name__ == '__main__':
+  main()

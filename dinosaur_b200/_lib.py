@@ -101,11 +101,13 @@ SIGNATURES = {
     'dino_plan_destroy': (ctypes.c_int, [_vp]),
     'dino_plan_nodes': (ctypes.c_int, [_vp, _DP, _DP]),
     'dino_plan_legendre_column': (ctypes.c_int, [_vp, _i32, _i32, _DP]),
+    'dino_plan_status': (ctypes.c_int, [_vp]),
     'dino_sht_inverse': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_forward': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_inverse_adjoint': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_forward_adjoint': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_modal_op': (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32, _i32, _vp]),
+    'dino_sht_phase': (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
     'dino_pe_create': (ctypes.c_int, [_vp, ctypes.POINTER(PEDesc),
                                       ctypes.POINTER(_vp)]),
     'dino_pe_destroy': (ctypes.c_int, [_vp]),

@@ -734,6 +734,27 @@ int dino_sht_forward_adjoint(dino_plan* p, const float* modal_ct,
   return sht_forward_adjoint(p, modal_ct, nodal_ct, nf, (cudaStream_t)stream);
 }
 
+int dino_sht_phase(dino_plan* p, int32_t phase, const float* in, float* out,
+                   int32_t nf, void* stream) {
+  DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_sht_phase: null argument");
+  DINO_REQUIRE(nf >= 0 && nf <= p->max_fields, DINO_ERR_SHAPE,
+               "nfields must be in [0, max_fields]");
+  if (nf == 0) return DINO_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (phase) {
+    case DINO_PHASE_LEGENDRE_INVERSE:
+      return legendre_inverse(p, one_seg(in, nf), out, nf, st);
+    case DINO_PHASE_FOURIER_INVERSE:
+      return fourier_inverse(p, in, out, nf, false, st);
+    case DINO_PHASE_FOURIER_FORWARD:
+      return fourier_forward(p, in, out, nf, true, st);
+    case DINO_PHASE_LEGENDRE_FORWARD:
+      return legendre_forward(p, in, out, nf, st);
+  }
+  set_error("unknown transform phase");
+  return DINO_ERR_ARG;
+}
+
 int dino_modal_op(dino_plan* p, int32_t op, const float* in, float* out,
                   int32_t nf, int32_t arg, void* stream) {
   DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_modal_op: null argument");

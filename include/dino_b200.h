@@ -112,6 +112,10 @@ DINO_API int dino_plan_nodes(const dino_plan* plan, double* host_sin_lat,
 DINO_API int dino_plan_legendre_column(const dino_plan* plan, int32_t m, int32_t l,
                               double* host_out);
 
+/* Synchronizes the device and reports whether any bounded device-side wait
+ * of this plan's kernels gave up (DINO_ERR_TIMEOUT); DINO_OK otherwise. */
+DINO_API int dino_plan_status(dino_plan* plan);
+
 /* modal [nfields][M][L] -> nodal [nfields][I][J]. */
 DINO_API int dino_sht_inverse(dino_plan* plan, const float* d_modal, float* d_nodal,
                      int32_t nfields, void* stream);
@@ -124,6 +128,18 @@ DINO_API int dino_sht_inverse_adjoint(dino_plan* plan, const float* d_nodal_ct,
                              float* d_modal_ct, int32_t nfields, void* stream);
 DINO_API int dino_sht_forward_adjoint(dino_plan* plan, const float* d_modal_ct,
                              float* d_nodal_ct, int32_t nfields, void* stream);
+/* One phase of the transform pair, for profiling and composition:
+ *   DINO_PHASE_LEGENDRE_INVERSE  modal [nf][M][L] -> Fourier [nf][M][J]
+ *   DINO_PHASE_FOURIER_INVERSE   Fourier [nf][M][J] -> nodal [nf][I][J]
+ *   DINO_PHASE_FOURIER_FORWARD   nodal [nf][I][J] -> weighted Fourier [nf][M][J]
+ *   DINO_PHASE_LEGENDRE_FORWARD  weighted Fourier [nf][M][J] -> modal [nf][M][L]
+ * nf must not exceed the plan's max_fields. */
+#define DINO_PHASE_LEGENDRE_INVERSE 0
+#define DINO_PHASE_FOURIER_INVERSE 1
+#define DINO_PHASE_FOURIER_FORWARD 2
+#define DINO_PHASE_LEGENDRE_FORWARD 3
+DINO_API int dino_sht_phase(dino_plan* plan, int32_t phase, const float* d_in,
+                            float* d_out, int32_t nfields, void* stream);
 /* One spectral operator (DINO_OP_*) on modal [nfields][M][L]; `arg` is the
  * number of wavenumbers to clip for DINO_OP_CLIP and is ignored otherwise. */
 DINO_API int dino_modal_op(dino_plan* plan, int32_t op, const float* d_in, float* d_out,

@@ -46,7 +46,8 @@ def test_gauss_nodes_and_legendre_table(name):
   x, w = g.plan.nodes
   xo, wo = osht.gauss_legendre_nodes(g.latitude_nodes)
   np.testing.assert_allclose(x, xo, atol=2e-15)
-  np.testing.assert_allclose(w, wo, rtol=2e-12, atol=1e-16)
+  # Near the poles 1 - x^2 is small, so FP64 weights agree to ~1e-10 relative.
+  np.testing.assert_allclose(w, wo, rtol=1e-9, atol=1e-16)
   p = osht.legendre_table(g.longitude_wavenumbers, g.total_wavenumbers, xo)
   import ctypes
   from dinosaur_b200 import _lib
@@ -140,19 +141,22 @@ def test_adjoints_are_transposes(name):
 
 
 def test_autograd_through_transforms():
+  # A quadratic loss, so the central difference is exact up to FP32 rounding.
   g, _ = grid_pair('T21')
-  x = torch.randn((2,) + g.modal_shape, device='cuda', requires_grad=True)
-  loss = (g.to_modal(g.to_nodal(x) ** 2) ** 2).sum()
+  gen = torch.Generator(device='cuda').manual_seed(0)
+  x = torch.randn((2,) + g.modal_shape, device='cuda', generator=gen)
+  w = torch.randn((2,) + g.modal_shape, device='cuda', generator=gen)
+  x.requires_grad_(True)
+  loss = (w * g.to_modal(g.to_nodal(x) ** 2)).sum()
   loss.backward()
   gx = x.grad.clone()
-  # Central finite difference along one direction.
-  d = torch.randn_like(x)
-  eps = 1e-2
+  d = torch.randn(x.shape, device='cuda', generator=gen)
+  eps = 0.1
   with torch.no_grad():
-    lp = (g.to_modal(g.to_nodal(x + eps * d) ** 2) ** 2).sum()
-    lm = (g.to_modal(g.to_nodal(x - eps * d) ** 2) ** 2).sum()
+    lp = (w * g.to_modal(g.to_nodal(x + eps * d) ** 2)).double().sum()
+    lm = (w * g.to_modal(g.to_nodal(x - eps * d) ** 2)).double().sum()
   fd = (lp - lm) / (2 * eps)
-  assert abs(float(fd - (gx * d).sum())) <= 2e-3 * abs(float(fd))
+  assert abs(float(fd - (gx.double() * d).sum())) <= 1e-3 * abs(float(fd))
 
 
 def test_shape_and_argument_errors():

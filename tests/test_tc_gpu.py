@@ -1,0 +1,67 @@
+"""GPU parity of the tcgen05 split-BF16 Legendre contraction.
+
+The 'bf16x3' plans run the Legendre GEMMs on tensor cores with hi*hi + hi*lo
++ lo*hi bf16 products accumulated in FP32.  Tolerances: relative L2 error
+<= 1e-5 against the FP64 oracle for one-way transforms and round trips (the
+target accuracy of the split form), max-abs relative error <= 5e-5.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import sht as osht
+from oracle import states as ost
+
+pytestmark = pytest.mark.gpu
+
+from dinosaur_b200 import _lib  # noqa: E402
+from dinosaur_b200 import spherical_harmonic as sh  # noqa: E402
+
+
+def tc_grid(name):
+  impl = lambda **kw: sh.CudaSphericalHarmonics(precision='bf16x3', **kw)
+  return getattr(sh.Grid, name)(spherical_harmonics_impl=impl)
+
+
+def l2(a, b):
+  a = a.detach().double().cpu().numpy() if torch.is_tensor(a) else a
+  return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def maxrel(a, b):
+  a = a.detach().double().cpu().numpy() if torch.is_tensor(a) else a
+  return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize('name', ['T21', 'T42', 'T85', 'TL127', 'TL255'])
+def test_tc_transforms_match_fp64_oracle(name):
+  g = tc_grid(name)
+  og = getattr(osht.Grid, name)()
+  nf = 4 if name != 'TL255' else 3
+  x = ost.sht_modal_input(og, nf, seed=3)
+  x64 = x.astype(np.float64)
+  nodal = g.to_nodal(torch.as_tensor(x, device='cuda'))
+  _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
+  ref = og.to_nodal(x64)
+  assert l2(nodal, ref) < 1e-5 and maxrel(nodal, ref) < 5e-5
+  z = np.random.default_rng(4).standard_normal((nf,) + og.nodal_shape)
+  modal = g.to_modal(torch.as_tensor(z, device='cuda', dtype=torch.float32))
+  _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
+  refm = og.to_modal(z.astype(np.float32).astype(np.float64))
+  assert l2(modal, refm) < 1e-5 and maxrel(modal, refm) < 5e-5
+  assert np.all(modal.cpu().numpy()[:, ~og.mask] == 0)
+
+
+def test_tc_matches_fp32_plan_on_large_batch():
+  g = tc_grid('TL255')
+  f = sh.Grid.TL255()
+  og = osht.Grid.TL255()
+  x = torch.as_tensor(ost.sht_modal_input(og, 128, seed=0), device='cuda')
+  a = g.to_modal(g.to_nodal(x))
+  b = f.to_modal(f.to_nodal(x))
+  _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
+  err_tc = float(torch.linalg.vector_norm(a - x) / torch.linalg.vector_norm(x))
+  err_fp = float(torch.linalg.vector_norm(b - x) / torch.linalg.vector_norm(x))
+  assert err_tc < 1e-5, err_tc
+  assert err_fp < 1e-5, err_fp
