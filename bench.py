@@ -77,24 +77,34 @@ class ClockSampler:
             'clocks_event_reasons.sw_power_cap')
 
   def __init__(self, device_index):
+    import tempfile
     self.proc = None
+    self.path = os.path.join(tempfile.gettempdir(), f'dino_clocks_{os.getpid()}.csv')
     try:
       self.proc = subprocess.Popen(
           ['nvidia-smi', f'--query-gpu={self.FIELDS}', '--format=csv,noheader,nounits',
-           '-lms', '100', '-i', str(device_index)],
-          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+           '-lms', '100', '-i', str(device_index), '-f', self.path],
+          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+      time.sleep(0.3)
     except (OSError, FileNotFoundError):
       self.proc = None
 
   def stop(self):
     if self.proc is None:
       return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+    time.sleep(0.2)
     self.proc.terminate()
     try:
-      out, _ = self.proc.communicate(timeout=5)
+      self.proc.wait(timeout=5)
     except subprocess.TimeoutExpired:
       self.proc.kill()
-      out, _ = self.proc.communicate()
+      self.proc.wait()
+    try:
+      with open(self.path) as fh:
+        out = fh.read()
+      os.remove(self.path)
+    except OSError:
+      out = ''
     sm, smax, reasons = [], None, set()
     names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
              'sw_power_cap']
@@ -338,7 +348,10 @@ def run_ours(args):
   hbm_peak = peaks.get('hbm_gbs', 6650.0)
   peak_src = 'measured' if 'hbm_gbs' in peaks else 'fallback'
   achieved = phase_bytes(dominant, fields, args.precision) / (phase_ms[dominant] * 1e-3) / 1e9
-  launches_per_step = 4 if args.precision == 'fp32' else 6
+  per_field = M * J * 4
+  cap = max(1, (48 << 20) // per_field)
+  chunks = -(-fields // min(cap, plan.max_fields))
+  launches_per_step = chunks * (4 if args.precision == 'fp32' else 6)
 
   extra = {}
   if not args.no_extra and world == 1:

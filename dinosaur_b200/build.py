@@ -64,7 +64,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
   newest_obj = max(os.path.getmtime(o) for o in objs)
   if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest_obj:
     tmp = LIB + '.tmp'
-    cmd = [nvcc(), *ARCH, '-shared', '-o', tmp, *objs]
+    cmd = [nvcc(), *ARCH, '-shared', '-Xlinker', '--no-undefined', '-o', tmp, *objs]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
       raise RuntimeError(f'link failed:\n{proc.stderr}')

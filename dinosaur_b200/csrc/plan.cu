@@ -73,7 +73,19 @@ __global__ void gauss_nodes_kernel(int J, double* __restrict__ x,
     dp = J * (xr * p1 - p0) / (xr * xr - 1.0);
     double dx = p1 / dp;
     xr -= dx;
-    if (fabs(dx) <= 1e-17) break;
+    // Quadratic convergence: once the update is below 1e-15 one more step
+    // reaches round-off (a tighter absolute test may never be met).
+    if (fabs(dx) < 1e-15) {
+      p0 = 1.0;
+      p1 = xr;
+      for (int n = 2; n <= J; ++n) {
+        double p2 = ((2.0 * n - 1.0) * xr * p1 - (n - 1.0) * p0) / n;
+        p0 = p1;
+        p1 = p2;
+      }
+      xr -= p1 / (J * (xr * p1 - p0) / (xr * xr - 1.0));
+      break;
+    }
   }
   {
     // Final derivative at the converged root for the weight.

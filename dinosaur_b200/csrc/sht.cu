@@ -39,6 +39,11 @@ __device__ __forceinline__ void row_map(int m, int r, int& b, int& row) {
   }
 }
 
+// Each thread stages 4 rows x 4 contraction indices of a 128 x 16 operand
+// chunk: rows (tid / 4) + 32 i, indices 4 (tid % 4) .. + 3.  Row pointers are
+// resolved once per CTA; the next chunk is prefetched into registers while
+// the current one is consumed from shared memory.
+
 // out_fourier[b][row][j] for all j from modal rows (inverse contraction).
 __global__ void __launch_bounds__(kLegThreads)
 legendre_inverse_simt(Segs in, float* __restrict__ out, int B, int M, int L,
@@ -58,6 +63,43 @@ legendre_inverse_simt(Segs in, float* __restrict__ out, int B, int M, int L,
   const int tid = threadIdx.x;
   const int tx = tid & 7;   // 8 groups of 4 latitudes
   const int ty = tid >> 3;  // 16 groups of 8 rows
+  const int lq = tid & 3;   // load quarter (4 contraction indices)
+  const float* xrow[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = r0 + (tid >> 2) + 32 * i;
+    xrow[i] = nullptr;
+    if (r < rows) {
+      int b, row;
+      row_map(m, r, b, row);
+      xrow[i] = seg_field(in, b, (size_t)M * L) + (size_t)row * L + m;
+    }
+  }
+  const int pk = tid >> 3, pj = (tid & 7) * 4;  // P chunk: 16 x 32 as float4
+  float xv[4][4];
+  float4 pv;
+  auto fetch = [&](int kc) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int k = kc + lq * 4 + e;
+        xv[i][e] = (xrow[i] && k < Lm) ? xrow[i][k] : 0.f;
+      }
+    const int k = kc + pk;
+    const int j = j0 + pj;
+    // Vector load only when the row start is 16-byte aligned (Jh % 4 == 0;
+    // the per-m table offsets are multiples of Jh).
+    if ((Jh & 3) == 0 && k < Lm && j + 3 < Jh) {
+      pv = *reinterpret_cast<const float4*>(P + (size_t)k * Jh + j);
+    } else {
+      float t[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        t[e] = (k < Lm && j + e < Jh) ? P[(size_t)k * Jh + j + e] : 0.f;
+      pv = make_float4(t[0], t[1], t[2], t[3]);
+    }
+  };
 
   float accE[8][4], accO[8][4];
 #pragma unroll
@@ -65,47 +107,37 @@ legendre_inverse_simt(Segs in, float* __restrict__ out, int B, int M, int L,
 #pragma unroll
     for (int t = 0; t < 4; ++t) accE[i][t] = accO[i][t] = 0.f;
 
+  fetch(0);
   for (int kc = 0; kc < Lm; kc += kLegKC) {
-    // Stage X chunk: rows r0.., l = m + kc + kk (contiguous in global).
-    for (int idx = tid; idx < kLegTB * kLegKC; idx += kLegThreads) {
-      int kk = idx % kLegKC, rl = idx / kLegKC;
-      int r = r0 + rl, k = kc + kk;
-      float v = 0.f;
-      if (r < rows && k < Lm) {
-        int b, row;
-        row_map(m, r, b, row);
-        v = seg_field(in, b, (size_t)M * L)[(size_t)row * L + m + k];
-      }
-      Xs[kk][rl] = v;
-    }
-    for (int idx = tid; idx < kLegKC * kLegTN; idx += kLegThreads) {
-      int jj = idx % kLegTN, kk = idx / kLegTN;
-      int j = j0 + jj, k = kc + kk;
-      Ps[kk][jj] = (j < Jh && k < Lm) ? P[(size_t)k * Jh + j] : 0.f;
-    }
     __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) Xs[lq * 4 + e][(tid >> 2) + 32 * i] = xv[i][e];
+    *reinterpret_cast<float4*>(&Ps[pk][pj]) = pv;
+    __syncthreads();
+    if (kc + kLegKC < Lm) fetch(kc + kLegKC);
 #pragma unroll
     for (int kk = 0; kk < kLegKC; kk += 2) {
       float4 xa = *reinterpret_cast<const float4*>(&Xs[kk][ty * 8]);
       float4 xb = *reinterpret_cast<const float4*>(&Xs[kk][ty * 8 + 4]);
       float4 pp = *reinterpret_cast<const float4*>(&Ps[kk][tx * 4]);
-      float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-      float pv[4] = {pp.x, pp.y, pp.z, pp.w};
+      float xe[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+      float pe[4] = {pp.x, pp.y, pp.z, pp.w};
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int t = 0; t < 4; ++t) accE[i][t] = fmaf(xv[i], pv[t], accE[i][t]);
+        for (int t = 0; t < 4; ++t) accE[i][t] = fmaf(xe[i], pe[t], accE[i][t]);
       xa = *reinterpret_cast<const float4*>(&Xs[kk + 1][ty * 8]);
       xb = *reinterpret_cast<const float4*>(&Xs[kk + 1][ty * 8 + 4]);
       pp = *reinterpret_cast<const float4*>(&Ps[kk + 1][tx * 4]);
-      float xw[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-      float pw[4] = {pp.x, pp.y, pp.z, pp.w};
+      float xo[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+      float po[4] = {pp.x, pp.y, pp.z, pp.w};
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int t = 0; t < 4; ++t) accO[i][t] = fmaf(xw[i], pw[t], accO[i][t]);
+        for (int t = 0; t < 4; ++t) accO[i][t] = fmaf(xo[i], po[t], accO[i][t]);
     }
-    __syncthreads();
   }
 
 #pragma unroll
@@ -162,56 +194,83 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
   __shared__ __align__(16) float Ds[kLegKC][kLegTB + 4];
   __shared__ float Ps[kLegKC][kLegTN + 1];
 
+  const int lq = tid & 3;
+  const float* grow[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = r0 + (tid >> 2) + 32 * i;
+    grow[i] = nullptr;
+    if (r < rows) {
+      int b, row;
+      row_map(m, r, b, row);
+      grow[i] = G + ((size_t)b * M + row) * J;
+    }
+  }
+  // P chunk 32 (l) x 16 (j): thread loads l = tid / 4, j = 4 (tid % 4) .. +3.
+  const int pl_ = tid >> 2, pjq = (tid & 3) * 4;
+  float sv[4][4], dv[4][4], pvr[4];
+  auto fetch = [&](int jc) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int j = jc + lq * 4 + e;
+        float g1 = 0.f, g2 = 0.f;
+        if (grow[i] && j < Jh) {
+          g1 = grow[i][j];
+          const int jm = J - 1 - j;
+          g2 = (jm != j) ? grow[i][jm] : 0.f;
+        }
+        sv[i][e] = g1 + g2;
+        dv[i][e] = g1 - g2;
+      }
+    const int k = k0 + pl_;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int j = jc + pjq + e;
+      pvr[e] = (k < Lm && j < Jh) ? P[(size_t)k * Jh + j] : 0.f;
+    }
+  };
+
   float acc[8][4];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int t = 0; t < 4; ++t) acc[i][t] = 0.f;
 
+  fetch(0);
   for (int jc = 0; jc < Jh; jc += kLegKC) {
-    for (int idx = tid; idx < kLegTB * kLegKC; idx += kLegThreads) {
-      int jj = idx % kLegKC, rl = idx / kLegKC;
-      int r = r0 + rl, j = jc + jj;
-      float s = 0.f, d = 0.f;
-      if (r < rows && j < Jh) {
-        int b, row;
-        row_map(m, r, b, row);
-        const float* g = G + ((size_t)b * M + row) * J;
-        float g1 = g[j];
-        int jm = J - 1 - j;
-        float g2 = (jm != j) ? g[jm] : 0.f;
-        s = g1 + g2;
-        d = g1 - g2;
-      }
-      Ss[jj][rl] = s;
-      Ds[jj][rl] = d;
-    }
-    for (int idx = tid; idx < kLegKC * kLegTN; idx += kLegThreads) {
-      int jj = idx % kLegKC, kk = idx / kLegKC;
-      int j = jc + jj, k = k0 + kk;
-      Ps[jj][kk] = (j < Jh && k < Lm) ? P[(size_t)k * Jh + j] : 0.f;
-    }
     __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        Ss[lq * 4 + e][(tid >> 2) + 32 * i] = sv[i][e];
+        Ds[lq * 4 + e][(tid >> 2) + 32 * i] = dv[i][e];
+      }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) Ps[pjq + e][pl_] = pvr[e];
+    __syncthreads();
+    if (jc + kLegKC < Jh) fetch(jc + kLegKC);
 #pragma unroll
     for (int jj = 0; jj < kLegKC; ++jj) {
       float4 sa = *reinterpret_cast<const float4*>(&Ss[jj][ty * 8]);
       float4 sb = *reinterpret_cast<const float4*>(&Ss[jj][ty * 8 + 4]);
       float4 da = *reinterpret_cast<const float4*>(&Ds[jj][ty * 8]);
       float4 db = *reinterpret_cast<const float4*>(&Ds[jj][ty * 8 + 4]);
-      float sv[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
-      float dv[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
-      float pv[4];
+      float s8[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
+      float d8[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+      float pw[4];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) pv[t] = Ps[jj][tx * 4 + t];
+      for (int t = 0; t < 4; ++t) pw[t] = Ps[jj][tx * 4 + t];
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        acc[i][0] = fmaf(sv[i], pv[0], acc[i][0]);
-        acc[i][1] = fmaf(dv[i], pv[1], acc[i][1]);
-        acc[i][2] = fmaf(sv[i], pv[2], acc[i][2]);
-        acc[i][3] = fmaf(dv[i], pv[3], acc[i][3]);
+        acc[i][0] = fmaf(s8[i], pw[0], acc[i][0]);
+        acc[i][1] = fmaf(d8[i], pw[1], acc[i][1]);
+        acc[i][2] = fmaf(s8[i], pw[2], acc[i][2]);
+        acc[i][3] = fmaf(d8[i], pw[3], acc[i][3]);
       }
     }
-    __syncthreads();
   }
 
 #pragma unroll
@@ -273,74 +332,130 @@ __device__ __forceinline__ float2 cmul_i(float2 a) {
   return kSign > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
-// Stockham passes over N points for kFftJS columns; data[n * JS + c].
-// kSign = +1: sum_k Z[k] e^{+2 pi i k n / N}; -1: e^{-...}.  Returns the
-// buffer holding the result.
-template <int N, int kSign>
-__device__ float2* stockham(float2* a, float2* b, const float2* twn) {
-  const int tid = threadIdx.x;
-#pragma unroll 1
-  for (int Ns = 1; Ns < N; ) {
-    if (Ns * 4 <= N) {
-      const int quarter = N / 4;
-      const int stride = N / (Ns * 4);
-      for (int item = tid; item < quarter * kFftJS; item += kFftThreads) {
-        int c = item % kFftJS, j = item / kFftJS;
-        int k = j % Ns;
-        float2 v0 = a[(j) * kFftJS + c];
-        float2 v1 = a[(j + quarter) * kFftJS + c];
-        float2 v2 = a[(j + 2 * quarter) * kFftJS + c];
-        float2 v3 = a[(j + 3 * quarter) * kFftJS + c];
-        if (k) {
-          float2 w1 = twn[k * stride], w2 = twn[2 * k * stride],
-                 w3 = twn[3 * k * stride];
-          if (kSign < 0) {
-            w1 = cconj(w1);
-            w2 = cconj(w2);
-            w3 = cconj(w3);
-          }
-          v1 = cmul(v1, w1);
-          v2 = cmul(v2, w2);
-          v3 = cmul(v3, w3);
-        }
-        float2 s02 = cadd(v0, v2), d02 = csub(v0, v2);
-        float2 s13 = cadd(v1, v3), d13 = cmul_i<kSign>(csub(v1, v3));
-        int dst = (j / Ns) * Ns * 4 + k;
-        b[(dst) * kFftJS + c] = cadd(s02, s13);
-        b[(dst + Ns) * kFftJS + c] = cadd(d02, d13);
-        b[(dst + 2 * Ns) * kFftJS + c] = csub(s02, s13);
-        b[(dst + 3 * Ns) * kFftJS + c] = csub(d02, d13);
-      }
-      Ns *= 4;
-    } else {
-      const int half = N / 2;
-      const int stride = N / (Ns * 2);
-      for (int item = tid; item < half * kFftJS; item += kFftThreads) {
-        int c = item % kFftJS, j = item / kFftJS;
-        int k = j % Ns;
-        float2 v0 = a[j * kFftJS + c];
-        float2 v1 = a[(j + half) * kFftJS + c];
-        if (k) {
-          float2 w = twn[k * stride];
-          if (kSign < 0) w = cconj(w);
-          v1 = cmul(v1, w);
-        }
-        int dst = (j / Ns) * Ns * 2 + k;
-        b[dst * kFftJS + c] = cadd(v0, v1);
-        b[(dst + Ns) * kFftJS + c] = csub(v0, v1);
-      }
-      Ns *= 2;
-    }
-    __syncthreads();
-    float2* t = a;
-    a = b;
-    b = t;
+// exp(2 pi i k / 16), k = 0..7 (the 16th roots of unity used by the
+// register DFTs; cos/sin of multiples of pi/8).
+__device__ __forceinline__ float2 root16(int k) {
+  constexpr float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f;
+  constexpr float h = 0.70710678118654757f;
+  switch (k & 7) {
+    case 0: return make_float2(1.f, 0.f);
+    case 1: return make_float2(c1, s1);
+    case 2: return make_float2(h, h);
+    case 3: return make_float2(s1, c1);
+    case 4: return make_float2(0.f, 1.f);
+    case 5: return make_float2(-s1, c1);
+    case 6: return make_float2(-h, h);
+    default: return make_float2(-c1, s1);
   }
-  return a;
+}
+
+// In-register DFT of length R (power of two <= 16), natural order in and
+// out: v_s <- sum_q v_q exp(kSign 2 pi i q s / R).
+template <int R, int kSign>
+__device__ __forceinline__ void dft_reg(float2* v) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else {
+    constexpr int H = R / 2;
+    float2 e[H], o[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    dft_reg<H, kSign>(e);
+    dft_reg<H, kSign>(o);
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      float2 w = root16(k * (16 / R));
+      if (kSign < 0) w = cconj(w);
+      float2 t = (k == 0) ? o[k] : cmul(o[k], w);
+      v[k] = cadd(e[k], t);
+      v[k + H] = csub(e[k], t);
+    }
+  }
+}
+
+// One radix-R Stockham pass over N points for kFftJS columns.  load(n, c)
+// returns element n of column c; store(n, c, v) writes output element n.
+template <int N, int R, int kSign, class Load, class Store>
+__device__ __forceinline__ void stockham_pass(int Ns, const float2* twn,
+                                              Load load, Store store) {
+  constexpr int Q = N / R;
+  const int stride = N / (Ns * R);
+  for (int item = threadIdx.x; item < Q * kFftJS; item += kFftThreads) {
+    const int c = item % kFftJS, j = item / kFftJS;
+    const int k = j % Ns;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = load(j + r * Q, c);
+    if (k) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = twn[r * k * stride];
+        if (kSign < 0) w = cconj(w);
+        v[r] = cmul(v[r], w);
+      }
+    }
+    dft_reg<R, kSign>(v);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) store(base + r * Ns, c, v[r]);
+  }
+}
+
+// Radix schedule (at most three passes) for each supported N; the kernels
+// use one N x kFftJS shared buffer per pass.
+template <int N> struct FftRadix;
+template <> struct FftRadix<8> { static constexpr int r1 = 8, r2 = 1, r3 = 1; };
+template <> struct FftRadix<16> { static constexpr int r1 = 16, r2 = 1, r3 = 1; };
+template <> struct FftRadix<32> { static constexpr int r1 = 8, r2 = 4, r3 = 1; };
+template <> struct FftRadix<64> { static constexpr int r1 = 8, r2 = 8, r3 = 1; };
+template <> struct FftRadix<128> { static constexpr int r1 = 16, r2 = 8, r3 = 1; };
+template <> struct FftRadix<256> { static constexpr int r1 = 16, r2 = 16, r3 = 1; };
+template <> struct FftRadix<512> { static constexpr int r1 = 8, r2 = 8, r3 = 8; };
+
+template <int N>
+constexpr int fft_buffers() {
+  return 1 + (FftRadix<N>::r2 > 1) + (FftRadix<N>::r3 > 1);
+}
+
+// Runs all passes: first pass reads via `first`, last pass writes via `last`,
+// intermediate passes ping-pong between the shared buffers a and b.
+template <int N, int kSign, class First, class Last>
+__device__ __forceinline__ void fft_passes(float2* a, float2* b,
+                                           const float2* twn, First first,
+                                           Last last) {
+  using Rd = FftRadix<N>;
+  auto smem_load = [](float2* buf) {
+    return [buf](int n, int c) { return buf[n * kFftJS + c]; };
+  };
+  auto smem_store = [](float2* buf) {
+    return [buf](int n, int c, float2 v) { buf[n * kFftJS + c] = v; };
+  };
+  if constexpr (Rd::r2 == 1) {
+    stockham_pass<N, Rd::r1, kSign>(1, twn, first, last);
+  } else if constexpr (Rd::r3 == 1) {
+    stockham_pass<N, Rd::r1, kSign>(1, twn, first, smem_store(a));
+    __syncthreads();
+    stockham_pass<N, Rd::r2, kSign>(Rd::r1, twn, smem_load(a), last);
+  } else {
+    stockham_pass<N, Rd::r1, kSign>(1, twn, first, smem_store(a));
+    __syncthreads();
+    stockham_pass<N, Rd::r2, kSign>(Rd::r1, twn, smem_load(a), smem_store(b));
+    __syncthreads();
+    stockham_pass<N, Rd::r3, kSign>(Rd::r1 * Rd::r2, twn, smem_load(b), last);
+  }
 }
 
 // Fourier coefficients F[b][row][j] -> nodal[b][i][j] (optionally scaled by
 // wq[j], which gives the adjoint of the weighted forward transform).
+// Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]) is formed from
+// global loads, then z = IDFT_N(Z) and x[2n] = Re z[n], x[2n+1] = Im z[n].
 template <int N>
 __global__ void __launch_bounds__(kFftThreads)
 rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
@@ -348,9 +463,11 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
                     const float2* __restrict__ tw_i,
                     const float* __restrict__ wq) {
   extern __shared__ float2 sm[];
-  float2* A = sm;
+  constexpr int kBufs = fft_buffers<N>();
+  float2* Zs = sm;
+  float2* A = Zs + N * kFftJS;
   float2* Bf = A + N * kFftJS;
-  float2* twn = Bf + N * kFftJS;
+  float2* twn = Zs + kBufs * N * kFftJS;
   float2* twi = twn + N;
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
@@ -360,44 +477,41 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
     twn[t] = tw_n[t];
     twi[t] = tw_i[t];
   }
-  // X[k]: half-weighted positive-frequency spectrum (X[0] full weight).
+  __syncthreads();
   const float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
   const float half_inv_sqrt_pi = 0.28209479177387814f;
-  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
-    int k = idx / kFftJS, c = idx % kFftJS;
-    float2 v = make_float2(0.f, 0.f);
-    if (c < ncol && k < lw) {
-      if (k == 0) {
-        v.x = Fb[c] * inv_sqrt_2pi;
-      } else {
-        v.x = Fb[(size_t)(2 * k - 1) * J + c] * half_inv_sqrt_pi;
-        v.y = -Fb[(size_t)(2 * k) * J + c] * half_inv_sqrt_pi;
-      }
+  auto X = [&](int k, int c) -> float2 {
+    if (c >= ncol || k >= lw || k >= N) return make_float2(0.f, 0.f);
+    if (k == 0) return make_float2(Fb[c] * inv_sqrt_2pi, 0.f);
+    return make_float2(Fb[(size_t)(2 * k - 1) * J + c] * half_inv_sqrt_pi,
+                       -Fb[(size_t)(2 * k) * J + c] * half_inv_sqrt_pi);
+  };
+  // Pairs (k, N - k), k = 0..N/2; k = 0 pairs with the (zero) Nyquist term.
+  for (int item = tid; item < (N / 2 + 1) * kFftJS; item += kFftThreads) {
+    const int k = item / kFftJS, c = item % kFftJS;
+    const float2 xk = X(k, c);
+    const float2 xn = (k == 0) ? make_float2(0.f, 0.f) : X(N - k, c);
+    const float2 xnc = cconj(xn), xkc = cconj(xk);
+    Zs[k * kFftJS + c] =
+        cadd(cadd(xk, xnc), cmul_i<1>(cmul(twi[k], csub(xk, xnc))));
+    if (k > 0 && k < N / 2 + (N & 1)) {
+      const int kn = N - k;
+      Zs[kn * kFftJS + c] =
+          cadd(cadd(xn, xkc), cmul_i<1>(cmul(twi[kn], csub(xn, xkc))));
     }
-    Bf[idx] = v;
   }
   __syncthreads();
-  // Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]), X[N] = 0.
-  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
-    int k = idx / kFftJS, c = idx % kFftJS;
-    float2 xk = Bf[idx];
-    float2 xc = (k == 0) ? make_float2(0.f, 0.f) : cconj(Bf[(N - k) * kFftJS + c]);
-    float2 s = cadd(xk, xc);
-    float2 d = cmul_i<1>(cmul(twi[k], csub(xk, xc)));
-    A[idx] = cadd(s, d);
-  }
-  __syncthreads();
-  float2* z = stockham<N, 1>(A, Bf, twn);
   float* ob = out + (size_t)b * (2 * N) * J + j0;
-  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
-    int n = idx / kFftJS, c = idx % kFftJS;
-    if (c >= ncol) continue;
-    float2 v = z[idx];
-    float s = wq ? wq[j0 + c] : 1.f;
-    ob[(size_t)(2 * n) * J + c] = v.x * s;
-    ob[(size_t)(2 * n + 1) * J + c] = v.y * s;
-  }
+  auto first = [Zs](int n, int c) { return Zs[n * kFftJS + c]; };
+  auto last = [ob, ncol, J, wq, j0](int n, int c, float2 v) {
+    if (c < ncol) {
+      const float s = wq ? wq[j0 + c] : 1.f;
+      ob[(size_t)(2 * n) * J + c] = v.x * s;
+      ob[(size_t)(2 * n + 1) * J + c] = v.y * s;
+    }
+  };
+  fft_passes<N, 1>(A, Bf, twn, first, last);
 }
 
 // nodal[b][i][j] -> F[b][row][j] (times wq[j] when given: the forward SHT's
@@ -409,9 +523,11 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
                     const float2* __restrict__ tw_i,
                     const float* __restrict__ wq) {
   extern __shared__ float2 sm[];
-  float2* A = sm;
+  constexpr int kBufs = fft_buffers<N>();
+  float2* Zs = sm;
+  float2* A = Zs + N * kFftJS;
   float2* Bf = A + N * kFftJS;
-  float2* twn = Bf + N * kFftJS;
+  float2* twn = Zs + kBufs * N * kFftJS;
   float2* twi = twn + N;
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
@@ -421,26 +537,23 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
     twn[t] = tw_n[t];
     twi[t] = tw_i[t];
   }
-  const float* xb = x + (size_t)b * (2 * N) * J + j0;
-  for (int idx = tid; idx < N * kFftJS; idx += kFftThreads) {
-    int n = idx / kFftJS, c = idx % kFftJS;
-    float2 v = make_float2(0.f, 0.f);
-    if (c < ncol) {
-      v.x = xb[(size_t)(2 * n) * J + c];
-      v.y = xb[(size_t)(2 * n + 1) * J + c];
-    }
-    A[idx] = v;
-  }
   __syncthreads();
-  float2* Z = stockham<N, -1>(A, Bf, twn);
+  const float* xb = x + (size_t)b * (2 * N) * J + j0;
+  auto first = [xb, ncol, J](int n, int c) {
+    if (c >= ncol) return make_float2(0.f, 0.f);
+    return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
+  };
+  auto last = [Zs](int n, int c, float2 v) { Zs[n * kFftJS + c] = v; };
+  fft_passes<N, -1>(A, Bf, twn, first, last);
+  __syncthreads();
   float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
   const float inv_sqrt_pi = 0.5641895835477563f;
   for (int idx = tid; idx < lw * kFftJS; idx += kFftThreads) {
     int k = idx / kFftJS, c = idx % kFftJS;
     if (c >= ncol) continue;
-    float2 zk = Z[(k % N) * kFftJS + c];
-    float2 zc = cconj(Z[((N - k) % N) * kFftJS + c]);
+    float2 zk = Zs[(k % N) * kFftJS + c];
+    float2 zc = cconj(Zs[((N - k) % N) * kFftJS + c]);
     float2 s = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
     float2 d = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
     // X[k] = s + e^{-2 pi i k / I} * (-i d)
@@ -493,7 +606,7 @@ static int configure_rfft() {
   // Kernel attributes are set once per process, outside any stream capture.
   static bool configured = false;
   if (configured) return DINO_OK;
-  const int smem = (int)(sizeof(float2) * (2 * (size_t)N * kFftJS + 2 * N));
+  const int smem = (int)(sizeof(float2) * (fft_buffers<N>() * (size_t)N * kFftJS + 2 * N));
   DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_inverse_kernel<N>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_forward_kernel<N>,
@@ -505,7 +618,7 @@ static int configure_rfft() {
 template <int N>
 static int launch_rfft(dino_plan* p, const float* in, float* out, int nf,
                        bool inverse, const float* wq, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * (2 * (size_t)N * kFftJS + 2 * N);
+  const size_t smem = sizeof(float2) * (fft_buffers<N>() * (size_t)N * kFftJS + 2 * N);
   if (!p) return configure_rfft<N>();
   DINO_TRY(configure_rfft<N>());
   dim3 grid(ceil_div(p->J, kFftJS), nf);
@@ -569,11 +682,24 @@ int fourier_forward(dino_plan* p, const float* nodal, float* F, int nf,
 // Transform drivers (chunked by workspace capacity)
 // ---------------------------------------------------------------------------
 
+// Fields per launch such that the intermediate Fourier coefficients of one
+// chunk (fields x M x J floats) stay resident in L2 between the Legendre and
+// FFT kernels; chunks are balanced.
+static int l2_chunk(dino_plan* p, int nf, int work_fields) {
+  const size_t per_field = (size_t)p->M * p->J * sizeof(float);
+  int cap = (int)((48ull << 20) / (per_field ? per_field : 1));
+  if (cap < 1) cap = 1;
+  if (cap > work_fields) cap = work_fields;
+  const int chunks = (nf + cap - 1) / cap;
+  return (nf + chunks - 1) / chunks;
+}
+
 int sht_inverse_segs(dino_plan* p, const Segs& in, float* out, int nf,
                      float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
-  for (int f0 = 0; f0 < nf; f0 += work_fields) {
-    int n = nf - f0 < work_fields ? nf - f0 : work_fields;
+  const int chunk = l2_chunk(p, nf, work_fields);
+  for (int f0 = 0; f0 < nf; f0 += chunk) {
+    int n = nf - f0 < chunk ? nf - f0 : chunk;
     Segs sub = seg_offset(in, f0, n, ms);
     DINO_TRY(legendre_inverse(p, sub, work, n, st));
     DINO_TRY(fourier_inverse(p, work, out + f0 * ns, n, false, st));
@@ -584,8 +710,9 @@ int sht_inverse_segs(dino_plan* p, const Segs& in, float* out, int nf,
 int sht_forward_to(dino_plan* p, const float* nodal, float* out, int nf,
                    float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
-  for (int f0 = 0; f0 < nf; f0 += work_fields) {
-    int n = nf - f0 < work_fields ? nf - f0 : work_fields;
+  const int chunk = l2_chunk(p, nf, work_fields);
+  for (int f0 = 0; f0 < nf; f0 += chunk) {
+    int n = nf - f0 < chunk ? nf - f0 : chunk;
     DINO_TRY(fourier_forward(p, nodal + f0 * ns, work, n, true, st));
     DINO_TRY(legendre_forward(p, work, out + f0 * ms, n, st));
   }
