@@ -103,6 +103,7 @@ SIGNATURES = {
     'dino_plan_legendre_column': (ctypes.c_int, [_vp, _i32, _i32, _DP]),
     'dino_plan_status': (ctypes.c_int, [_vp]),
     'dino_sht_inverse': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
+    'dino_sht_inverse_noalloc': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_forward': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_inverse_adjoint': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_forward_adjoint': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),

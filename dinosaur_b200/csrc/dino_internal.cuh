@@ -134,6 +134,9 @@ int modal_op(dino_plan* p, int op, const float* in, float* out, int nfields,
              int arg, cudaStream_t st);
 // Sets kernel attributes ahead of stream capture.
 int sht_prepare(dino_plan* p);
+// FP32 SIMT inverse Legendre contraction for any plan (no precision dispatch).
+int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
+                          cudaStream_t st);
 
 // legendre_tc.cu
 int tc_tables_build(dino_plan* p);

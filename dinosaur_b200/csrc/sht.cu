@@ -288,6 +288,15 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
   }
 }
 
+// The FP32 SIMT inverse contraction regardless of the plan's precision.
+int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
+                          cudaStream_t st) {
+  dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
+  legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
+      in, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
+  return check_launch("legendre_inverse_simt");
+}
+
 int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
                      cudaStream_t st) {
   if (p->precision == DINO_PREC_BF16X3)

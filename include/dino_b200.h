@@ -116,6 +116,26 @@ DINO_API int dino_plan_legendre_column(const dino_plan* plan, int32_t m, int32_t
  * of this plan's kernels gave up (DINO_ERR_TIMEOUT); DINO_OK otherwise. */
 DINO_API int dino_plan_status(dino_plan* plan);
 
+/* Allocation-free inverse transform (no counterpart in the reference).
+ * Same result as dino_sht_inverse on an FP32 plan, but the intermediate
+ * Fourier coefficients live in a fixed array of DINO_NOALLOC_SCRATCH_FLOATS
+ * floats (16 MiB) inside the library, held on every GPU that loads it, instead
+ * of the plan's workspace; the call performs no device allocation or free.
+ * It is meant for callers that may not allocate device memory at call time,
+ * for example a handler inside a framework that owns the GPU's memory pool,
+ * or a loop that cannot afford cudaMalloc's implicit device synchronization.
+ * The plan must already exist (its tables are read, not written).  Limits and
+ * rules: nfields * M * J <= DINO_NOALLOC_SCRATCH_FLOATS, otherwise
+ * DINO_ERR_SHAPE; the Legendre contraction always runs in FP32; the first
+ * call on a device looks the array up (cudaGetSymbolAddress) and sets kernel
+ * attributes, so make that first call before any stream capture; all calls on
+ * a device share the one array, so calls that overlap on the GPU (different
+ * streams or threads) race and must be serialised by the caller. */
+#define DINO_NOALLOC_SCRATCH_FLOATS (4 * 1024 * 1024)
+DINO_API int dino_sht_inverse_noalloc(dino_plan* plan, const float* d_modal,
+                                      float* d_nodal, int32_t nfields,
+                                      void* stream);
+
 /* modal [nfields][M][L] -> nodal [nfields][I][J]. */
 DINO_API int dino_sht_inverse(dino_plan* plan, const float* d_modal, float* d_nodal,
                      int32_t nfields, void* stream);
