@@ -416,14 +416,16 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
   if (ok) {
-    const int r = warp * 32 + lane;
-    const int rr = tile * 128 + r;
-    const bool valid = rr < rows;
-    int b = 0, row = 0;
-    if (valid) tc_row_map(m, rr, b, row);
+    // Epilogue.  Each warp owns TMEM lanes (rows) 32w .. 32w+31; a thread
+    // reads its row's accumulator columns, the warp stages a 32-row block in
+    // shared memory (the drained pipeline buffers) and writes it back with
+    // row-contiguous, coalesced stores.
+    constexpr int kStride = 36;  // floats per staged row (16-byte multiple)
+    float* stage = reinterpret_cast<float*>(base) + warp * 32 * kStride;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const int row0 = tile * 128 + warp * 32;  // first row of this warp
     if (!kForward) {
-      float* o = a.out + ((size_t)b * a.M + row) * a.J;
+      const bool vec = (a.J & 3) == 0;
       for (int c = 0; c < a.Nrows / 16; ++c) {
         float e[16], od[16];
         tmem_ld16(lane_base + c * 16, e);
@@ -433,22 +435,59 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
 #pragma unroll
           for (int t = 0; t < 16; ++t) od[t] = 0.f;
         }
-        if (valid) {
+        // stage[r][t] = E + O at j = 16c + t; stage[r][16 + t] = E - O at
+        // j = J - 16(c+1) + t (the mirrored block, ascending).
 #pragma unroll
-          for (int t = 0; t < 16; ++t) {
-            const int j = c * 16 + t;
-            if (j < a.Jh) {
-              o[j] = e[t] + od[t];
-              const int jm = a.J - 1 - j;
-              if (jm != j) o[jm] = e[t] - od[t];
+        for (int t = 0; t < 16; ++t) {
+          stage[lane * kStride + t] = e[t] + od[t];
+          stage[lane * kStride + 16 + (15 - t)] = e[t] - od[t];
+        }
+        __syncwarp();
+        const int jb = 16 * c;
+        const int jm = a.J - 16 * (c + 1);
+        // 4 threads per row, 8 rows per pass, 4 passes; two half-blocks.
+        for (int pass = 0; pass < 8; ++pass) {
+          const int half = pass >> 2;                 // 0: direct, 1: mirror
+          const int r = (pass & 3) * 8 + (lane >> 2);  // staged row
+          const int q = lane & 3;                      // float4 within 16
+          const int rr = row0 + r;
+          if (rr < rows) {
+            int b, row;
+            tc_row_map(m, rr, b, row);
+            float* o = a.out + ((size_t)b * a.M + row) * a.J;
+            const float* src = stage + r * kStride + half * 16 + q * 4;
+            const int j = (half ? jm : jb) + q * 4;
+            if (vec && jb + 16 <= a.Jh && (half == 0 || jm >= a.Jh)) {
+              *reinterpret_cast<float4*>(o + j) =
+                  *reinterpret_cast<const float4*>(src);
+            } else {
+#pragma unroll
+              for (int e2 = 0; e2 < 4; ++e2) {
+                const int jj = j + e2;
+                // direct half covers j < Jh; mirrored half covers j >= J - Jh
+                // except the self-mirrored middle row of an odd J.
+                if (half == 0) {
+                  if (jj < a.Jh) o[jj] = src[e2];
+                } else {
+                  const int jsrc = a.J - 1 - jj;  // its direct index
+                  if (jsrc >= 0 && jsrc < a.Jh && jsrc != jj) o[jj] = src[e2];
+                }
+              }
             }
           }
         }
+        __syncwarp();
       }
     } else {
-      float* o = a.out + ((size_t)b * a.M + row) * a.L;
-      if (valid)
-        for (int l = 0; l < m; ++l) o[l] = 0.f;
+      // Structural zeros l < m, one row at a time across the warp.
+      for (int r = 0; r < 32; ++r) {
+        const int rr = row0 + r;
+        if (rr >= rows) break;
+        int b, row;
+        tc_row_map(m, rr, b, row);
+        float* o = a.out + ((size_t)b * a.M + row) * a.L;
+        for (int l = lane; l < m; l += 32) o[l] = 0.f;
+      }
       const int nchunks = (max(n_par[0], n_par[1]) + 15) / 16;
       for (int c = 0; c < nchunks; ++c) {
         float e[16], od[16];
@@ -459,14 +498,27 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
 #pragma unroll
           for (int t = 0; t < 16; ++t) od[t] = 0.f;
         }
-        if (valid) {
+        // Interleave parities: l = m + 32c + 2t + p.
 #pragma unroll
-          for (int t = 0; t < 16; ++t) {
-            const int lp = c * 16 + t;
-            if (lp < n_par[0]) o[m + 2 * lp] = e[t];
-            if (lp < n_par[1]) o[m + 2 * lp + 1] = od[t];
+        for (int t = 0; t < 16; ++t) {
+          stage[lane * kStride + 2 * t] = e[t];
+          stage[lane * kStride + 2 * t + 1] = od[t];
+        }
+        __syncwarp();
+        const int lbase = m + 32 * c;
+        for (int r = 0; r < 32; ++r) {
+          const int rr = row0 + r;
+          if (rr >= rows) break;
+          const int l = lbase + lane;
+          const int lp = 16 * c + (lane >> 1);
+          const bool keep = (lane & 1) ? (lp < n_par[1]) : (lp < n_par[0]);
+          if (keep && l < a.L) {
+            int b, row;
+            tc_row_map(m, rr, b, row);
+            a.out[((size_t)b * a.M + row) * a.L + l] = stage[r * kStride + lane];
           }
         }
+        __syncwarp();
       }
     }
   }

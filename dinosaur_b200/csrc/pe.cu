@@ -9,11 +9,13 @@
 // described in include/dino_b200.h; one explicit evaluation is
 //   modal pre-pass -> inverse SHT -> fused nodal column kernel ->
 //   forward SHT -> modal post-pass,
-// and each RK stage is one fused kernel (combine, per-l implicit solve,
-// implicit terms of the solution, final combination and filter).
+// and each RK stage is an elementwise combine over all planes plus one
+// per-(m, l) kernel for the implicit solve, the implicit terms of the
+// solution, the final combination and the filter.
 
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <vector>
 
 #include "dino_internal.cuh"
@@ -79,6 +81,7 @@ struct dino_pe {
   float* d_f[3] = {nullptr, nullptr, nullptr};
   float* d_g[2] = {nullptr, nullptr};
   float* d_Y = nullptr;
+  float* d_ystar = nullptr;  // Y* of the current stage (implicit planes)
   int* d_flag = nullptr;
   std::vector<dino::InvCacheEntry> inv_cache;
   std::vector<dino::FilterCacheEntry> filter_cache;
@@ -159,8 +162,9 @@ __global__ void pe_prep_kernel(PrepArgs a) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= ML) return;
   const int l = idx % a.L, row = idx / a.L;
-  const int mb = blockIdx.y;
-  for (int k = 0; k < a.K; ++k) {
+  const int k = blockIdx.y;
+  const int mb = blockIdx.z;
+  {
     const float* vort = a.state + pl(a.p_vort, mb, a.K, k) * ML;
     const float* div = a.state + pl(a.p_div, mb, a.K, k) * ML;
     // psi = lap^-1 vort, chi = lap^-1 div (l = 0 -> 0)
@@ -178,6 +182,7 @@ __global__ void pe_prep_kernel(PrepArgs a) {
           dlat_at(q, nullptr, row, l, a.L, a.lw, a.deriv, 0) * a.inv_radius;
     }
   }
+  if (k != 0) return;
   const float* lnps = a.state + ((size_t)a.p_lnps + mb) * ML;
   a.aux[((size_t)a.a_gx + mb) * ML + idx] = d_dlon_at(lnps, row, l, a.L) * a.inv_radius;
   a.aux[((size_t)a.a_gy + mb) * ML + idx] =
@@ -428,13 +433,14 @@ __global__ void pe_post_kernel(PostArgs a) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= ML) return;
   const int l = idx % a.L, row = idx / a.L;
-  const int mb = blockIdx.y;
+  const int k = blockIdx.y;
+  const int mb = blockIdx.z;
   const int K = a.K;
   const bool clip = (l == a.L - 1);
   const float lam = a.lap[l];
 #define FM(p, k) (a.fm + pl(p, mb, K, k) * ML)
 #define OUT(p, k) a.tend[pl(p, mb, K, k) * ML + idx]
-  for (int k = 0; k < K; ++k) {
+  {
     const float* Au = FM(a.o_Au, k);
     const float* Av = FM(a.o_Av, k);
     float vort = -(d_dlon_at(Av, row, l, a.L) -
@@ -470,8 +476,10 @@ __global__ void pe_post_kernel(PostArgs a) {
       OUT(a.p_tr + t * a.mem * K, k) = clip ? 0.f : q;
     }
   }
-  float lnps = a.fm[((size_t)a.o_lnps + mb) * ML + idx];
-  a.tend[((size_t)a.p_lnps + mb) * ML + idx] = clip ? 0.f : lnps;
+  if (k == 0) {
+    float lnps = a.fm[((size_t)a.o_lnps + mb) * ML + idx];
+    a.tend[((size_t)a.p_lnps + mb) * ML + idx] = clip ? 0.f : lnps;
+  }
 #undef FM
 #undef OUT
 }
@@ -566,10 +574,15 @@ __global__ void implicit_inverse_build_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// IMEX stage kernel
+// IMEX stage: an elementwise combine and a per-(m, l) implicit solve
 // ---------------------------------------------------------------------------
 
-struct StageArgs {
+// Y* = y0 + sum_t fc_t f_t + sum_t gc_t g_t over every plane of the packed
+// state (g terms exist on the divergence, temperature and ln ps planes only).
+// Planes without an implicit part (vorticity, tracers) are final after the
+// combine: they go to `out` (times the per-l filter when given); the
+// implicit planes go to `ystar` for the solve.
+struct CombineArgs {
   const float* y0;
   const float* f[3];
   float fc[3];
@@ -577,53 +590,82 @@ struct StageArgs {
   const float* g[2];
   float gc[2];
   int ng;
-  float* g0_out;    // if set: G(y0) is written here and added with g0c
-  float g0c;
-  const float* inv; // [L][N][NP] or null (no solve)
-  float* g_out;     // if set: G(Y) written here
-  float final_c;    // if use_final: out = Y* + final_c G(Y)
-  int use_final;
-  int mode;         // 0: stage, 1: implicit terms of y0
-  const float* filter;  // per-l scaling or null
+  const float* filter;
   float* out;
+  float* ystar;
+  int mK, nT, L;
+  size_t ML;
+};
+
+__global__ void pe_combine_kernel(CombineArgs a) {
+  const int plane = blockIdx.y;
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.ML) return;
+  const bool implicit_plane =
+      (plane >= a.mK && plane < 3 * a.mK) || plane >= (3 + a.nT) * a.mK;
+  const size_t p = (size_t)plane * a.ML + idx;
+  float v = a.y0[p];
+#pragma unroll
+  for (int t = 0; t < 3; ++t)
+    if (t < a.nf) v = fmaf(a.fc[t], a.f[t][p], v);
+  if (implicit_plane) {
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+      if (t < a.ng) v = fmaf(a.gc[t], a.g[t][p], v);
+    a.ystar[p] = v;
+  } else {
+    if (a.filter) v *= a.filter[idx % a.L];
+    a.out[p] = v;
+  }
+}
+
+struct SolveArgs {
+  const float* src;    // Y* (or y0 for the implicit terms)
+  const float* inv;    // [L][N][NP] or null: no solve (Y = src)
+  float* g_out;        // if set: G(Y) (implicit terms of the solution)
+  float* out;          // Y, or the final combination
+  float final_c;       // use_final: out = (Y* + final_c G(Y)) * filter
+  int use_final;
+  int mode;            // 0: solve, 1: out = G(src)
+  const float* filter;
   int K, mem, nT, M, L;
-  int p_vort, p_div, p_temp, p_tr, p_lnps;
+  int p_div, p_temp, p_lnps;
   const float* mat;  // padded G then H (KM x KM each)
-  const float* lev;  // level constants (tref at lo_tref, dsig at 0)
+  const float* lev;  // level constants (dsig at 0, tref at lo_tref)
   int lo_tref;
   const float* lap;
   float R;
   int LT;            // l values per CTA
 };
 
+// Row i of G(v) in the padded (div, temp, ln ps) layout: div rows
+// -lam (G T + R Tref lnps), temp rows -H div, ln ps -dsig . div
+// (primitive_equations.py:1196-1249).
 template <int KM>
-__device__ __forceinline__ void apply_implicit(const float* Gs, const float* Hs,
-                                               const float* trs,
-                                               const float* dss, float lam,
-                                               float R, const float* v,
-                                               float* o) {
-  constexpr int N = 2 * KM + 1;
-  (void)N;
+__device__ __forceinline__ float implicit_row(int i, const float* Gs,
+                                              const float* Hs, const float* trs,
+                                              const float* dss, float lam,
+                                              float R, const float* v) {
+  if (i < KM) {
+    float s = R * trs[i] * v[2 * KM];
 #pragma unroll
-  for (int k = 0; k < KM; ++k) {
-    float s = R * trs[k] * v[2 * KM];
+    for (int c = 0; c < KM; ++c) s = fmaf(Gs[i * KM + c], v[KM + c], s);
+    return -lam * s;
+  }
+  if (i < 2 * KM) {
     float h = 0.f;
 #pragma unroll
-    for (int c = 0; c < KM; ++c) {
-      s = fmaf(Gs[k * KM + c], v[KM + c], s);
-      h = fmaf(Hs[k * KM + c], v[c], h);
-    }
-    o[k] = -lam * s;
-    o[KM + k] = -h;
+    for (int c = 0; c < KM; ++c) h = fmaf(Hs[(i - KM) * KM + c], v[c], h);
+    return -h;
   }
-  float p = 0.f;
+  float q = 0.f;
 #pragma unroll
-  for (int c = 0; c < KM; ++c) p = fmaf(dss[c], v[c], p);
-  o[2 * KM] = -p;
+  for (int c = 0; c < KM; ++c) q = fmaf(dss[c], v[c], q);
+  return -q;
 }
 
 template <int KM>
-__global__ void __launch_bounds__(256) pe_stage_kernel(StageArgs a) {
+__global__ void __launch_bounds__(256) pe_solve_kernel(SolveArgs a) {
   constexpr int N = 2 * KM + 1;
   constexpr int NP = (N + 3) & ~3;
   extern __shared__ __align__(16) float smem[];
@@ -636,7 +678,6 @@ __global__ void __launch_bounds__(256) pe_stage_kernel(StageArgs a) {
   const int l0 = blockIdx.x * a.LT;
   const int rows_per = blockDim.x / a.LT;
   const int K = a.K;
-  // Stage constants in shared memory.
   if (a.inv) {
     for (int lo = 0; lo < a.LT; ++lo) {
       int l = l0 + lo;
@@ -661,115 +702,68 @@ __global__ void __launch_bounds__(256) pe_stage_kernel(StageArgs a) {
   const size_t off = (size_t)row * a.L + l;
   const float lam = a.lap[l];
   const float filt = a.filter ? a.filter[l] : 1.f;
-
-  // Gather the (div, temp, ln ps) column and form Y*.
-  float ys[N];
-#pragma unroll
-  for (int i = 0; i < N; ++i) ys[i] = 0.f;
+  // padded index -> plane of the packed state
   auto plane_of = [&](int i) -> size_t {
-    // padded index -> packed plane
     if (i < KM) return pl(a.p_div, mb, K, i);
     if (i < 2 * KM) return pl(a.p_temp, mb, K, i - KM);
     return (size_t)a.p_lnps + mb;
   };
-  auto valid = [&](int i) { return (i < KM) ? i < K : (i < 2 * KM ? i - KM < K : true); };
+  auto valid = [&](int i) {
+    return (i < KM) ? i < K : (i < 2 * KM ? i - KM < K : true);
+  };
+  float ys[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) ys[i] = valid(i) ? a.src[plane_of(i) * ML + off] : 0.f;
+  if (a.mode == 1) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      if (valid(i))
+        a.out[plane_of(i) * ML + off] = implicit_row<KM>(i, Gs, Hs, trs, dss, lam, a.R, ys);
+    return;
+  }
+  float y[N];
+  if (a.inv) {
+    const float* Mt = Ms + (size_t)lo * N * NP;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      float acc = 0.f;
+      const float4* mrow = reinterpret_cast<const float4*>(Mt + i * NP);
+#pragma unroll
+      for (int c4 = 0; c4 < NP / 4; ++c4) {
+        float4 mv = mrow[c4];
+        if (4 * c4 + 0 < N) acc = fmaf(mv.x, ys[4 * c4 + 0], acc);
+        if (4 * c4 + 1 < N) acc = fmaf(mv.y, ys[4 * c4 + 1], acc);
+        if (4 * c4 + 2 < N) acc = fmaf(mv.z, ys[4 * c4 + 2], acc);
+        if (4 * c4 + 3 < N) acc = fmaf(mv.w, ys[4 * c4 + 3], acc);
+      }
+      y[i] = acc;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) y[i] = ys[i];
+  }
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     if (!valid(i)) continue;
-    size_t p = plane_of(i) * ML + off;
-    float v = a.y0[p];
-    if (a.mode == 0) {
-      for (int t = 0; t < a.nf; ++t) v = fmaf(a.fc[t], a.f[t][p], v);
-      for (int t = 0; t < a.ng; ++t) v = fmaf(a.gc[t], a.g[t][p], v);
-    }
-    ys[i] = v;
-  }
-  if (a.mode == 1) {
-    float gv[N];
-    apply_implicit<KM>(Gs, Hs, trs, dss, lam, a.R, ys, gv);
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-      if (valid(i)) a.out[plane_of(i) * ML + off] = gv[i];
-  } else {
-    if (a.g0_out) {
-      // G(y0) needs the bare y0 column.
-      float y0v[N], gv[N];
-#pragma unroll
-      for (int i = 0; i < N; ++i)
-        y0v[i] = valid(i) ? a.y0[plane_of(i) * ML + off] : 0.f;
-      apply_implicit<KM>(Gs, Hs, trs, dss, lam, a.R, y0v, gv);
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        if (!valid(i)) continue;
-        a.g0_out[plane_of(i) * ML + off] = gv[i];
-        ys[i] = fmaf(a.g0c, gv[i], ys[i]);
-      }
-    }
-    float y[N];
-    if (a.inv) {
-      const float* Mt = Ms + (size_t)lo * N * NP;
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        float acc = 0.f;
-        const float4* mrow = reinterpret_cast<const float4*>(Mt + i * NP);
-#pragma unroll
-        for (int c4 = 0; c4 < NP / 4; ++c4) {
-          float4 mv = mrow[c4];
-          if (4 * c4 + 0 < N) acc = fmaf(mv.x, ys[4 * c4 + 0], acc);
-          if (4 * c4 + 1 < N) acc = fmaf(mv.y, ys[4 * c4 + 1], acc);
-          if (4 * c4 + 2 < N) acc = fmaf(mv.z, ys[4 * c4 + 2], acc);
-          if (4 * c4 + 3 < N) acc = fmaf(mv.w, ys[4 * c4 + 3], acc);
-        }
-        y[i] = acc;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < N; ++i) y[i] = ys[i];
-    }
+    const size_t p = plane_of(i) * ML + off;
+    float o = y[i];
     if (a.g_out || a.use_final) {
-      float gy[N];
-      apply_implicit<KM>(Gs, Hs, trs, dss, lam, a.R, y, gy);
-      if (a.g_out) {
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-          if (valid(i)) a.g_out[plane_of(i) * ML + off] = gy[i];
-      }
-      if (a.use_final) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) y[i] = fmaf(a.final_c, gy[i], ys[i]);
-      }
+      const float gi = implicit_row<KM>(i, Gs, Hs, trs, dss, lam, a.R, y);
+      if (a.g_out) a.g_out[p] = gi;
+      if (a.use_final) o = fmaf(a.final_c, gi, ys[i]);
     }
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-      if (valid(i)) a.out[plane_of(i) * ML + off] = y[i] * filt;
-  }
-  // Vorticity and tracers: no implicit part.
-  const int nkind = 1 + a.nT;
-  for (int kd = 0; kd < nkind; ++kd) {
-    const int pb = (kd == 0) ? a.p_vort : a.p_tr + (kd - 1) * a.mem * K;
-    for (int k = 0; k < K; ++k) {
-      size_t p = pl(pb, mb, K, k) * ML + off;
-      float v;
-      if (a.mode == 1) {
-        v = 0.f;
-      } else {
-        v = a.y0[p];
-        for (int t = 0; t < a.nf; ++t) v = fmaf(a.fc[t], a.f[t][p], v);
-        v *= filt;
-      }
-      a.out[p] = v;
-    }
+    a.out[p] = o * filt;
   }
 }
 
 template <int KM>
-static int launch_stage_km(dino_pe* pe, StageArgs a, cudaStream_t st) {
+static int launch_solve_km(dino_pe* pe, SolveArgs a, cudaStream_t st) {
   constexpr int N = 2 * KM + 1;
   constexpr int NP = (N + 3) & ~3;
   const size_t per_l = sizeof(float) * N * NP;
-  int LT = (int)((64 * 1024) / per_l);
+  int LT = (int)((48 * 1024) / per_l);
   if (LT < 1) LT = 1;
-  if (LT > 16) LT = 16;
+  if (LT > 8) LT = 8;
   int p2 = 1;
   while (p2 * 2 <= LT) p2 *= 2;
   LT = p2;
@@ -780,48 +774,46 @@ static int launch_stage_km(dino_pe* pe, StageArgs a, cudaStream_t st) {
   const size_t smem = per_l * LT + sizeof(float) * (2 * KM * KM + 2 * KM);
   static bool configured = false;
   if (!configured) {
-    DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_stage_kernel<KM>,
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_solve_kernel<KM>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          200 * 1024));
     configured = true;
   }
   if (!pe) return DINO_OK;  // attribute set-up only
   dim3 grid(ceil_div(pe->L, LT), ceil_div(pe->M, threads / LT), pe->mem);
-  pe_stage_kernel<KM><<<grid, threads, smem, st>>>(a);
-  return check_launch("pe_stage");
+  pe_solve_kernel<KM><<<grid, threads, smem, st>>>(a);
+  return check_launch("pe_solve");
 }
 
-static int launch_stage_n(int km, dino_pe* pe, StageArgs a, cudaStream_t st) {
+static int launch_solve_n(int km, dino_pe* pe, SolveArgs a, cudaStream_t st) {
   switch (km) {
-    case 8: return launch_stage_km<8>(pe, a, st);
-    case 16: return launch_stage_km<16>(pe, a, st);
-    case 24: return launch_stage_km<24>(pe, a, st);
-    case 32: return launch_stage_km<32>(pe, a, st);
-    case 48: return launch_stage_km<48>(pe, a, st);
+    case 8: return launch_solve_km<8>(pe, a, st);
+    case 16: return launch_solve_km<16>(pe, a, st);
+    case 24: return launch_solve_km<24>(pe, a, st);
+    case 32: return launch_solve_km<32>(pe, a, st);
+    case 48: return launch_solve_km<48>(pe, a, st);
   }
   set_error("internal: unsupported padded level count");
   return DINO_ERR_UNSUPPORTED;
 }
 
-static int launch_stage(dino_pe* pe, StageArgs a, cudaStream_t st) {
-  return launch_stage_n(pe->KM, pe, a, st);
+static int launch_solve(dino_pe* pe, SolveArgs a, cudaStream_t st) {
+  return launch_solve_n(pe->KM, pe, a, st);
 }
 
 // ---------------------------------------------------------------------------
 // Host orchestration
 // ---------------------------------------------------------------------------
 
-static StageArgs base_stage(dino_pe* pe) {
-  StageArgs a{};
+static SolveArgs base_solve(dino_pe* pe) {
+  SolveArgs a{};
   a.K = pe->K;
   a.mem = pe->mem;
   a.nT = pe->nT;
   a.M = pe->M;
   a.L = pe->L;
-  a.p_vort = 0;
   a.p_div = pe->mem * pe->K;
   a.p_temp = 2 * pe->mem * pe->K;
-  a.p_tr = 3 * pe->mem * pe->K;
   a.p_lnps = (3 + pe->nT) * pe->mem * pe->K;
   a.mat = pe->d_mat;
   a.lev = pe->d_lev;
@@ -829,6 +821,37 @@ static StageArgs base_stage(dino_pe* pe) {
   a.lap = pe->plan->d_lap;
   a.R = (float)pe->R;
   return a;
+}
+
+struct Term {
+  float c;
+  const float* x;
+};
+
+static int launch_combine(dino_pe* pe, const float* y0,
+                          std::initializer_list<Term> f,
+                          std::initializer_list<Term> g, const float* filter,
+                          float* out, cudaStream_t st) {
+  CombineArgs a{};
+  a.y0 = y0;
+  for (const Term& t : f) {
+    a.fc[a.nf] = t.c;
+    a.f[a.nf++] = t.x;
+  }
+  for (const Term& t : g) {
+    a.gc[a.ng] = t.c;
+    a.g[a.ng++] = t.x;
+  }
+  a.filter = filter;
+  a.out = out;
+  a.ystar = pe->d_ystar;
+  a.mK = pe->mem * pe->K;
+  a.nT = pe->nT;
+  a.L = pe->L;
+  a.ML = pe->ML;
+  dim3 grid(ceil_div((int)pe->ML, 256), pe->n_state);
+  pe_combine_kernel<<<grid, 256, 0, st>>>(a);
+  return check_launch("pe_combine");
 }
 
 static int get_inverse(dino_pe* pe, double eta, const float** out) {
@@ -939,7 +962,7 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
     a.lap = p->d_lap;
     a.invlap = p->d_invlap;
     a.inv_radius = (float)(1.0 / p->radius);
-    dim3 grid(ceil_div((int)pe->ML, 256), mem);
+    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
     pe_prep_kernel<<<grid, 256, 0, st>>>(a);
     DINO_TRY(check_launch("pe_prep"));
   }
@@ -1059,7 +1082,7 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
     a.lap = p->d_lap;
     a.inv_radius = (float)(1.0 / p->radius);
     a.gravity = (float)pe->g;
-    dim3 grid(ceil_div((int)pe->ML, 256), mem);
+    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
     pe_post_kernel<<<grid, 256, 0, st>>>(a);
     DINO_TRY(check_launch("pe_post"));
   }
@@ -1067,64 +1090,62 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
 }
 
 // One filtered imex_rk_sil3 step in place (time_integration.py:329-405 with
-// the SIL3 tableau; see the launch sequence in the file header).
+// the SIL3 tableau a_ex = [[1/3], [1/6, 1/2], [1/2, -1/2, 1]],
+// a_im = [[1/6, 1/6], [1/3, 0, 1/3], [3/8, 0, 3/8, 1/4]]):
+//   f0 = F(y), g0 = G(y)
+//   Y1 = (1 - dt/6 G)^-1 (y + dt/3 f0 + dt/6 g0),            f1 = F(Y1)
+//   Y2 = (1 - dt/3 G)^-1 (y + dt/6 f0 + dt/2 f1 + dt/3 g0),  f2 = F(Y2), g2 = G(Y2)
+//   Y3* = y + dt/2 f0 - dt/2 f1 + dt f2 + 3dt/8 g0 + 3dt/8 g2
+//   y_next = filter(Y3* + dt/4 G((1 - dt/4 G)^-1 Y3*))
+// Each stage is one elementwise combine plus one per-(m, l) solve.
 static int pe_step_once(dino_pe* pe, float* y, double dt, const float* filt,
                         const float* inv1, const float* inv2, const float* inv3,
                         cudaStream_t st) {
-  const float fdt = (float)dt;
   DINO_TRY(pe_explicit_impl(pe, y, pe->d_f[0], st));
   {
-    StageArgs a = base_stage(pe);
-    a.y0 = y;
-    a.f[0] = pe->d_f[0];
-    a.fc[0] = (float)(dt * (1.0 / 3.0));
-    a.nf = 1;
-    a.ng = 0;
-    a.g0_out = pe->d_g[0];
-    a.g0c = (float)(dt * (1.0 / 6.0));
+    SolveArgs a = base_solve(pe);
+    a.src = y;
+    a.mode = 1;
+    a.out = pe->d_g[0];
+    DINO_TRY(launch_solve(pe, a, st));
+  }
+  DINO_TRY(launch_combine(pe, y, {{(float)(dt / 3.0), pe->d_f[0]}},
+                          {{(float)(dt / 6.0), pe->d_g[0]}}, nullptr, pe->d_Y, st));
+  {
+    SolveArgs a = base_solve(pe);
+    a.src = pe->d_ystar;
     a.inv = inv1;
     a.out = pe->d_Y;
-    DINO_TRY(launch_stage(pe, a, st));
+    DINO_TRY(launch_solve(pe, a, st));
   }
   DINO_TRY(pe_explicit_impl(pe, pe->d_Y, pe->d_f[1], st));
+  DINO_TRY(launch_combine(
+      pe, y, {{(float)(dt / 6.0), pe->d_f[0]}, {(float)(dt * 0.5), pe->d_f[1]}},
+      {{(float)(dt / 3.0), pe->d_g[0]}}, nullptr, pe->d_Y, st));
   {
-    StageArgs a = base_stage(pe);
-    a.y0 = y;
-    a.f[0] = pe->d_f[0];
-    a.f[1] = pe->d_f[1];
-    a.fc[0] = (float)(dt * (1.0 / 6.0));
-    a.fc[1] = (float)(dt * 0.5);
-    a.nf = 2;
-    a.g[0] = pe->d_g[0];
-    a.gc[0] = (float)(dt * (1.0 / 3.0));
-    a.ng = 1;
+    SolveArgs a = base_solve(pe);
+    a.src = pe->d_ystar;
     a.inv = inv2;
     a.g_out = pe->d_g[1];
     a.out = pe->d_Y;
-    DINO_TRY(launch_stage(pe, a, st));
+    DINO_TRY(launch_solve(pe, a, st));
   }
   DINO_TRY(pe_explicit_impl(pe, pe->d_Y, pe->d_f[2], st));
+  DINO_TRY(launch_combine(
+      pe, y,
+      {{(float)(dt * 0.5), pe->d_f[0]}, {(float)(dt * -0.5), pe->d_f[1]},
+       {(float)dt, pe->d_f[2]}},
+      {{(float)(dt * 0.375), pe->d_g[0]}, {(float)(dt * 0.375), pe->d_g[1]}},
+      filt, y, st));
   {
-    StageArgs a = base_stage(pe);
-    a.y0 = y;
-    a.f[0] = pe->d_f[0];
-    a.f[1] = pe->d_f[1];
-    a.f[2] = pe->d_f[2];
-    a.fc[0] = (float)(dt * 0.5);
-    a.fc[1] = (float)(dt * -0.5);
-    a.fc[2] = fdt;
-    a.nf = 3;
-    a.g[0] = pe->d_g[0];
-    a.g[1] = pe->d_g[1];
-    a.gc[0] = (float)(dt * 0.375);
-    a.gc[1] = (float)(dt * 0.375);
-    a.ng = 2;
+    SolveArgs a = base_solve(pe);
+    a.src = pe->d_ystar;
     a.inv = inv3;
     a.use_final = 1;
     a.final_c = (float)(dt * 0.25);
     a.filter = filt;
     a.out = y;
-    DINO_TRY(launch_stage(pe, a, st));
+    DINO_TRY(launch_solve(pe, a, st));
   }
   return DINO_OK;
 }
@@ -1155,6 +1176,7 @@ static void pe_free(dino_pe* pe) {
   for (auto* f : pe->d_f) cudaFree(f);
   for (auto* g : pe->d_g) cudaFree(g);
   cudaFree(pe->d_Y);
+  cudaFree(pe->d_ystar);
   cudaFree(pe->d_flag);
   delete pe;
 }
@@ -1275,6 +1297,7 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
   for (auto*& f : pe->d_f) DINO_CHECK_CUDA(cudaMalloc(&f, sizeof(float) * pe->n_state * ML));
   for (auto*& g : pe->d_g) DINO_CHECK_CUDA(cudaMalloc(&g, sizeof(float) * pe->n_state * ML));
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_Y, sizeof(float) * pe->n_state * ML));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_ystar, sizeof(float) * pe->n_state * ML));
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_flag, sizeof(int)));
   DINO_CHECK_CUDA(cudaDeviceSynchronize());
   return DINO_OK;
@@ -1360,11 +1383,14 @@ int dino_pe_explicit(dino_pe* pe, const float* state, float* tend, void* stream)
 int dino_pe_implicit(dino_pe* pe, const float* state, float* out, void* stream) {
   DINO_REQUIRE(pe && state && out, DINO_ERR_ARG, "dino_pe_implicit: null argument");
   DINO_REQUIRE(state != out, DINO_ERR_ARG, "dino_pe_implicit: in and out must differ");
-  StageArgs a = base_stage(pe);
-  a.y0 = state;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Vorticity and tracers have no implicit terms.
+  DINO_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * pe->n_state * pe->ML, st));
+  SolveArgs a = base_solve(pe);
+  a.src = state;
   a.mode = 1;
   a.out = out;
-  return launch_stage(pe, a, (cudaStream_t)stream);
+  return launch_solve(pe, a, st);
 }
 
 int dino_pe_implicit_inverse(dino_pe* pe, const float* state, float* out,
@@ -1373,11 +1399,22 @@ int dino_pe_implicit_inverse(dino_pe* pe, const float* state, float* out,
   DINO_REQUIRE(std::isfinite(eta), DINO_ERR_ARG, "step_size must be finite");
   const float* inv = nullptr;
   DINO_TRY(get_inverse(pe, eta, &inv));
-  StageArgs a = base_stage(pe);
-  a.y0 = state;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (out != state) {
+    // Vorticity and tracer planes pass through unchanged.
+    const size_t mK = (size_t)pe->mem * pe->K;
+    DINO_CHECK_CUDA(cudaMemcpyAsync(out, state, sizeof(float) * mK * pe->ML,
+                                    cudaMemcpyDeviceToDevice, st));
+    if (pe->nT > 0)
+      DINO_CHECK_CUDA(cudaMemcpyAsync(out + 3 * mK * pe->ML, state + 3 * mK * pe->ML,
+                                      sizeof(float) * pe->nT * mK * pe->ML,
+                                      cudaMemcpyDeviceToDevice, st));
+  }
+  SolveArgs a = base_solve(pe);
+  a.src = state;
   a.inv = inv;
   a.out = out;
-  return launch_stage(pe, a, (cudaStream_t)stream);
+  return launch_solve(pe, a, st);
 }
 
 int dino_pe_step(dino_pe* pe, float* state, double dt, const double* host_filter,
@@ -1413,7 +1450,7 @@ int dino_pe_step_graph(dino_pe* pe, float* state, double dt,
     if (g.graph) cudaGraphDestroy(g.graph);
     g = GraphEntry{};
     DINO_TRY(sht_prepare(pe->plan));
-    DINO_TRY(launch_stage_n(pe->KM, nullptr, StageArgs{}, st));
+    DINO_TRY(launch_solve_n(pe->KM, nullptr, SolveArgs{}, st));
     // Capture on a private stream so that the caller's stream (possibly the
     // legacy default stream) is never put in capture mode.
     cudaStream_t cap;

@@ -147,9 +147,20 @@ legendre_inverse_simt(Segs in, float* __restrict__ out, int B, int M, int L,
     int b, row;
     row_map(m, r, b, row);
     float* o = out + ((size_t)b * M + row) * J;
+    const int jv = j0 + tx * 4;
+    if ((J & 3) == 0 && jv + 3 < Jh) {
+      // Row starts are 16-byte aligned; the mirrored block J-4-jv.. is too.
+      *reinterpret_cast<float4*>(o + jv) =
+          make_float4(accE[i][0] + accO[i][0], accE[i][1] + accO[i][1],
+                      accE[i][2] + accO[i][2], accE[i][3] + accO[i][3]);
+      *reinterpret_cast<float4*>(o + (J - 4 - jv)) =
+          make_float4(accE[i][3] - accO[i][3], accE[i][2] - accO[i][2],
+                      accE[i][1] - accO[i][1], accE[i][0] - accO[i][0]);
+      continue;
+    }
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-      int j = j0 + tx * 4 + t;
+      int j = jv + t;
       if (j >= Jh) continue;
       o[j] = accE[i][t] + accO[i][t];
       int jm = J - 1 - j;
@@ -252,24 +263,21 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
     for (int e = 0; e < 4; ++e) Ps[pjq + e][pl_] = pvr[e];
     __syncthreads();
     if (jc + kLegKC < Jh) fetch(jc + kLegKC);
+    // Output l - m = k0 + tx + 8 t: its parity is that of tx, so a thread
+    // reads only the symmetric (even) or antisymmetric (odd) fold.
+    const float* fold = (tx & 1) ? &Ds[0][0] : &Ss[0][0];
 #pragma unroll
     for (int jj = 0; jj < kLegKC; ++jj) {
-      float4 sa = *reinterpret_cast<const float4*>(&Ss[jj][ty * 8]);
-      float4 sb = *reinterpret_cast<const float4*>(&Ss[jj][ty * 8 + 4]);
-      float4 da = *reinterpret_cast<const float4*>(&Ds[jj][ty * 8]);
-      float4 db = *reinterpret_cast<const float4*>(&Ds[jj][ty * 8 + 4]);
-      float s8[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
-      float d8[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
+      float4 fa = *reinterpret_cast<const float4*>(fold + jj * (kLegTB + 4) + ty * 8);
+      float4 fb = *reinterpret_cast<const float4*>(fold + jj * (kLegTB + 4) + ty * 8 + 4);
+      float f8[8] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w};
       float pw[4];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) pw[t] = Ps[jj][tx * 4 + t];
+      for (int t = 0; t < 4; ++t) pw[t] = Ps[jj][tx + 8 * t];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        acc[i][0] = fmaf(s8[i], pw[0], acc[i][0]);
-        acc[i][1] = fmaf(d8[i], pw[1], acc[i][1]);
-        acc[i][2] = fmaf(s8[i], pw[2], acc[i][2]);
-        acc[i][3] = fmaf(d8[i], pw[3], acc[i][3]);
-      }
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) acc[i][t] = fmaf(f8[i], pw[t], acc[i][t]);
     }
   }
 
@@ -282,7 +290,7 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
     float* o = out + ((size_t)b * M + row) * L + m;
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-      int k = k0 + tx * 4 + t;
+      int k = k0 + tx + 8 * t;
       if (k < Lm) o[k] = acc[i][t];
     }
   }
