@@ -15,6 +15,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <initializer_list>
 #include <vector>
 
@@ -28,9 +29,13 @@ constexpr int kMaxTracers = 4;
 // Object
 // ---------------------------------------------------------------------------
 
-struct InvCacheEntry {
-  double eta;
-  float* d_inv;  // [L][N][NP] padded FP32 inverse matrices
+// One per-l operator of the implicit part (see pe_matrix_build_kernel).
+struct MatEntry {
+  int kind = 0;
+  double eta = 0;
+  std::vector<double> filter;  // folded-in step filter (kMatFinal), else empty
+  float* d = nullptr;          // [L][n][RP], transposed, rows zero-padded
+  int R = 0, RP = 0;
 };
 
 struct FilterCacheEntry {
@@ -51,7 +56,6 @@ struct GraphEntry {
 struct dino_pe {
   dino_plan* plan = nullptr;
   int K = 0, mem = 0, nT = 0, hum = -1, vadv = 1, hs = 0, tref_varies = 0;
-  int KM = 0;  // padded level count for the per-l solves
   int M = 0, L = 0, I = 0, J = 0;
   size_t ML = 0, IJ = 0;
   double R = 0, Rv = 0, Cpv = 0, kappa = 0, g = 0, Omega = 0;
@@ -62,7 +66,6 @@ struct dino_pe {
   // Device constants.
   float* d_lev = nullptr;   // per-level constants (see LevOff)
   float* d_lat = nullptr;   // per-latitude constants: sec2, f, sin2, cos2
-  float* d_mat = nullptr;   // padded G and H (KM x KM each)
   float* d_orog = nullptr;  // modal orography [M][L]
   // Field bookkeeping (planes).
   int n_state = 0, n_inv = 0, n_fwd = 0, n_aux = 0;
@@ -83,7 +86,7 @@ struct dino_pe {
   float* d_Y = nullptr;
   float* d_ystar = nullptr;  // Y* of the current stage (implicit planes)
   int* d_flag = nullptr;
-  std::vector<dino::InvCacheEntry> inv_cache;
+  std::deque<dino::MatEntry> mat_cache;  // stable element addresses
   std::vector<dino::FilterCacheEntry> filter_cache;
   dino::GraphEntry graph;
 };
@@ -485,47 +488,73 @@ __global__ void pe_post_kernel(PostArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Per-l implicit matrices (FP64 on the GPU): build (I - eta L_l) as in
-// _get_implicit_term_matrix_sigma (:544-598) and invert with Gauss-Jordan
-// elimination with partial pivoting; store FP32 in the padded layout.
+// Per-l operators of the implicit part, composed in FP64 on the GPU.
+//
+// On the stacked vector (div[K], T'[K], ln ps) of total wavenumber l the
+// implicit terms are y -> L_l y (primitive_equations.py:1196-1249):
+//   div rows  -lam_l (G T' + R Tref ln ps)
+//   T' rows   -H div
+//   ln ps     -dsig . div
+// and implicit_inverse(eta) applies (I - eta L_l)^-1 (_get_implicit_term_
+// matrix_sigma, :544-598, and :1251-1330).  The builder inverts I - eta L_l by
+// Gauss-Jordan elimination with partial pivoting in FP64 (one CTA per l) and
+// writes one FP32 operator per l, transposed ([column k][row r]) with rows
+// zero-padded to the apply kernel's row tile:
+//   kMatL      L_l
+//   kMatInv    (I - eta L_l)^-1
+//   kMatInvG   [(I - eta L_l)^-1 ; L_l (I - eta L_l)^-1]: the solution and its
+//              implicit terms from one product
+//   kMatFinal  f_l (I + eta L_l (I - eta L_l)^-1): the last SIL3 stage,
+//              Y* + eta G(Y) with Y = (I - eta L_l)^-1 Y*, times the filter
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ int pad_index(int i, int K, int KM) {
-  return i < K ? i : (i < 2 * K ? KM + (i - K) : 2 * KM);
-}
+enum MatKind { kMatL = 0, kMatInv = 1, kMatInvG = 2, kMatFinal = 3 };
 
-__global__ void implicit_inverse_build_kernel(
-    int K, int KM, int L, double eta, double R, const double* __restrict__ G,
-    const double* __restrict__ H, const double* __restrict__ tref,
-    const double* __restrict__ dsig, const double* __restrict__ lam,
-    float* __restrict__ out, int* __restrict__ flag) {
+constexpr int kMaxLevels = 48;
+
+struct MatBuildArgs {
+  int K, kind, RP;
+  double eta, R;
+  const double* G;       // K x K
+  const double* H;       // K x K
+  const double* tref;    // K
+  const double* dsig;    // K
+  const double* lam;     // L
+  const double* filter;  // L, or null
+  float* out;            // [L][n][RP]
+  int* flag;
+};
+
+__global__ void pe_matrix_build_kernel(MatBuildArgs a) {
   extern __shared__ double aug[];  // n x 2n
-  const int l = blockIdx.x;
-  const int n = 2 * K + 1, n2 = 2 * n;
-  const int N = 2 * KM + 1, NP = (N + 3) & ~3;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  __shared__ double factor[2 * 64 + 1];
+  __shared__ double factor[2 * kMaxLevels + 1];
   __shared__ int piv;
-  const double lm = lam[l];
-  for (int e = tid; e < n * n2; e += nt) {
-    int r = e / n2, c = e % n2;
-    double v = 0.0;
-    if (c >= n) {
-      v = (c - n == r) ? 1.0 : 0.0;
-    } else if (r < K) {
-      if (c < K) v = (r == c) ? 1.0 : 0.0;
-      else if (c < 2 * K) v = eta * lm * G[r * K + (c - K)];
-      else v = eta * R * lm * tref[r];
-    } else if (r < 2 * K) {
-      if (c < K) v = eta * H[(r - K) * K + c];
-      else if (c < 2 * K) v = (r == c) ? 1.0 : 0.0;
-      else v = 0.0;
-    } else {
-      if (c < K) v = eta * dsig[c];
-      else if (c < 2 * K) v = 0.0;
-      else v = 1.0;
+  const int l = blockIdx.x;
+  const int K = a.K, n = 2 * K + 1, n2 = 2 * n;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const double lm = a.lam[l];
+  const double eta = a.eta;
+  float* o = a.out + (size_t)l * n * a.RP;
+  auto Lrc = [&](int r, int c) -> double {
+    if (r < K) {
+      if (c < K) return 0.0;
+      if (c < 2 * K) return -lm * a.G[r * K + (c - K)];
+      return -lm * a.R * a.tref[r];
     }
-    aug[e] = v;
+    if (r < 2 * K) return c < K ? -a.H[(r - K) * K + c] : 0.0;
+    return c < K ? -a.dsig[c] : 0.0;
+  };
+  if (a.kind == kMatL) {
+    for (int e = tid; e < n * a.RP; e += nt) {
+      const int c = e / a.RP, r = e - c * a.RP;
+      o[e] = r < n ? (float)Lrc(r, c) : 0.f;
+    }
+    return;
+  }
+  for (int e = tid; e < n * n2; e += nt) {
+    const int r = e / n2, c = e - r * n2;
+    aug[e] = c >= n ? ((c - n == r) ? 1.0 : 0.0)
+                    : ((r == c) ? 1.0 : 0.0) - eta * Lrc(r, c);
   }
   __syncthreads();
   for (int col = 0; col < n; ++col) {
@@ -533,19 +562,19 @@ __global__ void implicit_inverse_build_kernel(
       int best = col;
       double bv = fabs(aug[col * n2 + col]);
       for (int r = col + 1; r < n; ++r) {
-        double v = fabs(aug[r * n2 + col]);
+        const double v = fabs(aug[r * n2 + col]);
         if (v > bv) {
           bv = v;
           best = r;
         }
       }
       piv = best;
-      if (!(bv > 0.0)) atomicExch(flag, 1);
+      if (!(bv > 0.0)) atomicExch(a.flag, 1);
     }
     __syncthreads();
     if (piv != col) {
       for (int c = tid; c < n2; c += nt) {
-        double t = aug[col * n2 + c];
+        const double t = aug[col * n2 + c];
         aug[col * n2 + c] = aug[piv * n2 + c];
         aug[piv * n2 + c] = t;
       }
@@ -557,19 +586,39 @@ __global__ void implicit_inverse_build_kernel(
     for (int r = tid; r < n; r += nt) factor[r] = aug[r * n2 + col];
     __syncthreads();
     for (int e = tid; e < n * n2; e += nt) {
-      int r = e / n2, c = e % n2;
+      const int r = e / n2, c = e - r * n2;
       if (r != col) aug[e] -= factor[r] * aug[col * n2 + c];
     }
     __syncthreads();
   }
-  float* o = out + (size_t)l * N * NP;
-  for (int e = tid; e < N * NP; e += nt) o[e] = 0.f;
-  __syncthreads();
-  for (int e = tid; e < n * n; e += nt) {
-    int r = e / n, c = e % n;
-    double v = aug[r * n2 + n + c];
-    if (!isfinite(v)) atomicExch(flag, 2);
-    o[pad_index(r, K, KM) * NP + pad_index(c, K, KM)] = (float)v;
+  auto inv = [&](int r, int c) { return aug[r * n2 + n + c]; };
+  auto l_inv = [&](int r, int c) -> double {
+    double s = 0.0;
+    if (r < K) {
+      for (int j = 0; j < K; ++j) s += a.G[r * K + j] * inv(K + j, c);
+      return -lm * (s + a.R * a.tref[r] * inv(2 * K, c));
+    }
+    if (r < 2 * K) {
+      for (int j = 0; j < K; ++j) s += a.H[(r - K) * K + j] * inv(j, c);
+      return -s;
+    }
+    for (int j = 0; j < K; ++j) s += a.dsig[j] * inv(j, c);
+    return -s;
+  };
+  const double f = a.filter ? a.filter[l] : 1.0;
+  for (int e = tid; e < n * a.RP; e += nt) {
+    const int c = e / a.RP, r = e - c * a.RP;
+    double v = 0.0;
+    if (a.kind == kMatInv) {
+      if (r < n) v = inv(r, c);
+    } else if (a.kind == kMatInvG) {
+      if (r < n) v = inv(r, c);
+      else if (r < 2 * n) v = l_inv(r - n, c);
+    } else if (r < n) {
+      v = f * (((r == c) ? 1.0 : 0.0) + eta * l_inv(r, c));
+    }
+    if (!isfinite(v)) atomicExch(a.flag, 2);
+    o[e] = (float)v;
   }
 }
 
@@ -619,208 +668,183 @@ __global__ void pe_combine_kernel(CombineArgs a) {
   }
 }
 
-struct SolveArgs {
-  const float* src;    // Y* (or y0 for the implicit terms)
-  const float* inv;    // [L][N][NP] or null: no solve (Y = src)
-  float* g_out;        // if set: G(Y) (implicit terms of the solution)
-  float* out;          // Y, or the final combination
-  float final_c;       // use_final: out = (Y* + final_c G(Y)) * filter
-  int use_final;
-  int mode;            // 0: solve, 1: out = G(src)
-  const float* filter;
-  int K, mem, nT, M, L;
+// Per-(l, column) application of an implicit operator: for every total
+// wavenumber l, Out[R x C] = A_l[R x n] Ys[n x C], where the C = members * M
+// columns are the (member, m-row) pairs and Ys stacks the n = 2K+1 implicit
+// planes (div, T', ln ps).  A CTA takes one l, 64 columns and 16*TR rows of
+// A_l: it stages A_l^T and the gathered Ys in shared memory and each thread
+// accumulates a TR x 4 register tile (broadcast A reads, float4 Ys reads).
+// Rows [0, n) go to `out`, rows [n, 2n) (kMatInvG) to `out2`.  Every element
+// is read and written by one CTA, with a barrier in between, so src may
+// alias out.
+struct ApplyArgs {
+  const float* src;
+  const float* A;
+  float* out;
+  float* out2;
+  int R, n, RP;
+  int K, M, L, C;
   int p_div, p_temp, p_lnps;
-  const float* mat;  // padded G then H (KM x KM each)
-  const float* lev;  // level constants (dsig at 0, tref at lo_tref)
-  int lo_tref;
-  const float* lap;
-  float R;
-  int LT;            // l values per CTA
+  size_t ML;
 };
 
-// Row i of G(v) in the padded (div, temp, ln ps) layout: div rows
-// -lam (G T + R Tref lnps), temp rows -H div, ln ps -dsig . div
-// (primitive_equations.py:1196-1249).
-template <int KM>
-__device__ __forceinline__ float implicit_row(int i, const float* Gs,
-                                              const float* Hs, const float* trs,
-                                              const float* dss, float lam,
-                                              float R, const float* v) {
-  if (i < KM) {
-    float s = R * trs[i] * v[2 * KM];
-#pragma unroll
-    for (int c = 0; c < KM; ++c) s = fmaf(Gs[i * KM + c], v[KM + c], s);
-    return -lam * s;
-  }
-  if (i < 2 * KM) {
-    float h = 0.f;
-#pragma unroll
-    for (int c = 0; c < KM; ++c) h = fmaf(Hs[(i - KM) * KM + c], v[c], h);
-    return -h;
-  }
-  float q = 0.f;
-#pragma unroll
-  for (int c = 0; c < KM; ++c) q = fmaf(dss[c], v[c], q);
-  return -q;
+constexpr int kApplyCols = 64;
+constexpr int kApplyMaxTR = 13;
+
+__device__ __forceinline__ size_t stacked_plane(const ApplyArgs& a, int i, int mb) {
+  if (i < a.K) return pl(a.p_div, mb, a.K, i);
+  if (i < 2 * a.K) return pl(a.p_temp, mb, a.K, i - a.K);
+  return (size_t)a.p_lnps + mb;
 }
 
-template <int KM>
-__global__ void __launch_bounds__(256) pe_solve_kernel(SolveArgs a) {
-  constexpr int N = 2 * KM + 1;
-  constexpr int NP = (N + 3) & ~3;
+template <int TR>
+__global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
+  constexpr int RPT = 16 * TR;
   extern __shared__ __align__(16) float smem[];
-  float* Ms = smem;                               // LT * N * NP
-  float* Gs = Ms + (size_t)a.LT * N * NP;         // KM*KM
-  float* Hs = Gs + KM * KM;                       // KM*KM
-  float* trs = Hs + KM * KM;                      // KM
-  float* dss = trs + KM;                          // KM
+  const int n = a.n;
+  float* At = smem;                    // [n][RPT]
+  float* Ys = At + (size_t)n * RPT;    // [n][kApplyCols]
   const int tid = threadIdx.x;
-  const int l0 = blockIdx.x * a.LT;
-  const int rows_per = blockDim.x / a.LT;
-  const int K = a.K;
-  if (a.inv) {
-    for (int lo = 0; lo < a.LT; ++lo) {
-      int l = l0 + lo;
-      if (l >= a.L) break;
-      const float4* src = reinterpret_cast<const float4*>(a.inv + (size_t)l * N * NP);
-      float4* dst = reinterpret_cast<float4*>(Ms + (size_t)lo * N * NP);
-      for (int e = tid; e < N * NP / 4; e += blockDim.x) dst[e] = src[e];
+  const int c0 = blockIdx.x * kApplyCols;
+  const int l = blockIdx.y;
+  const int r0 = blockIdx.z * RPT;
+  {
+    const float* Ag = a.A + (size_t)l * n * a.RP + r0;
+    constexpr int Q = RPT / 4;
+    for (int e = tid; e < n * Q; e += 256) {
+      const int k = e / Q, q = e - k * Q;
+      reinterpret_cast<float4*>(At)[e] =
+          reinterpret_cast<const float4*>(Ag + (size_t)k * a.RP)[q];
     }
   }
-  for (int e = tid; e < 2 * KM * KM; e += blockDim.x) Gs[e] = a.mat[e];
-  for (int e = tid; e < KM; e += blockDim.x) {
-    trs[e] = e < K ? a.lev[a.lo_tref + e] : 0.f;
-    dss[e] = e < K ? a.lev[e] : 0.f;
+  for (int e = tid; e < n * kApplyCols; e += 256) {
+    const int k = e / kApplyCols, c = c0 + (e % kApplyCols);
+    float v = 0.f;
+    if (c < a.C) {
+      const int mb = c / a.M, row = c - mb * a.M;
+      v = a.src[stacked_plane(a, k, mb) * a.ML + (size_t)row * a.L + l];
+    }
+    Ys[e] = v;
   }
   __syncthreads();
-  const int lo = tid % a.LT;
-  const int l = l0 + lo;
-  const int row = blockIdx.y * rows_per + tid / a.LT;
-  const int mb = blockIdx.z;
-  if (l >= a.L || row >= a.M) return;
-  const size_t ML = (size_t)a.M * a.L;
-  const size_t off = (size_t)row * a.L + l;
-  const float lam = a.lap[l];
-  const float filt = a.filter ? a.filter[l] : 1.f;
-  // padded index -> plane of the packed state
-  auto plane_of = [&](int i) -> size_t {
-    if (i < KM) return pl(a.p_div, mb, K, i);
-    if (i < 2 * KM) return pl(a.p_temp, mb, K, i - KM);
-    return (size_t)a.p_lnps + mb;
-  };
-  auto valid = [&](int i) {
-    return (i < KM) ? i < K : (i < 2 * KM ? i - KM < K : true);
-  };
-  float ys[N];
+  const int cg = tid & 15, rg = tid >> 4;
+  float acc[TR][4];
 #pragma unroll
-  for (int i = 0; i < N; ++i) ys[i] = valid(i) ? a.src[plane_of(i) * ML + off] : 0.f;
-  if (a.mode == 1) {
+  for (int i = 0; i < TR; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+  const float* ar = At + rg * TR;
+  const float4* yr = reinterpret_cast<const float4*>(Ys) + cg;
+#pragma unroll 2
+  for (int k = 0; k < n; ++k) {
+    const float4 y = yr[k * (kApplyCols / 4)];
 #pragma unroll
-    for (int i = 0; i < N; ++i)
-      if (valid(i))
-        a.out[plane_of(i) * ML + off] = implicit_row<KM>(i, Gs, Hs, trs, dss, lam, a.R, ys);
-    return;
-  }
-  float y[N];
-  if (a.inv) {
-    const float* Mt = Ms + (size_t)lo * N * NP;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      float acc = 0.f;
-      const float4* mrow = reinterpret_cast<const float4*>(Mt + i * NP);
-#pragma unroll
-      for (int c4 = 0; c4 < NP / 4; ++c4) {
-        float4 mv = mrow[c4];
-        if (4 * c4 + 0 < N) acc = fmaf(mv.x, ys[4 * c4 + 0], acc);
-        if (4 * c4 + 1 < N) acc = fmaf(mv.y, ys[4 * c4 + 1], acc);
-        if (4 * c4 + 2 < N) acc = fmaf(mv.z, ys[4 * c4 + 2], acc);
-        if (4 * c4 + 3 < N) acc = fmaf(mv.w, ys[4 * c4 + 3], acc);
-      }
-      y[i] = acc;
+    for (int i = 0; i < TR; ++i) {
+      const float av = ar[k * RPT + i];
+      acc[i][0] = fmaf(av, y.x, acc[i][0]);
+      acc[i][1] = fmaf(av, y.y, acc[i][1]);
+      acc[i][2] = fmaf(av, y.z, acc[i][2]);
+      acc[i][3] = fmaf(av, y.w, acc[i][3]);
     }
-  } else {
-#pragma unroll
-    for (int i = 0; i < N; ++i) y[i] = ys[i];
   }
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    if (!valid(i)) continue;
-    const size_t p = plane_of(i) * ML + off;
-    float o = y[i];
-    if (a.g_out || a.use_final) {
-      const float gi = implicit_row<KM>(i, Gs, Hs, trs, dss, lam, a.R, y);
-      if (a.g_out) a.g_out[p] = gi;
-      if (a.use_final) o = fmaf(a.final_c, gi, ys[i]);
+  for (int j = 0; j < 4; ++j) {
+    const int c = c0 + cg * 4 + j;
+    if (c >= a.C) continue;
+    const int mb = c / a.M, row = c - mb * a.M;
+    const size_t off = (size_t)row * a.L + l;
+#pragma unroll
+    for (int i = 0; i < TR; ++i) {
+      const int r = r0 + rg * TR + i;
+      if (r >= a.R) continue;
+      float* dst = r < n ? a.out + stacked_plane(a, r, mb) * a.ML
+                         : a.out2 + stacked_plane(a, r - n, mb) * a.ML;
+      dst[off] = acc[i][j];
     }
-    a.out[p] = o * filt;
   }
 }
 
-template <int KM>
-static int launch_solve_km(dino_pe* pe, SolveArgs a, cudaStream_t st) {
-  constexpr int N = 2 * KM + 1;
-  constexpr int NP = (N + 3) & ~3;
-  const size_t per_l = sizeof(float) * N * NP;
-  int LT = (int)((48 * 1024) / per_l);
-  if (LT < 1) LT = 1;
-  if (LT > 8) LT = 8;
-  int p2 = 1;
-  while (p2 * 2 <= LT) p2 *= 2;
-  LT = p2;
-  a.LT = LT;
-  const int threads = 256;
-  // The matrix area is reserved even when no solve runs: the kernel places
-  // G, H and the level constants after it unconditionally.
-  const size_t smem = per_l * LT + sizeof(float) * (2 * KM * KM + 2 * KM);
-  static bool configured = false;
-  if (!configured) {
-    DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_solve_kernel<KM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         200 * 1024));
-    configured = true;
-  }
-  if (!pe) return DINO_OK;  // attribute set-up only
-  dim3 grid(ceil_div(pe->L, LT), ceil_div(pe->M, threads / LT), pe->mem);
-  pe_solve_kernel<KM><<<grid, threads, smem, st>>>(a);
-  return check_launch("pe_solve");
+// Rows per thread for an operator of R rows (one row tile while R <= 208).
+static int apply_tr(int R) {
+  int tr = (R + 15) / 16;
+  return tr > kApplyMaxTR ? kApplyMaxTR : tr;
 }
 
-static int launch_solve_n(int km, dino_pe* pe, SolveArgs a, cudaStream_t st) {
-  switch (km) {
-    case 8: return launch_solve_km<8>(pe, a, st);
-    case 16: return launch_solve_km<16>(pe, a, st);
-    case 24: return launch_solve_km<24>(pe, a, st);
-    case 32: return launch_solve_km<32>(pe, a, st);
-    case 48: return launch_solve_km<48>(pe, a, st);
-  }
-  set_error("internal: unsupported padded level count");
-  return DINO_ERR_UNSUPPORTED;
+static size_t apply_smem(int n, int tr) {
+  return sizeof(float) * (size_t)n * (16 * tr + kApplyCols);
 }
 
-static int launch_solve(dino_pe* pe, SolveArgs a, cudaStream_t st) {
-  return launch_solve_n(pe->KM, pe, a, st);
+template <int TR>
+static int apply_attr() {
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_apply_kernel<TR>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)apply_smem(2 * kMaxLevels + 1, TR)));
+  return DINO_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Host orchestration
-// ---------------------------------------------------------------------------
+// Sets the shared-memory attribute of every instantiation once (kept out of
+// graph capture).
+static int prepare_apply() {
+  static bool done = false;
+  if (done) return DINO_OK;
+  DINO_TRY(apply_attr<1>());
+  DINO_TRY(apply_attr<2>());
+  DINO_TRY(apply_attr<3>());
+  DINO_TRY(apply_attr<4>());
+  DINO_TRY(apply_attr<5>());
+  DINO_TRY(apply_attr<6>());
+  DINO_TRY(apply_attr<7>());
+  DINO_TRY(apply_attr<8>());
+  DINO_TRY(apply_attr<9>());
+  DINO_TRY(apply_attr<10>());
+  DINO_TRY(apply_attr<11>());
+  DINO_TRY(apply_attr<12>());
+  DINO_TRY(apply_attr<13>());
+  done = true;
+  return DINO_OK;
+}
 
-static SolveArgs base_solve(dino_pe* pe) {
-  SolveArgs a{};
+template <int TR>
+static void apply_launch(dim3 grid, size_t smem, cudaStream_t st, const ApplyArgs& a) {
+  pe_apply_kernel<TR><<<grid, 256, smem, st>>>(a);
+}
+
+static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
+                        float* out, float* out2, cudaStream_t st) {
+  ApplyArgs a{};
+  a.src = src;
+  a.A = m->d;
+  a.out = out;
+  a.out2 = out2;
+  a.R = m->R;
+  a.n = 2 * pe->K + 1;
+  a.RP = m->RP;
   a.K = pe->K;
-  a.mem = pe->mem;
-  a.nT = pe->nT;
   a.M = pe->M;
   a.L = pe->L;
+  a.C = pe->mem * pe->M;
   a.p_div = pe->mem * pe->K;
   a.p_temp = 2 * pe->mem * pe->K;
   a.p_lnps = (3 + pe->nT) * pe->mem * pe->K;
-  a.mat = pe->d_mat;
-  a.lev = pe->d_lev;
-  a.lo_tref = lev_offsets(pe->K).tref;
-  a.lap = pe->plan->d_lap;
-  a.R = (float)pe->R;
-  return a;
+  a.ML = pe->ML;
+  const int tr = apply_tr(m->R);
+  const int rpt = 16 * tr;
+  dim3 grid(ceil_div(a.C, kApplyCols), pe->L, ceil_div(m->R, rpt));
+  const size_t smem = apply_smem(a.n, tr);
+  switch (tr) {
+    case 1: apply_launch<1>(grid, smem, st, a); break;
+    case 2: apply_launch<2>(grid, smem, st, a); break;
+    case 3: apply_launch<3>(grid, smem, st, a); break;
+    case 4: apply_launch<4>(grid, smem, st, a); break;
+    case 5: apply_launch<5>(grid, smem, st, a); break;
+    case 6: apply_launch<6>(grid, smem, st, a); break;
+    case 7: apply_launch<7>(grid, smem, st, a); break;
+    case 8: apply_launch<8>(grid, smem, st, a); break;
+    case 9: apply_launch<9>(grid, smem, st, a); break;
+    case 10: apply_launch<10>(grid, smem, st, a); break;
+    case 11: apply_launch<11>(grid, smem, st, a); break;
+    case 12: apply_launch<12>(grid, smem, st, a); break;
+    default: apply_launch<13>(grid, smem, st, a); break;
+  }
+  return check_launch("pe_apply");
 }
 
 struct Term {
@@ -854,55 +878,80 @@ static int launch_combine(dino_pe* pe, const float* y0,
   return check_launch("pe_combine");
 }
 
-static int get_inverse(dino_pe* pe, double eta, const float** out) {
-  for (auto& e : pe->inv_cache) {
-    if (e.eta == eta) {
-      *out = e.d_inv;
+static int get_matrix(dino_pe* pe, int kind, double eta, const double* host_filter,
+                      const MatEntry** out) {
+  const int K = pe->K, L = pe->L, n = 2 * K + 1;
+  if (kind == kMatL) eta = 0.0;
+  if (kind != kMatFinal) host_filter = nullptr;
+  for (auto& e : pe->mat_cache) {
+    if (e.kind != kind || e.eta != eta) continue;
+    if (host_filter ? (e.filter.size() == (size_t)L &&
+                       std::memcmp(e.filter.data(), host_filter, sizeof(double) * L) == 0)
+                    : e.filter.empty()) {
+      *out = &e;
       return DINO_OK;
     }
   }
-  const int K = pe->K, KM = pe->KM, L = pe->L;
-  const int N = 2 * KM + 1, NP = (N + 3) & ~3;
-  const int n = 2 * K + 1;
-  DINO_REQUIRE(K <= 64, DINO_ERR_UNSUPPORTED, "implicit inverse supports up to 64 levels");
-  double *dG, *dH, *dT, *dS, *dL;
+  DINO_REQUIRE(K <= kMaxLevels, DINO_ERR_UNSUPPORTED, "implicit operators support up to 48 levels");
+  DINO_TRY(prepare_apply());
+  MatEntry m;
+  m.kind = kind;
+  m.eta = eta;
+  if (host_filter) m.filter.assign(host_filter, host_filter + L);
+  m.R = kind == kMatInvG ? 2 * n : n;
+  const int rpt = 16 * apply_tr(m.R);
+  m.RP = ceil_div(m.R, rpt) * rpt;
   std::vector<double> lam(L);
   for (int l = 0; l < L; ++l)
     lam[l] = -(double)l * (l + 1) / (pe->plan->radius * pe->plan->radius);
-  DINO_CHECK_CUDA(cudaMalloc(&dG, sizeof(double) * K * K));
-  DINO_CHECK_CUDA(cudaMalloc(&dH, sizeof(double) * K * K));
-  DINO_CHECK_CUDA(cudaMalloc(&dT, sizeof(double) * K));
-  DINO_CHECK_CUDA(cudaMalloc(&dS, sizeof(double) * K));
-  DINO_CHECK_CUDA(cudaMalloc(&dL, sizeof(double) * L));
-  DINO_CHECK_CUDA(cudaMemcpy(dG, pe->G.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
-  DINO_CHECK_CUDA(cudaMemcpy(dH, pe->H.data(), sizeof(double) * K * K, cudaMemcpyHostToDevice));
-  DINO_CHECK_CUDA(cudaMemcpy(dT, pe->tref.data(), sizeof(double) * K, cudaMemcpyHostToDevice));
-  DINO_CHECK_CUDA(cudaMemcpy(dS, pe->dsig.data(), sizeof(double) * K, cudaMemcpyHostToDevice));
-  DINO_CHECK_CUDA(cudaMemcpy(dL, lam.data(), sizeof(double) * L, cudaMemcpyHostToDevice));
-  float* d_inv;
-  DINO_CHECK_CUDA(cudaMalloc(&d_inv, sizeof(float) * (size_t)L * N * NP));
-  DINO_CHECK_CUDA(cudaMemset(pe->d_flag, 0, sizeof(int)));
-  size_t smem = sizeof(double) * n * 2 * n;
-  DINO_CHECK_CUDA(cudaFuncSetAttribute(implicit_inverse_build_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-  implicit_inverse_build_kernel<<<L, 256, smem>>>(K, KM, L, eta, pe->R, dG, dH, dT,
-                                                  dS, dL, d_inv, pe->d_flag);
-  DINO_TRY(check_launch("implicit_inverse_build"));
-  int flag = 0;
-  DINO_CHECK_CUDA(cudaMemcpy(&flag, pe->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
-  cudaFree(dG);
-  cudaFree(dH);
-  cudaFree(dT);
-  cudaFree(dS);
-  cudaFree(dL);
-  if (flag) {
-    cudaFree(d_inv);
-    set_error("implicit matrix is singular or its inverse is not finite");
-    return DINO_ERR_NAN;
+  std::vector<double> consts;
+  consts.insert(consts.end(), pe->G.begin(), pe->G.end());
+  consts.insert(consts.end(), pe->H.begin(), pe->H.end());
+  consts.insert(consts.end(), pe->tref.begin(), pe->tref.end());
+  consts.insert(consts.end(), pe->dsig.begin(), pe->dsig.end());
+  consts.insert(consts.end(), lam.begin(), lam.end());
+  if (host_filter) consts.insert(consts.end(), host_filter, host_filter + L);
+  double* dc = nullptr;
+  auto build = [&]() -> int {
+    DINO_CHECK_CUDA(cudaMalloc(&dc, sizeof(double) * consts.size()));
+    DINO_CHECK_CUDA(cudaMemcpy(dc, consts.data(), sizeof(double) * consts.size(),
+                               cudaMemcpyHostToDevice));
+    DINO_CHECK_CUDA(cudaMalloc(&m.d, sizeof(float) * (size_t)L * n * m.RP));
+    DINO_CHECK_CUDA(cudaMemset(pe->d_flag, 0, sizeof(int)));
+    MatBuildArgs b{};
+    b.K = K;
+    b.kind = kind;
+    b.RP = m.RP;
+    b.eta = eta;
+    b.R = pe->R;
+    b.G = dc;
+    b.H = dc + K * K;
+    b.tref = dc + 2 * K * K;
+    b.dsig = dc + 2 * K * K + K;
+    b.lam = dc + 2 * K * K + 2 * K;
+    b.filter = host_filter ? dc + 2 * K * K + 2 * K + L : nullptr;
+    b.out = m.d;
+    b.flag = pe->d_flag;
+    const size_t smem = sizeof(double) * n * 2 * n;
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_matrix_build_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+    pe_matrix_build_kernel<<<L, 256, smem>>>(b);
+    DINO_TRY(check_launch("pe_matrix_build"));
+    int flag = 0;
+    DINO_CHECK_CUDA(cudaMemcpy(&flag, pe->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    DINO_REQUIRE(flag == 0, DINO_ERR_NAN,
+                 "implicit matrix is singular or its inverse is not finite");
+    return DINO_OK;
+  };
+  const int rc = build();
+  cudaFree(dc);
+  if (rc != DINO_OK) {
+    cudaFree(m.d);
+    return rc;
   }
-  pe->inv_cache.push_back({eta, d_inv});
-  *out = d_inv;
+  pe->mat_cache.push_back(std::move(m));
+  *out = &pe->mat_cache.back();
   return DINO_OK;
 }
 
@@ -1097,39 +1146,35 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
 //   Y2 = (1 - dt/3 G)^-1 (y + dt/6 f0 + dt/2 f1 + dt/3 g0),  f2 = F(Y2), g2 = G(Y2)
 //   Y3* = y + dt/2 f0 - dt/2 f1 + dt f2 + 3dt/8 g0 + 3dt/8 g2
 //   y_next = filter(Y3* + dt/4 G((1 - dt/4 G)^-1 Y3*))
-// Each stage is one elementwise combine plus one per-(m, l) solve.
+// Each stage is one elementwise combine plus one per-l operator product.
+struct StepMats {
+  const MatEntry* L;      // G
+  const MatEntry* inv1;   // (1 - dt/6 G)^-1
+  const MatEntry* invg2;  // (1 - dt/3 G)^-1 and G of the result
+  const MatEntry* fin3;   // filter (1 + dt/4 G (1 - dt/4 G)^-1)
+};
+
+static int get_step_mats(dino_pe* pe, double dt, const double* host_filter,
+                         StepMats* m) {
+  DINO_TRY(get_matrix(pe, kMatL, 0.0, nullptr, &m->L));
+  DINO_TRY(get_matrix(pe, kMatInv, dt / 6.0, nullptr, &m->inv1));
+  DINO_TRY(get_matrix(pe, kMatInvG, dt / 3.0, nullptr, &m->invg2));
+  DINO_TRY(get_matrix(pe, kMatFinal, dt / 4.0, host_filter, &m->fin3));
+  return DINO_OK;
+}
+
 static int pe_step_once(dino_pe* pe, float* y, double dt, const float* filt,
-                        const float* inv1, const float* inv2, const float* inv3,
-                        cudaStream_t st) {
+                        const StepMats& m, cudaStream_t st) {
   DINO_TRY(pe_explicit_impl(pe, y, pe->d_f[0], st));
-  {
-    SolveArgs a = base_solve(pe);
-    a.src = y;
-    a.mode = 1;
-    a.out = pe->d_g[0];
-    DINO_TRY(launch_solve(pe, a, st));
-  }
+  DINO_TRY(launch_apply(pe, m.L, y, pe->d_g[0], nullptr, st));
   DINO_TRY(launch_combine(pe, y, {{(float)(dt / 3.0), pe->d_f[0]}},
                           {{(float)(dt / 6.0), pe->d_g[0]}}, nullptr, pe->d_Y, st));
-  {
-    SolveArgs a = base_solve(pe);
-    a.src = pe->d_ystar;
-    a.inv = inv1;
-    a.out = pe->d_Y;
-    DINO_TRY(launch_solve(pe, a, st));
-  }
+  DINO_TRY(launch_apply(pe, m.inv1, pe->d_ystar, pe->d_Y, nullptr, st));
   DINO_TRY(pe_explicit_impl(pe, pe->d_Y, pe->d_f[1], st));
   DINO_TRY(launch_combine(
       pe, y, {{(float)(dt / 6.0), pe->d_f[0]}, {(float)(dt * 0.5), pe->d_f[1]}},
       {{(float)(dt / 3.0), pe->d_g[0]}}, nullptr, pe->d_Y, st));
-  {
-    SolveArgs a = base_solve(pe);
-    a.src = pe->d_ystar;
-    a.inv = inv2;
-    a.g_out = pe->d_g[1];
-    a.out = pe->d_Y;
-    DINO_TRY(launch_solve(pe, a, st));
-  }
+  DINO_TRY(launch_apply(pe, m.invg2, pe->d_ystar, pe->d_Y, pe->d_g[1], st));
   DINO_TRY(pe_explicit_impl(pe, pe->d_Y, pe->d_f[2], st));
   DINO_TRY(launch_combine(
       pe, y,
@@ -1137,16 +1182,7 @@ static int pe_step_once(dino_pe* pe, float* y, double dt, const float* filt,
        {(float)dt, pe->d_f[2]}},
       {{(float)(dt * 0.375), pe->d_g[0]}, {(float)(dt * 0.375), pe->d_g[1]}},
       filt, y, st));
-  {
-    SolveArgs a = base_solve(pe);
-    a.src = pe->d_ystar;
-    a.inv = inv3;
-    a.use_final = 1;
-    a.final_c = (float)(dt * 0.25);
-    a.filter = filt;
-    a.out = y;
-    DINO_TRY(launch_solve(pe, a, st));
-  }
+  DINO_TRY(launch_apply(pe, m.fin3, pe->d_ystar, y, nullptr, st));
   return DINO_OK;
 }
 
@@ -1162,11 +1198,10 @@ static void pe_free(dino_pe* pe) {
   if (!pe) return;
   if (pe->graph.exec) cudaGraphExecDestroy(pe->graph.exec);
   if (pe->graph.graph) cudaGraphDestroy(pe->graph.graph);
-  for (auto& e : pe->inv_cache) cudaFree(e.d_inv);
+  for (auto& e : pe->mat_cache) cudaFree(e.d);
   for (auto& e : pe->filter_cache) cudaFree(e.d_filter);
   cudaFree(pe->d_lev);
   cudaFree(pe->d_lat);
-  cudaFree(pe->d_mat);
   cudaFree(pe->d_orog);
   cudaFree(pe->d_aux);
   cudaFree(pe->d_nodal);
@@ -1231,14 +1266,6 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
     lat[3 * J + j] = (float)(std::cos(latr) * std::cos(latr));
   }
   DINO_TRY(upload_vec(&pe->d_lat, lat));
-  // Padded G and H.
-  std::vector<float> mat(2 * pe->KM * pe->KM, 0.f);
-  for (int r = 0; r < K; ++r)
-    for (int c = 0; c < K; ++c) {
-      mat[r * pe->KM + c] = (float)pe->G[r * K + c];
-      mat[pe->KM * pe->KM + r * pe->KM + c] = (float)pe->H[r * K + c];
-    }
-  DINO_TRY(upload_vec(&pe->d_mat, mat));
   {
     std::vector<float> orog(pe->ML, 0.f);
     if (d->orography_modal) std::memcpy(orog.data(), d->orography_modal, sizeof(float) * pe->ML);
@@ -1333,7 +1360,6 @@ int dino_pe_create(dino_plan* plan, const dino_pe_desc* d, dino_pe** out) {
   pe->hum = d->humidity_tracer;
   pe->vadv = d->include_vertical_advection ? 1 : 0;
   pe->hs = d->held_suarez ? 1 : 0;
-  pe->KM = pe->K <= 8 ? 8 : pe->K <= 16 ? 16 : pe->K <= 24 ? 24 : pe->K <= 32 ? 32 : 48;
   pe->M = plan->M;
   pe->L = plan->L;
   pe->I = plan->I;
@@ -1386,19 +1412,17 @@ int dino_pe_implicit(dino_pe* pe, const float* state, float* out, void* stream) 
   cudaStream_t st = (cudaStream_t)stream;
   // Vorticity and tracers have no implicit terms.
   DINO_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * pe->n_state * pe->ML, st));
-  SolveArgs a = base_solve(pe);
-  a.src = state;
-  a.mode = 1;
-  a.out = out;
-  return launch_solve(pe, a, st);
+  const MatEntry* m = nullptr;
+  DINO_TRY(get_matrix(pe, kMatL, 0.0, nullptr, &m));
+  return launch_apply(pe, m, state, out, nullptr, st);
 }
 
 int dino_pe_implicit_inverse(dino_pe* pe, const float* state, float* out,
                              double eta, void* stream) {
   DINO_REQUIRE(pe && state && out, DINO_ERR_ARG, "dino_pe_implicit_inverse: null argument");
   DINO_REQUIRE(std::isfinite(eta), DINO_ERR_ARG, "step_size must be finite");
-  const float* inv = nullptr;
-  DINO_TRY(get_inverse(pe, eta, &inv));
+  const MatEntry* m = nullptr;
+  DINO_TRY(get_matrix(pe, kMatInv, eta, nullptr, &m));
   cudaStream_t st = (cudaStream_t)stream;
   if (out != state) {
     // Vorticity and tracer planes pass through unchanged.
@@ -1410,25 +1434,19 @@ int dino_pe_implicit_inverse(dino_pe* pe, const float* state, float* out,
                                       sizeof(float) * pe->nT * mK * pe->ML,
                                       cudaMemcpyDeviceToDevice, st));
   }
-  SolveArgs a = base_solve(pe);
-  a.src = state;
-  a.inv = inv;
-  a.out = out;
-  return launch_solve(pe, a, st);
+  return launch_apply(pe, m, state, out, nullptr, st);
 }
 
 int dino_pe_step(dino_pe* pe, float* state, double dt, const double* host_filter,
                  int32_t n_steps, void* stream) {
   DINO_REQUIRE(pe && state, DINO_ERR_ARG, "dino_pe_step: null argument");
   DINO_REQUIRE(n_steps >= 0, DINO_ERR_ARG, "n_steps must be >= 0");
-  const float *i1, *i2, *i3;
-  DINO_TRY(get_inverse(pe, dt / 6.0, &i1));
-  DINO_TRY(get_inverse(pe, dt / 3.0, &i2));
-  DINO_TRY(get_inverse(pe, dt / 4.0, &i3));
+  StepMats mats;
+  DINO_TRY(get_step_mats(pe, dt, host_filter, &mats));
   float* filt = nullptr;
   DINO_TRY(get_filter(pe, host_filter, &filt));
   for (int s = 0; s < n_steps; ++s)
-    DINO_TRY(pe_step_once(pe, state, dt, filt, i1, i2, i3, (cudaStream_t)stream));
+    DINO_TRY(pe_step_once(pe, state, dt, filt, mats, (cudaStream_t)stream));
   return DINO_OK;
 }
 
@@ -1438,10 +1456,8 @@ int dino_pe_step_graph(dino_pe* pe, float* state, double dt,
   DINO_REQUIRE(pe && state, DINO_ERR_ARG, "dino_pe_step_graph: null argument");
   DINO_REQUIRE(n_steps >= 0, DINO_ERR_ARG, "n_steps must be >= 0");
   cudaStream_t st = (cudaStream_t)stream;
-  const float *i1, *i2, *i3;
-  DINO_TRY(get_inverse(pe, dt / 6.0, &i1));
-  DINO_TRY(get_inverse(pe, dt / 3.0, &i2));
-  DINO_TRY(get_inverse(pe, dt / 4.0, &i3));
+  StepMats mats;
+  DINO_TRY(get_step_mats(pe, dt, host_filter, &mats));
   float* filt = nullptr;
   DINO_TRY(get_filter(pe, host_filter, &filt));
   GraphEntry& g = pe->graph;
@@ -1450,13 +1466,13 @@ int dino_pe_step_graph(dino_pe* pe, float* state, double dt,
     if (g.graph) cudaGraphDestroy(g.graph);
     g = GraphEntry{};
     DINO_TRY(sht_prepare(pe->plan));
-    DINO_TRY(launch_solve_n(pe->KM, nullptr, SolveArgs{}, st));
+    DINO_TRY(prepare_apply());
     // Capture on a private stream so that the caller's stream (possibly the
     // legacy default stream) is never put in capture mode.
     cudaStream_t cap;
     DINO_CHECK_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     DINO_CHECK_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-    int rc = pe_step_once(pe, state, dt, filt, i1, i2, i3, cap);
+    int rc = pe_step_once(pe, state, dt, filt, mats, cap);
     cudaGraph_t graph = nullptr;
     cudaError_t ce = cudaStreamEndCapture(cap, &graph);
     cudaStreamDestroy(cap);
