@@ -120,6 +120,12 @@ SIGNATURES = {
     'dino_pe_step': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32, _vp]),
     'dino_pe_step_graph': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32,
                                           _vp]),
+    'dino_pe_explicit_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    'dino_pe_implicit_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    'dino_pe_implicit_inverse_vjp': (ctypes.c_int, [_vp, _vp, _vp,
+                                                    ctypes.c_double, _vp]),
+    'dino_pe_step_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double,
+                                        _DP, _vp]),
 }
 
 

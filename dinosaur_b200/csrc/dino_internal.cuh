@@ -122,6 +122,10 @@ int sht_inverse_segs(dino_plan* p, const Segs& in, float* out_nodal, int nfields
                      float* work, int work_fields, cudaStream_t st);
 int sht_forward_to(dino_plan* p, const float* nodal, float* out_modal,
                    int nfields, float* work, int work_fields, cudaStream_t st);
+int sht_inverse_adjoint_to(dino_plan* p, const float* nodal_ct, float* modal_ct,
+                           int nfields, float* work, int work_fields, cudaStream_t st);
+int sht_forward_adjoint_to(dino_plan* p, const float* modal_ct, float* nodal_ct,
+                           int nfields, float* work, int work_fields, cudaStream_t st);
 int legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
                      int nfields, cudaStream_t st);
 int legendre_forward(dino_plan* p, const float* fourier, float* out_modal,

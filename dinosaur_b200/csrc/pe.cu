@@ -34,8 +34,9 @@ struct MatEntry {
   int kind = 0;
   double eta = 0;
   std::vector<double> filter;  // folded-in step filter (kMatFinal), else empty
-  float* d = nullptr;          // [L][n][RP], transposed, rows zero-padded
-  int R = 0, RP = 0;
+  bool transposed = false;     // the transpose of the operator of `kind`
+  float* d = nullptr;          // [L][nin][RP]: operator^T, rows zero-padded
+  int R = 0, nin = 0, RP = 0;  // rows, columns (inputs), padded rows
 };
 
 struct FilterCacheEntry {
@@ -85,6 +86,10 @@ struct dino_pe {
   float* d_g[2] = {nullptr, nullptr};
   float* d_Y = nullptr;
   float* d_ystar = nullptr;  // Y* of the current stage (implicit planes)
+  // Adjoint work (allocated by the first VJP call).
+  float* d_xbar_n = nullptr;  // nodal cotangents, n_inv planes
+  float* d_xbar_m = nullptr;  // their modal adjoint, n_inv planes
+  float* d_adj[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int* d_flag = nullptr;
   std::deque<dino::MatEntry> mat_cache;  // stable element addresses
   std::vector<dino::FilterCacheEntry> filter_cache;
@@ -488,6 +493,445 @@ __global__ void pe_post_kernel(PostArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Adjoint of the explicit terms (the VJP of explicit_terms,
+// primitive_equations.py:1126-1194): the transposed post-pass, the forward
+// transform's adjoint, the VJP of the nodal column kernel (recomputing its
+// inputs), the inverse transform's adjoint and the transposed pre-pass.
+// ---------------------------------------------------------------------------
+
+// Transposed cos_lat_d_dlat (tab 0) / sec_lat_d_dlat_cos2 (tab 2) at (row, l)
+// of a plane y whose entries at l >= lclip count as zero:
+//   (D^T y)[l] = ta[l] y[l-1] + tb[l] y[l+1].
+__device__ __forceinline__ float dlat_t_at(const float* y, int row, int l, int L,
+                                           int lclip, int lw, const float* deriv,
+                                           int tab) {
+  const int m = (row + 1) >> 1;
+  const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
+  const float* tb = ta + (size_t)lw * L;
+  const float* yr = y + (size_t)row * L;
+  float v = 0.f;
+  if (l >= 1 && l - 1 < lclip) v += ta[l] * yr[l - 1];
+  if (l + 1 < lclip) v += tb[l] * yr[l + 1];
+  return v;
+}
+
+// Transposed post-pass: tendency cotangents (packed state layout) ->
+// cotangents of the forward-transform outputs.  d/dlon is antisymmetric
+// (its transpose is -d/dlon); the top total wavenumber of every clipped
+// tendency has a zero cotangent.
+struct PostAdjArgs {
+  const float* tbar;
+  float* fbar;
+  int K, mem, nT, hum, hs;
+  int M, L, lw;
+  int o_Au, o_Av, o_KE, o_uT, o_vT, o_Tn, o_tr, o_vh, o_gh, o_dh, o_hsT,
+      o_lnps;
+  int p_vort, p_div, p_temp, p_tr, p_lnps;
+  const float* deriv;
+  const float* lap;
+  float inv_radius;
+};
+
+__global__ void pe_post_adjoint_kernel(PostAdjArgs a) {
+  const size_t ML = (size_t)a.M * a.L;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ML) return;
+  const int l = idx % a.L, row = idx / a.L;
+  const int k = blockIdx.y, mb = blockIdx.z, K = a.K;
+  const int Lc = a.L - 1;
+  const bool keep = l < Lc;
+  const float ir = a.inv_radius;
+  const float lam = a.lap[l];
+#define TB(p) (a.tbar + pl(p, mb, K, k) * ML)
+#define FB(p) a.fbar[pl(p, mb, K, k) * ML + idx]
+  const float* vb = TB(a.p_vort);
+  const float* db = TB(a.p_div);
+  const float* Tb = TB(a.p_temp);
+  const float vc = keep ? vb[idx] : 0.f;
+  const float dc = keep ? db[idx] : 0.f;
+  const float Tc = keep ? Tb[idx] : 0.f;
+  const float dlon_v = keep ? d_dlon_at(vb, row, l, a.L) : 0.f;
+  const float dlon_d = keep ? d_dlon_at(db, row, l, a.L) : 0.f;
+  const float dlon_T = keep ? d_dlon_at(Tb, row, l, a.L) : 0.f;
+  FB(a.o_Au) = (dlat_t_at(vb, row, l, a.L, Lc, a.lw, a.deriv, 2) + dlon_d) * ir;
+  FB(a.o_Av) = (dlon_v - dlat_t_at(db, row, l, a.L, Lc, a.lw, a.deriv, 2)) * ir;
+  FB(a.o_KE) = -lam * dc;
+  if (a.hum >= 0) {
+    FB(a.o_vh) = vc;
+    FB(a.o_gh) = -lam * dc;
+    FB(a.o_dh) = -dc;
+  }
+  FB(a.o_Tn) = Tc;
+  FB(a.o_uT) = dlon_T * ir;
+  FB(a.o_vT) = -dlat_t_at(Tb, row, l, a.L, Lc, a.lw, a.deriv, 2) * ir;
+  if (a.hs) FB(a.o_hsT) = Tb[idx];
+  for (int t = 0; t < a.nT; ++t) {
+    const int ob = a.o_tr + 3 * t * a.mem * K;
+    const float* qb = TB(a.p_tr + t * a.mem * K);
+    FB(ob) = (keep ? d_dlon_at(qb, row, l, a.L) : 0.f) * ir;
+    FB(ob + a.mem * K) = -dlat_t_at(qb, row, l, a.L, Lc, a.lw, a.deriv, 2) * ir;
+    FB(ob + 2 * a.mem * K) = keep ? qb[idx] : 0.f;
+  }
+  if (k == 0)
+    a.fbar[((size_t)a.o_lnps + mb) * ML + idx] =
+        keep ? a.tbar[((size_t)a.p_lnps + mb) * ML + idx] : 0.f;
+#undef TB
+#undef FB
+}
+
+// VJP of pe_nodal_kernel for one column.  Pass 0 forms the column totals;
+// pass 1 runs bottom-up with a (k, k+1) window: each half level k+1/2 takes
+// the cotangents of the centred vertical advection of u, v, T' and the
+// tracers (and of the reference-temperature term), and the cumulative sigma
+// sums become suffix sums of their cotangents; pass 2 adds the cotangents of
+// the column totals, which reach every level.
+struct NodalAdjArgs {
+  NodalArgs f;        // forward arguments; f.nod holds the forward inputs
+  const float* fbar;  // cotangents of the nodal outputs (forward-input layout)
+  float* xbar;        // cotangents of the nodal inputs (nodal-buffer layout)
+};
+
+__global__ void __launch_bounds__(128) pe_nodal_adjoint_kernel(NodalAdjArgs A) {
+  const NodalArgs& a = A.f;
+  const size_t IJ = (size_t)a.I * a.J;
+  const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= IJ) return;
+  const int mb = blockIdx.y;
+  const int K = a.K;
+  const int j = col % a.J;
+  const float sec2 = a.lat[j];
+  const float fcor = a.lat[a.J + j];
+  const float* dsig = a.lev + a.lo.dsig;
+  const float* c2ci = a.lev + a.lo.c2ci;
+  const float* alpha = a.lev + a.lo.alpha;
+  const float* tref = a.lev + a.lo.tref;
+  const float* sumsig = a.lev + a.lo.sumsig;
+  const float* trd = a.lev + a.lo.trefdiff;
+  const float* nod = a.nod;
+  const float* fb = A.fbar;
+  float* xb = A.xbar;
+#define NOD(p, k) nod[pl(p, mb, K, k) * IJ + col]
+#define FB(p, k) fb[pl(p, mb, K, k) * IJ + col]
+#define XB(p, k) xb[pl(p, mb, K, k) * IJ + col]
+  const bool moist = a.hum >= 0;
+  const float gx = nod[((size_t)a.p_gx + mb) * IJ + col];
+  const float gy = nod[((size_t)a.p_gy + mb) * IJ + col];
+  const float ra = a.Rv_over_R - 1.f;
+  const float rb = a.Cpv_over_Cp - 1.f;
+  const float rc = a.Rv_over_R - a.Cpv_over_Cp;
+  const float kap = a.kappa;
+
+  // Pass 0: column totals.
+  float Fe = 0.f, Ff = 0.f, Su = 0.f, Sv = 0.f, Gh = 0.f;
+  for (int k = 0; k < K; ++k) {
+    const float u = NOD(a.p_u, k), v = NOD(a.p_v, k), d = NOD(a.p_div, k);
+    const float ugl = (u * gx + v * gy) * sec2;
+    Fe += ugl * dsig[k];
+    Ff += (d + ugl) * dsig[k];
+    Su += u * dsig[k];
+    Sv += v * dsig[k];
+    if (moist) Gh += FB(a.o_gh, k);
+  }
+  float laplnps = 0.f;
+  if (moist) laplnps = nod[((size_t)a.p_laplnps + mb) * IJ + col];
+  float hs_ps = 0.f, sin2 = 0.f, cos2 = 0.f;
+  if (a.hs) {
+    hs_ps = expf(nod[((size_t)a.p_lnps + mb) * IJ + col]);
+    sin2 = a.lat[2 * a.J + j];
+    cos2 = a.lat[3 * a.J + j];
+  }
+
+  float gxb = 0.f, gyb = 0.f, laplnpsb = 0.f, lnpsb = 0.f;
+  float Feb = -fb[((size_t)a.o_lnps + mb) * IJ + col], Ffb = 0.f;
+  // Window: values of level k+1.
+  float u_n = 0.f, v_n = 0.f, T_n = 0.f;
+  float Vu_n = 0.f, Vv_n = 0.f, VT_n = 0.f, Tnb_n = 0.f;
+  float ub_n = 0.f, vb_n = 0.f, Tb_n = 0.f;
+  float q_n[kMaxTracers], Vq_n[kMaxTracers], qb_n[kMaxTracers];
+#pragma unroll
+  for (int t = 0; t < kMaxTracers; ++t) q_n[t] = Vq_n[t] = qb_n[t] = 0.f;
+  float carry_fe = 0.f, carry_ff = 0.f;  // from ge/gf of level k+1
+  float Se = 0.f, Sf = 0.f, SGh = 0.f;   // suffix sums
+  float fe = Fe, ff = Ff;                // prefix sums through level k
+
+  for (int k = K - 1; k >= 0; --k) {
+    const bool has_next = k + 1 < K;
+    const float u = NOD(a.p_u, k), v = NOD(a.p_v, k), d = NOD(a.p_div, k);
+    const float z = NOD(a.p_vort, k), T = NOD(a.p_temp, k);
+    float q[kMaxTracers];
+    float q_h = 0.f;
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t) {
+      q[t] = (t < a.nT) ? NOD(a.p_tr + t * a.mem * K, k) : 0.f;
+      if (t == a.hum) q_h = q[t];
+    }
+    const float ugl = (u * gx + v * gy) * sec2;
+    const float fe_k = fe, ff_k = ff;
+    const float fe_km = fe_k - ugl * dsig[k];
+    const float ff_km = ff_k - (d + ugl) * dsig[k];
+    const float inv_ds = 1.f / dsig[k];
+
+    const float Aub = FB(a.o_Au, k), Avb = FB(a.o_Av, k), KEb = FB(a.o_KE, k);
+    const float uTb = FB(a.o_uT, k), vTb = FB(a.o_vT, k), Tnb = FB(a.o_Tn, k);
+    const float adj = moist ? 1.f + ra * q_h : 1.f;
+    const float rt = a.R * T * adj;
+    const float tv = z + fcor;
+    const float zb = sec2 * (-v * Aub + u * Avb);
+    float ub = tv * sec2 * Avb + u * sec2 * KEb + T * sec2 * uTb;
+    float vb = -tv * sec2 * Aub + v * sec2 * KEb + T * sec2 * vTb;
+    if (a.hs) {
+      const float kv = a.lev[a.lo.kv + k];
+      ub += kv * sec2 * Aub;
+      vb += kv * sec2 * Avb;
+    }
+    const float rtb = sec2 * (gx * Aub + gy * Avb);
+    float Tb = a.R * adj * rtb + u * sec2 * uTb + v * sec2 * vTb + d * Tnb;
+    float qhb = moist ? a.R * T * ra * rtb : 0.f;
+    gxb += rt * sec2 * Aub;
+    gyb += rt * sec2 * Avb;
+    float db = T * Tnb;
+    // Adiabatic term kappa (Tref (ugl - ge) + P (ugl - gf)).
+    const float gf = (alpha[k] * ff_k + (k > 0 ? alpha[k - 1] * ff_km : 0.f)) * inv_ds;
+    float uglb = kap * tref[k] * Tnb;
+    const float geb = -kap * tref[k] * Tnb;
+    float gfb;
+    if (!moist) {
+      Tb += kap * (ugl - gf) * Tnb;
+      uglb += kap * T * Tnb;
+      gfb = -kap * T * Tnb;
+    } else {
+      const float den = 1.f + rb * q_h;
+      const float P = (T * (1.f + ra * q_h) + tref[k] * rc * q_h) / den;
+      Tb += kap * (ugl - gf) * Tnb * (1.f + ra * q_h) / den;
+      qhb += kap * (ugl - gf) * Tnb * (T * (ra - rb) + tref[k] * rc) / (den * den);
+      uglb += kap * P * Tnb;
+      gfb = -kap * P * Tnb;
+    }
+    // Tracers.
+    float qb[kMaxTracers], Vq[kMaxTracers];
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t) {
+      qb[t] = 0.f;
+      Vq[t] = 0.f;
+      if (t < a.nT) {
+        const int ob = a.o_tr + 3 * t * a.mem * K;
+        const float uqb = FB(ob, k), vqb = FB(ob + a.mem * K, k);
+        const float qnb = FB(ob + 2 * a.mem * K, k);
+        ub += q[t] * sec2 * uqb;
+        vb += q[t] * sec2 * vqb;
+        qb[t] = u * sec2 * uqb + v * sec2 * vqb + d * qnb;
+        db += q[t] * qnb;
+        Vq[t] = a.vadv ? qnb : 0.f;
+      }
+    }
+    if (moist) {
+      const float gqx = NOD(a.p_gqx, k), gqy = NOD(a.p_gqy, k);
+      const float vhb = FB(a.o_vh, k), dhb = FB(a.o_dh, k), ghb = FB(a.o_gh, k);
+      const float coef = tref[k] * a.Rv_minus_R;
+      gxb += coef * sec2 * (gqy * vhb + gqx * dhb);
+      gyb += coef * sec2 * (-gqx * vhb + gqy * dhb);
+      XB(a.p_gqx, k) = coef * sec2 * (-gy * vhb + gx * dhb);
+      XB(a.p_gqy, k) = coef * sec2 * (gx * vhb + gy * dhb);
+      qhb += laplnps * coef * dhb;
+      laplnpsb += q_h * coef * dhb;
+      // Geopotential of the virtual-temperature difference.
+      SGh += ghb;
+      const float above = Gh - SGh;  // sum of the cotangents of levels < k
+      const float tdb = a.R * alpha[k] * ghb +
+                        (k > 0 ? a.R * (alpha[k] + alpha[k - 1]) * above : 0.f);
+      qhb += (T + tref[k]) * ra * tdb;
+      Tb += q_h * ra * tdb;
+#pragma unroll
+      for (int t = 0; t < kMaxTracers; ++t)
+        if (t == a.hum) qb[t] += qhb;
+    }
+    if (a.hs) {
+      const float hsTb = FB(a.o_hsT, k);
+      const float sig = a.lev[a.lo.sigma + k];
+      const float cutoff = fmaxf(0.f, (sig - a.hs_sigma_b) / (1.f - a.hs_sigma_b));
+      const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (cutoff * cos2 * cos2);
+      const float pp0 = sig * hs_ps / a.hs_p0;
+      const float pk = powf(pp0, kap);
+      const float B = a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * logf(pp0) * cos2;
+      Tb += -kt * hsTb;
+      if (pk * B > a.hs_minT) lnpsb += kt * hsTb * pk * (kap * B - a.hs_dThz * cos2);
+    }
+    const float Vu = a.vadv ? -sec2 * Aub : 0.f;
+    const float Vv = a.vadv ? -sec2 * Avb : 0.f;
+    const float VT = a.vadv ? Tnb : 0.f;
+    float fe_b = alpha[k] * inv_ds * geb + carry_fe;
+    float ff_b = alpha[k] * inv_ds * gfb + carry_ff;
+    if (has_next) {
+      // Half level k+1/2.
+      const float c = c2ci[k];
+      if (a.vadv) {
+        const float wf = sumsig[k] * Ff - ff_k;
+        float wfb = 0.f;
+        auto half = [&](float xc, float xn, float Vc, float Vn, float& xbc, float& xbn) {
+          const float vs = Vc + Vn;
+          wfb += -0.5f * c * (xn - xc) * vs;
+          const float Db = -0.5f * wf * vs;
+          xbn += c * Db;
+          xbc -= c * Db;
+        };
+        half(u, u_n, Vu, Vu_n, ub, ub_n);
+        half(v, v_n, Vv, Vv_n, vb, vb_n);
+        half(T, T_n, VT, VT_n, Tb, Tb_n);
+#pragma unroll
+        for (int t = 0; t < kMaxTracers; ++t)
+          if (t < a.nT) half(q[t], q_n[t], Vq[t], Vq_n[t], qb[t], qb_n[t]);
+        ff_b -= wfb;
+        Ffb += sumsig[k] * wfb;
+      }
+      if (a.tref_varies) {
+        const float web = -0.5f * trd[k] * (Tnb + Tnb_n);
+        fe_b -= web;
+        Feb += sumsig[k] * web;
+      }
+      // Level k+1 has all its contributions.
+      XB(a.p_u, k + 1) = ub_n;
+      XB(a.p_v, k + 1) = vb_n;
+      XB(a.p_temp, k + 1) = Tb_n;
+#pragma unroll
+      for (int t = 0; t < kMaxTracers; ++t)
+        if (t < a.nT) XB(a.p_tr + t * a.mem * K, k + 1) = qb_n[t];
+    }
+    Se += fe_b;
+    Sf += ff_b;
+    uglb += dsig[k] * (Se + Sf);
+    db += dsig[k] * Sf;
+    ub += gx * sec2 * uglb;
+    vb += gy * sec2 * uglb;
+    gxb += u * sec2 * uglb;
+    gyb += v * sec2 * uglb;
+    XB(a.p_vort, k) = zb;
+    XB(a.p_div, k) = db;
+    carry_fe = k > 0 ? alpha[k - 1] * inv_ds * geb : 0.f;
+    carry_ff = k > 0 ? alpha[k - 1] * inv_ds * gfb : 0.f;
+    u_n = u; v_n = v; T_n = T;
+    Vu_n = Vu; Vv_n = Vv; VT_n = VT; Tnb_n = Tnb;
+    ub_n = ub; vb_n = vb; Tb_n = Tb;
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t) {
+      q_n[t] = q[t];
+      Vq_n[t] = Vq[t];
+      qb_n[t] = qb[t];
+    }
+    fe = fe_km;
+    ff = ff_km;
+  }
+  XB(a.p_u, 0) = ub_n;
+  XB(a.p_v, 0) = vb_n;
+  XB(a.p_temp, 0) = Tb_n;
+#pragma unroll
+  for (int t = 0; t < kMaxTracers; ++t)
+    if (t < a.nT) XB(a.p_tr + t * a.mem * K, 0) = qb_n[t];
+
+  // Pass 2: cotangents of the column totals.
+  const float Ftb = Feb + Ffb;
+  for (int k = 0; k < K; ++k) {
+    XB(a.p_u, k) += gx * sec2 * dsig[k] * Ftb;
+    XB(a.p_v, k) += gy * sec2 * dsig[k] * Ftb;
+    XB(a.p_div, k) += dsig[k] * Ffb;
+  }
+  gxb += sec2 * Ftb * Su;
+  gyb += sec2 * Ftb * Sv;
+  xb[((size_t)a.p_gx + mb) * IJ + col] = gxb;
+  xb[((size_t)a.p_gy + mb) * IJ + col] = gyb;
+  if (moist) xb[((size_t)a.p_laplnps + mb) * IJ + col] = laplnpsb;
+  if (a.hs) xb[((size_t)a.p_lnps + mb) * IJ + col] = lnpsb;
+#undef NOD
+#undef FB
+#undef XB
+}
+
+// Transposed pre-pass: modal cotangents of the inverse-transform inputs
+// (nodal-buffer plane order) -> cotangent of the packed state.
+struct PrepAdjArgs {
+  const float* xbar;
+  float* sbar;
+  int K, mem, nT, hum, hs;
+  int M, L, lw;
+  int p_u, p_v, p_gqx, p_gqy, p_gx, p_gy, p_laplnps, p_lnps;
+  int s_lnps;
+  const float* deriv;
+  const float* lap;
+  const float* invlap;
+  float inv_radius;
+};
+
+__global__ void pe_prep_adjoint_kernel(PrepAdjArgs a) {
+  const size_t ML = (size_t)a.M * a.L;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ML) return;
+  const int l = idx % a.L, row = idx / a.L;
+  const int k = blockIdx.y, mb = blockIdx.z, K = a.K;
+  const int mK = a.mem * K;
+  const float ir = a.inv_radius;
+  const float* ub = a.xbar + pl(a.p_u, mb, K, k) * ML;
+  const float* vb = a.xbar + pl(a.p_v, mb, K, k) * ML;
+  const float s = a.invlap[l] * ir;
+  const size_t pz = pl(0, mb, K, k) * ML + idx;
+  a.sbar[pz] = a.xbar[pz] + s * (-dlat_t_at(ub, row, l, a.L, a.L, a.lw, a.deriv, 0) -
+                                 d_dlon_at(vb, row, l, a.L));
+  const size_t pd = pl(mK, mb, K, k) * ML + idx;
+  a.sbar[pd] = a.xbar[pd] + s * (-d_dlon_at(ub, row, l, a.L) +
+                                 dlat_t_at(vb, row, l, a.L, a.L, a.lw, a.deriv, 0));
+  const size_t pt = pl(2 * mK, mb, K, k) * ML + idx;
+  a.sbar[pt] = a.xbar[pt];
+  for (int t = 0; t < a.nT; ++t) {
+    const size_t pq = pl((3 + t) * mK, mb, K, k) * ML + idx;
+    float v = a.xbar[pq];
+    if (t == a.hum) {
+      const float* gqxb = a.xbar + pl(a.p_gqx, mb, K, k) * ML;
+      const float* gqyb = a.xbar + pl(a.p_gqy, mb, K, k) * ML;
+      v += ir * (-d_dlon_at(gqxb, row, l, a.L) +
+                 dlat_t_at(gqyb, row, l, a.L, a.L, a.lw, a.deriv, 0));
+    }
+    a.sbar[pq] = v;
+  }
+  if (k != 0) return;
+  const float* gxb = a.xbar + ((size_t)a.p_gx + mb) * ML;
+  const float* gyb = a.xbar + ((size_t)a.p_gy + mb) * ML;
+  float v = a.hs ? a.xbar[((size_t)a.p_lnps + mb) * ML + idx] : 0.f;
+  v += ir * (-d_dlon_at(gxb, row, l, a.L) +
+             dlat_t_at(gyb, row, l, a.L, a.L, a.lw, a.deriv, 0));
+  if (a.hum >= 0) v += a.lap[l] * a.xbar[((size_t)a.p_laplnps + mb) * ML + idx];
+  a.sbar[((size_t)a.s_lnps + mb) * ML + idx] = v;
+}
+
+// out = sum_t c_t x_t over the packed state, with coefficients ci on the
+// implicit planes (div, T', ln ps) and ce on the others; `filt` (per l)
+// scales the result on the other planes; `only` restricts the planes written
+// (0: all, 1: implicit, 2: others).
+struct LinCombArgs {
+  const float* x[6];
+  float ci[6], ce[6];
+  int nx;
+  const float* filt;
+  float* out;
+  int mK, nT, L, only;
+  size_t ML;
+};
+
+__global__ void pe_lincomb_kernel(LinCombArgs a) {
+  const int plane = blockIdx.y;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.ML) return;
+  const bool imp = (plane >= a.mK && plane < 3 * a.mK) || plane >= (3 + a.nT) * a.mK;
+  if ((a.only == 1 && !imp) || (a.only == 2 && imp)) return;
+  const size_t p = (size_t)plane * a.ML + idx;
+  float v = 0.f;
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    const float c = imp ? a.ci[t] : a.ce[t];
+    if (t < a.nx && c != 0.f) v = fmaf(c, a.x[t][p], v);
+  }
+  if (!imp && a.filt) v *= a.filt[idx % a.L];
+  a.out[p] = v;
+}
+
+// ---------------------------------------------------------------------------
 // Per-l operators of the implicit part, composed in FP64 on the GPU.
 //
 // On the stacked vector (div[K], T'[K], ln ps) of total wavenumber l the
@@ -513,7 +957,7 @@ enum MatKind { kMatL = 0, kMatInv = 1, kMatInvG = 2, kMatFinal = 3 };
 constexpr int kMaxLevels = 48;
 
 struct MatBuildArgs {
-  int K, kind, RP;
+  int K, kind, RP, nin, transposed;
   double eta, R;
   const double* G;       // K x K
   const double* H;       // K x K
@@ -534,7 +978,7 @@ __global__ void pe_matrix_build_kernel(MatBuildArgs a) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const double lm = a.lam[l];
   const double eta = a.eta;
-  float* o = a.out + (size_t)l * n * a.RP;
+  float* o = a.out + (size_t)l * a.nin * a.RP;
   auto Lrc = [&](int r, int c) -> double {
     if (r < K) {
       if (c < K) return 0.0;
@@ -545,9 +989,9 @@ __global__ void pe_matrix_build_kernel(MatBuildArgs a) {
     return c < K ? -a.dsig[c] : 0.0;
   };
   if (a.kind == kMatL) {
-    for (int e = tid; e < n * a.RP; e += nt) {
+    for (int e = tid; e < a.nin * a.RP; e += nt) {
       const int c = e / a.RP, r = e - c * a.RP;
-      o[e] = r < n ? (float)Lrc(r, c) : 0.f;
+      o[e] = r < n ? (float)(a.transposed ? Lrc(c, r) : Lrc(r, c)) : 0.f;
     }
     return;
   }
@@ -606,16 +1050,20 @@ __global__ void pe_matrix_build_kernel(MatBuildArgs a) {
     return -s;
   };
   const double f = a.filter ? a.filter[l] : 1.0;
-  for (int e = tid; e < n * a.RP; e += nt) {
+  // Entry (r, c) of the operator of `kind` (r < n, or r < 2n for kMatInvG).
+  auto op = [&](int r, int c) -> double {
+    if (a.kind == kMatInv) return inv(r, c);
+    if (a.kind == kMatInvG) return r < n ? inv(r, c) : l_inv(r - n, c);
+    return f * (((r == c) ? 1.0 : 0.0) + eta * l_inv(r, c));
+  };
+  const int rows = a.kind == kMatInvG ? 2 * n : n;
+  for (int e = tid; e < a.nin * a.RP; e += nt) {
     const int c = e / a.RP, r = e - c * a.RP;
     double v = 0.0;
-    if (a.kind == kMatInv) {
-      if (r < n) v = inv(r, c);
-    } else if (a.kind == kMatInvG) {
-      if (r < n) v = inv(r, c);
-      else if (r < 2 * n) v = l_inv(r - n, c);
-    } else if (r < n) {
-      v = f * (((r == c) ? 1.0 : 0.0) + eta * l_inv(r, c));
+    if (a.transposed) {
+      if (r < n && c < rows) v = op(c, r);
+    } else if (r < rows) {
+      v = op(r, c);
     }
     if (!isfinite(v)) atomicExch(a.flag, 2);
     o[e] = (float)v;
@@ -669,20 +1117,22 @@ __global__ void pe_combine_kernel(CombineArgs a) {
 }
 
 // Per-(l, column) application of an implicit operator: for every total
-// wavenumber l, Out[R x C] = A_l[R x n] Ys[n x C], where the C = members * M
+// wavenumber l, Out[R x C] = A_l[R x nin] Ys[nin x C], where the C = members * M
 // columns are the (member, m-row) pairs and Ys stacks the n = 2K+1 implicit
-// planes (div, T', ln ps).  A CTA takes one l, 64 columns and 16*TR rows of
+// planes (div, T', ln ps) of src (and, for nin = 2n, those of src2).  A CTA takes one l, 64 columns and 16*TR rows of
 // A_l: it stages A_l^T and the gathered Ys in shared memory and each thread
 // accumulates a TR x 4 register tile (broadcast A reads, float4 Ys reads).
 // Rows [0, n) go to `out`, rows [n, 2n) (kMatInvG) to `out2`.  Every element
 // is read and written by one CTA, with a barrier in between, so src may
 // alias out.
 struct ApplyArgs {
-  const float* src;
+  const float* src;   // inputs [0, n), scaled by s1
+  const float* src2;  // inputs [n, 2n) when nin = 2n, scaled by s2
+  float s1, s2;
   const float* A;
   float* out;
   float* out2;
-  int R, n, RP;
+  int R, n, nin, RP;
   int K, M, L, C;
   int p_div, p_temp, p_lnps;
   size_t ML;
@@ -701,30 +1151,42 @@ template <int TR>
 __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
   constexpr int RPT = 16 * TR;
   extern __shared__ __align__(16) float smem[];
-  const int n = a.n;
-  float* At = smem;                    // [n][RPT]
-  float* Ys = At + (size_t)n * RPT;    // [n][kApplyCols]
+  const int n = a.n, nin = a.nin;
+  float* At = smem;                    // [nin][RPT]
+  float* Ys = At + (size_t)nin * RPT;  // [nin][kApplyCols]
   const int tid = threadIdx.x;
   const int c0 = blockIdx.x * kApplyCols;
   const int l = blockIdx.y;
   const int r0 = blockIdx.z * RPT;
   {
-    const float* Ag = a.A + (size_t)l * n * a.RP + r0;
+    const float* Ag = a.A + (size_t)l * nin * a.RP + r0;
     constexpr int Q = RPT / 4;
-    for (int e = tid; e < n * Q; e += 256) {
+    for (int e = tid; e < nin * Q; e += 256) {
       const int k = e / Q, q = e - k * Q;
       reinterpret_cast<float4*>(At)[e] =
           reinterpret_cast<const float4*>(Ag + (size_t)k * a.RP)[q];
     }
   }
-  for (int e = tid; e < n * kApplyCols; e += 256) {
-    const int k = e / kApplyCols, c = c0 + (e % kApplyCols);
-    float v = 0.f;
-    if (c < a.C) {
-      const int mb = c / a.M, row = c - mb * a.M;
-      v = a.src[stacked_plane(a, k, mb) * a.ML + (size_t)row * a.L + l];
+  {
+    // Each thread gathers one column at every 4th stacked index; the column
+    // is decoded once and four loads are kept in flight.
+    constexpr int kLanes = 256 / kApplyCols;
+    const int cc = tid % kApplyCols, k0 = tid / kApplyCols;
+    const int c = c0 + cc;
+    const bool ok = c < a.C;
+    const int mb = ok ? c / a.M : 0;
+    const size_t off = (size_t)(ok ? c - mb * a.M : 0) * a.L + l;
+    const float* base = a.src + off;
+#pragma unroll 4
+    for (int k = k0; k < n; k += kLanes)
+      Ys[k * kApplyCols + cc] = ok ? a.s1 * base[stacked_plane(a, k, mb) * a.ML] : 0.f;
+    if (nin > n) {
+      const float* base2 = a.src2 + off;
+#pragma unroll 4
+      for (int k = k0; k < n; k += kLanes)
+        Ys[(n + k) * kApplyCols + cc] =
+            ok ? a.s2 * base2[stacked_plane(a, k, mb) * a.ML] : 0.f;
     }
-    Ys[e] = v;
   }
   __syncthreads();
   const int cg = tid & 15, rg = tid >> 4;
@@ -734,7 +1196,7 @@ __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
   const float* ar = At + rg * TR;
   const float4* yr = reinterpret_cast<const float4*>(Ys) + cg;
 #pragma unroll 2
-  for (int k = 0; k < n; ++k) {
+  for (int k = 0; k < nin; ++k) {
     const float4 y = yr[k * (kApplyCols / 4)];
 #pragma unroll
     for (int i = 0; i < TR; ++i) {
@@ -776,7 +1238,7 @@ template <int TR>
 static int apply_attr() {
   DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_apply_kernel<TR>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)apply_smem(2 * kMaxLevels + 1, TR)));
+                                       (int)apply_smem(2 * (2 * kMaxLevels + 1), TR)));
   return DINO_OK;
 }
 
@@ -808,14 +1270,19 @@ static void apply_launch(dim3 grid, size_t smem, cudaStream_t st, const ApplyArg
 }
 
 static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
-                        float* out, float* out2, cudaStream_t st) {
+                        float* out, float* out2, cudaStream_t st,
+                        const float* src2 = nullptr, float s1 = 1.f, float s2 = 1.f) {
   ApplyArgs a{};
   a.src = src;
+  a.src2 = src2;
+  a.s1 = s1;
+  a.s2 = s2;
   a.A = m->d;
   a.out = out;
   a.out2 = out2;
   a.R = m->R;
   a.n = 2 * pe->K + 1;
+  a.nin = m->nin;
   a.RP = m->RP;
   a.K = pe->K;
   a.M = pe->M;
@@ -828,7 +1295,7 @@ static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
   const int tr = apply_tr(m->R);
   const int rpt = 16 * tr;
   dim3 grid(ceil_div(a.C, kApplyCols), pe->L, ceil_div(m->R, rpt));
-  const size_t smem = apply_smem(a.n, tr);
+  const size_t smem = apply_smem(a.nin, tr);
   switch (tr) {
     case 1: apply_launch<1>(grid, smem, st, a); break;
     case 2: apply_launch<2>(grid, smem, st, a); break;
@@ -879,12 +1346,12 @@ static int launch_combine(dino_pe* pe, const float* y0,
 }
 
 static int get_matrix(dino_pe* pe, int kind, double eta, const double* host_filter,
-                      const MatEntry** out) {
+                      const MatEntry** out, bool transposed = false) {
   const int K = pe->K, L = pe->L, n = 2 * K + 1;
   if (kind == kMatL) eta = 0.0;
   if (kind != kMatFinal) host_filter = nullptr;
   for (auto& e : pe->mat_cache) {
-    if (e.kind != kind || e.eta != eta) continue;
+    if (e.kind != kind || e.eta != eta || e.transposed != transposed) continue;
     if (host_filter ? (e.filter.size() == (size_t)L &&
                        std::memcmp(e.filter.data(), host_filter, sizeof(double) * L) == 0)
                     : e.filter.empty()) {
@@ -898,7 +1365,9 @@ static int get_matrix(dino_pe* pe, int kind, double eta, const double* host_filt
   m.kind = kind;
   m.eta = eta;
   if (host_filter) m.filter.assign(host_filter, host_filter + L);
-  m.R = kind == kMatInvG ? 2 * n : n;
+  m.transposed = transposed;
+  m.R = (kind == kMatInvG && !transposed) ? 2 * n : n;
+  m.nin = (kind == kMatInvG && transposed) ? 2 * n : n;
   const int rpt = 16 * apply_tr(m.R);
   m.RP = ceil_div(m.R, rpt) * rpt;
   std::vector<double> lam(L);
@@ -916,12 +1385,14 @@ static int get_matrix(dino_pe* pe, int kind, double eta, const double* host_filt
     DINO_CHECK_CUDA(cudaMalloc(&dc, sizeof(double) * consts.size()));
     DINO_CHECK_CUDA(cudaMemcpy(dc, consts.data(), sizeof(double) * consts.size(),
                                cudaMemcpyHostToDevice));
-    DINO_CHECK_CUDA(cudaMalloc(&m.d, sizeof(float) * (size_t)L * n * m.RP));
+    DINO_CHECK_CUDA(cudaMalloc(&m.d, sizeof(float) * (size_t)L * m.nin * m.RP));
     DINO_CHECK_CUDA(cudaMemset(pe->d_flag, 0, sizeof(int)));
     MatBuildArgs b{};
     b.K = K;
     b.kind = kind;
     b.RP = m.RP;
+    b.nin = m.nin;
+    b.transposed = transposed ? 1 : 0;
     b.eta = eta;
     b.R = pe->R;
     b.G = dc;
@@ -974,8 +1445,9 @@ static int get_filter(dino_pe* pe, const double* host, float** out) {
   return DINO_OK;
 }
 
-static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
-                            cudaStream_t st) {
+// Modal pre-pass and inverse transforms: the nodal inputs of the column
+// kernel in pe->d_nodal.
+static int pe_nodal_inputs(dino_pe* pe, const float* state, cudaStream_t st) {
   dino_plan* p = pe->plan;
   const int K = pe->K, mem = pe->mem;
   const int mK = mem * K;
@@ -1035,9 +1507,14 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
     DINO_TRY(sht_inverse_segs(p, s, pe->d_nodal, pe->n_inv, pe->d_work,
                               pe->work_fields, st));
   }
-  // 3. fused nodal column kernel
+  return DINO_OK;
+}
+
+static NodalArgs make_nodal_args(dino_pe* pe) {
+  const int K = pe->K, mem = pe->mem;
+  const int mK = mem * K;
+  NodalArgs a{};
   {
-    NodalArgs a{};
     a.nod = pe->d_nodal;
     a.fwd = pe->d_fwd_in;
     a.K = K;
@@ -1089,6 +1566,19 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
     a.hs_maxT = (float)pe->hs_maxT;
     a.hs_dTy = (float)pe->hs_dTy;
     a.hs_dThz = (float)pe->hs_dThz;
+  }
+  return a;
+}
+
+static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
+                            cudaStream_t st) {
+  dino_plan* p = pe->plan;
+  const int K = pe->K, mem = pe->mem;
+  const int mK = mem * K;
+  DINO_TRY(pe_nodal_inputs(pe, state, st));
+  // 3. fused nodal column kernel
+  {
+    NodalArgs a = make_nodal_args(pe);
     dim3 grid(ceil_div((int)pe->IJ, 128), mem);
     pe_nodal_kernel<<<grid, 128, 0, st>>>(a);
     DINO_TRY(check_launch("pe_nodal"));
@@ -1186,6 +1676,212 @@ static int pe_step_once(dino_pe* pe, float* y, double dt, const float* filt,
   return DINO_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Reverse mode
+// ---------------------------------------------------------------------------
+
+static int pe_ensure_adjoint(dino_pe* pe) {
+  if (pe->d_xbar_n) return DINO_OK;
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_xbar_n, sizeof(float) * pe->n_inv * pe->IJ));
+  DINO_CHECK_CUDA(cudaMalloc(&pe->d_xbar_m, sizeof(float) * pe->n_inv * pe->ML));
+  for (auto*& b : pe->d_adj)
+    DINO_CHECK_CUDA(cudaMalloc(&b, sizeof(float) * pe->n_state * pe->ML));
+  return DINO_OK;
+}
+
+// state_ct = (d explicit_terms / d state)^T tend_ct at `state`.
+static int pe_explicit_vjp_impl(dino_pe* pe, const float* state, const float* tbar,
+                                float* sbar, cudaStream_t st) {
+  dino_plan* p = pe->plan;
+  const int K = pe->K, mem = pe->mem, mK = mem * K;
+  DINO_TRY(pe_nodal_inputs(pe, state, st));
+  {
+    PostAdjArgs a{};
+    a.tbar = tbar;
+    a.fbar = pe->d_fwd_out;
+    a.K = K;
+    a.mem = mem;
+    a.nT = pe->nT;
+    a.hum = pe->hum;
+    a.hs = pe->hs;
+    a.M = pe->M;
+    a.L = pe->L;
+    a.lw = p->lw;
+    a.o_Au = pe->o_Au;
+    a.o_Av = pe->o_Av;
+    a.o_KE = pe->o_KE;
+    a.o_uT = pe->o_uT;
+    a.o_vT = pe->o_vT;
+    a.o_Tn = pe->o_Tn;
+    a.o_tr = pe->o_tr;
+    a.o_vh = pe->o_vh;
+    a.o_gh = pe->o_gh;
+    a.o_dh = pe->o_dh;
+    a.o_hsT = pe->o_hsT;
+    a.o_lnps = pe->o_lnps;
+    a.p_vort = 0;
+    a.p_div = mK;
+    a.p_temp = 2 * mK;
+    a.p_tr = 3 * mK;
+    a.p_lnps = (3 + pe->nT) * mK;
+    a.deriv = p->d_deriv;
+    a.lap = p->d_lap;
+    a.inv_radius = (float)(1.0 / p->radius);
+    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
+    pe_post_adjoint_kernel<<<grid, 256, 0, st>>>(a);
+    DINO_TRY(check_launch("pe_post_adjoint"));
+  }
+  DINO_TRY(sht_forward_adjoint_to(p, pe->d_fwd_out, pe->d_fwd_in, pe->n_fwd,
+                                  pe->d_work, pe->work_fields, st));
+  {
+    NodalAdjArgs a{};
+    a.f = make_nodal_args(pe);
+    a.fbar = pe->d_fwd_in;
+    a.xbar = pe->d_xbar_n;
+    dim3 grid(ceil_div((int)pe->IJ, 128), mem);
+    pe_nodal_adjoint_kernel<<<grid, 128, 0, st>>>(a);
+    DINO_TRY(check_launch("pe_nodal_adjoint"));
+  }
+  DINO_TRY(sht_inverse_adjoint_to(p, pe->d_xbar_n, pe->d_xbar_m, pe->n_inv,
+                                  pe->d_work, pe->work_fields, st));
+  {
+    PrepAdjArgs a{};
+    a.xbar = pe->d_xbar_m;
+    a.sbar = sbar;
+    a.K = K;
+    a.mem = mem;
+    a.nT = pe->nT;
+    a.hum = pe->hum;
+    a.hs = pe->hs;
+    a.M = pe->M;
+    a.L = pe->L;
+    a.lw = p->lw;
+    a.p_u = pe->p_u;
+    a.p_v = pe->p_v;
+    a.p_gqx = pe->p_gqx;
+    a.p_gqy = pe->p_gqy;
+    a.p_gx = pe->p_gx;
+    a.p_gy = pe->p_gy;
+    a.p_laplnps = pe->p_laplnps;
+    a.p_lnps = pe->p_lnps;
+    a.s_lnps = (3 + pe->nT) * mK;
+    a.deriv = p->d_deriv;
+    a.lap = p->d_lap;
+    a.invlap = p->d_invlap;
+    a.inv_radius = (float)(1.0 / p->radius);
+    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
+    pe_prep_adjoint_kernel<<<grid, 256, 0, st>>>(a);
+    DINO_TRY(check_launch("pe_prep_adjoint"));
+  }
+  return DINO_OK;
+}
+
+struct LinTerm {
+  const float* x;
+  float ci, ce;
+};
+
+static int launch_lincomb(dino_pe* pe, std::initializer_list<LinTerm> terms,
+                          const float* filt, float* out, int only, cudaStream_t st) {
+  LinCombArgs a{};
+  for (const LinTerm& t : terms) {
+    a.x[a.nx] = t.x;
+    a.ci[a.nx] = t.ci;
+    a.ce[a.nx] = t.ce;
+    ++a.nx;
+  }
+  a.filt = filt;
+  a.out = out;
+  a.mK = pe->mem * pe->K;
+  a.nT = pe->nT;
+  a.L = pe->L;
+  a.only = only;
+  a.ML = pe->ML;
+  dim3 grid(ceil_div((int)pe->ML, 256), pe->n_state);
+  pe_lincomb_kernel<<<grid, 256, 0, st>>>(a);
+  return check_launch("pe_lincomb");
+}
+
+struct StepMatsT {
+  const MatEntry* L;      // G^T
+  const MatEntry* inv1;   // ((1 - dt/6 G)^-1)^T
+  const MatEntry* invg2;  // [(1 - dt/3 G)^-1 ; G (1 - dt/3 G)^-1]^T
+  const MatEntry* fin3;   // (filter (1 + dt/4 G (1 - dt/4 G)^-1))^T
+};
+
+static int get_step_mats_t(dino_pe* pe, double dt, const double* host_filter,
+                           StepMatsT* m) {
+  DINO_TRY(get_matrix(pe, kMatL, 0.0, nullptr, &m->L, true));
+  DINO_TRY(get_matrix(pe, kMatInv, dt / 6.0, nullptr, &m->inv1, true));
+  DINO_TRY(get_matrix(pe, kMatInvG, dt / 3.0, nullptr, &m->invg2, true));
+  DINO_TRY(get_matrix(pe, kMatFinal, dt / 4.0, host_filter, &m->fin3, true));
+  return DINO_OK;
+}
+
+// VJP of one filtered SIL3 step at y: in_ct = (d step / d y)^T out_ct.  The
+// stage states Y1, Y2 are recomputed from y; the reverse sweep follows the
+// forward tableau (see pe_step_once):
+//   Z3 = Fin3^T out_ct (implicit planes), filter * out_ct (others)
+//   V2 = F'(Y2)^T (dt Z3);           Z2 = [Inv2; G Inv2]^T [V2; 3dt/8 Z3]
+//   V1 = F'(Y1)^T (dt/2 (Z2 - Z3));  Z1 = Inv1^T V1
+//   V0 = F'(y)^T (dt/2 Z3 + dt/6 Z2 + dt/3 Z1)
+//   in_ct = Z1 + Z2 + Z3 + V0 + G^T (3dt/8 Z3 + dt/3 Z2 + dt/6 Z1)
+// (Inv_i act on the implicit planes only; elsewhere they are the identity.)
+static int pe_step_vjp_impl(dino_pe* pe, const float* y, const float* out_ct,
+                            float* in_ct, double dt, const float* filt,
+                            const StepMats& m, const StepMatsT& mt, cudaStream_t st) {
+  float* Y1 = pe->d_adj[0];
+  float* Y2 = pe->d_adj[1];
+  float* Z1 = pe->d_adj[2];
+  float* Z2 = pe->d_adj[3];
+  float* Z3 = pe->d_adj[4];
+  float* V = pe->d_adj[5];
+  const float fdt = (float)dt;
+  // Stage states.
+  DINO_TRY(pe_explicit_impl(pe, y, pe->d_f[0], st));
+  DINO_TRY(launch_apply(pe, m.L, y, pe->d_g[0], nullptr, st));
+  DINO_TRY(launch_combine(pe, y, {{(float)(dt / 3.0), pe->d_f[0]}},
+                          {{(float)(dt / 6.0), pe->d_g[0]}}, nullptr, Y1, st));
+  DINO_TRY(launch_apply(pe, m.inv1, pe->d_ystar, Y1, nullptr, st));
+  DINO_TRY(pe_explicit_impl(pe, Y1, pe->d_f[1], st));
+  DINO_TRY(launch_combine(
+      pe, y, {{(float)(dt / 6.0), pe->d_f[0]}, {(float)(dt * 0.5), pe->d_f[1]}},
+      {{(float)(dt / 3.0), pe->d_g[0]}}, nullptr, Y2, st));
+  DINO_TRY(launch_apply(pe, m.invg2, pe->d_ystar, Y2, pe->d_g[1], st));
+  // Reverse sweep.
+  float* C = pe->d_f[0];
+  DINO_TRY(launch_apply(pe, mt.fin3, out_ct, Z3, nullptr, st));
+  DINO_TRY(launch_lincomb(pe, {{out_ct, 0.f, 1.f}}, filt, Z3, 2, st));
+  DINO_TRY(launch_lincomb(pe, {{Z3, fdt, fdt}}, nullptr, C, 0, st));
+  DINO_TRY(pe_explicit_vjp_impl(pe, Y2, C, V, st));
+  DINO_TRY(launch_apply(pe, mt.invg2, V, Z2, nullptr, st, Z3, 1.f,
+                        (float)(dt * 0.375)));
+  DINO_TRY(launch_lincomb(pe, {{V, 0.f, 1.f}}, nullptr, Z2, 2, st));
+  const float h = (float)(dt * 0.5);
+  DINO_TRY(launch_lincomb(pe, {{Z3, -h, -h}, {Z2, h, h}}, nullptr, C, 0, st));
+  DINO_TRY(pe_explicit_vjp_impl(pe, Y1, C, V, st));
+  DINO_TRY(launch_apply(pe, mt.inv1, V, Z1, nullptr, st));
+  DINO_TRY(launch_lincomb(pe, {{V, 0.f, 1.f}}, nullptr, Z1, 2, st));
+  const float c3 = (float)(dt * 0.5), c2 = (float)(dt / 6.0), c1 = (float)(dt / 3.0);
+  DINO_TRY(launch_lincomb(pe, {{Z3, c3, c3}, {Z2, c2, c2}, {Z1, c1, c1}}, nullptr, C,
+                          0, st));
+  DINO_TRY(pe_explicit_vjp_impl(pe, y, C, V, st));
+  float* Gb = pe->d_f[1];
+  float* Tt = pe->d_f[2];
+  DINO_TRY(launch_lincomb(pe,
+                          {{Z3, (float)(dt * 0.375), 0.f},
+                           {Z2, (float)(dt / 3.0), 0.f},
+                           {Z1, (float)(dt / 6.0), 0.f}},
+                          nullptr, Gb, 1, st));
+  DINO_TRY(launch_apply(pe, mt.L, Gb, Tt, nullptr, st));
+  DINO_TRY(launch_lincomb(pe,
+                          {{Z1, 1.f, 1.f}, {Z2, 1.f, 1.f}, {Z3, 1.f, 1.f},
+                           {V, 1.f, 1.f}, {Tt, 1.f, 0.f}},
+                          nullptr, in_ct, 0, st));
+  return DINO_OK;
+}
+
 template <typename T>
 static int upload_vec(T** dst, const std::vector<T>& v) {
   DINO_CHECK_CUDA(cudaMalloc((void**)dst, sizeof(T) * (v.empty() ? 1 : v.size())));
@@ -1212,6 +1908,9 @@ static void pe_free(dino_pe* pe) {
   for (auto* g : pe->d_g) cudaFree(g);
   cudaFree(pe->d_Y);
   cudaFree(pe->d_ystar);
+  cudaFree(pe->d_xbar_n);
+  cudaFree(pe->d_xbar_m);
+  for (auto* b : pe->d_adj) cudaFree(b);
   cudaFree(pe->d_flag);
   delete pe;
 }
@@ -1491,4 +2190,57 @@ int dino_pe_step_graph(dino_pe* pe, float* state, double dt,
   return DINO_OK;
 }
 
+int dino_pe_explicit_vjp(dino_pe* pe, const float* state, const float* tend_ct,
+                         float* state_ct, void* stream) {
+  DINO_REQUIRE(pe && state && tend_ct && state_ct, DINO_ERR_ARG,
+               "dino_pe_explicit_vjp: null argument");
+  DINO_REQUIRE(state_ct != state && state_ct != tend_ct, DINO_ERR_ARG,
+               "dino_pe_explicit_vjp: state_ct must not alias the inputs");
+  DINO_TRY(pe_ensure_adjoint(pe));
+  DINO_TRY(sht_prepare(pe->plan));
+  return pe_explicit_vjp_impl(pe, state, tend_ct, state_ct, (cudaStream_t)stream);
+}
+
+int dino_pe_implicit_vjp(dino_pe* pe, const float* out_ct, float* in_ct, void* stream) {
+  DINO_REQUIRE(pe && out_ct && in_ct, DINO_ERR_ARG, "dino_pe_implicit_vjp: null argument");
+  DINO_REQUIRE(out_ct != in_ct, DINO_ERR_ARG, "dino_pe_implicit_vjp: in and out must differ");
+  cudaStream_t st = (cudaStream_t)stream;
+  DINO_CHECK_CUDA(cudaMemsetAsync(in_ct, 0, sizeof(float) * pe->n_state * pe->ML, st));
+  const MatEntry* m = nullptr;
+  DINO_TRY(get_matrix(pe, kMatL, 0.0, nullptr, &m, true));
+  return launch_apply(pe, m, out_ct, in_ct, nullptr, st);
+}
+
+int dino_pe_implicit_inverse_vjp(dino_pe* pe, const float* out_ct, float* in_ct,
+                                 double eta, void* stream) {
+  DINO_REQUIRE(pe && out_ct && in_ct, DINO_ERR_ARG,
+               "dino_pe_implicit_inverse_vjp: null argument");
+  DINO_REQUIRE(std::isfinite(eta), DINO_ERR_ARG, "step_size must be finite");
+  const MatEntry* m = nullptr;
+  DINO_TRY(get_matrix(pe, kMatInv, eta, nullptr, &m, true));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (out_ct != in_ct)
+    DINO_TRY(launch_lincomb(pe, {{out_ct, 0.f, 1.f}}, nullptr, in_ct, 2, st));
+  return launch_apply(pe, m, out_ct, in_ct, nullptr, st);
+}
+
+int dino_pe_step_vjp(dino_pe* pe, const float* state, const float* out_ct,
+                     float* in_ct, double dt, const double* host_filter,
+                     void* stream) {
+  DINO_REQUIRE(pe && state && out_ct && in_ct, DINO_ERR_ARG,
+               "dino_pe_step_vjp: null argument");
+  DINO_REQUIRE(in_ct != state, DINO_ERR_ARG, "dino_pe_step_vjp: in_ct must not alias state");
+  DINO_TRY(pe_ensure_adjoint(pe));
+  DINO_TRY(sht_prepare(pe->plan));
+  StepMats m;
+  DINO_TRY(get_step_mats(pe, dt, host_filter, &m));
+  StepMatsT mt;
+  DINO_TRY(get_step_mats_t(pe, dt, host_filter, &mt));
+  float* filt = nullptr;
+  DINO_TRY(get_filter(pe, host_filter, &filt));
+  return pe_step_vjp_impl(pe, state, out_ct, in_ct, dt, filt, m, mt,
+                          (cudaStream_t)stream);
+}
+
 }  // extern "C"
+

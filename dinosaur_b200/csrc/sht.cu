@@ -738,27 +738,42 @@ int sht_forward_to(dino_plan* p, const float* nodal, float* out, int nf,
 
 // Adjoint of the inverse transform: unweighted forward Fourier, then the
 // forward contraction.  Adjoint of the forward transform: the inverse
-// contraction, then the inverse Fourier synthesis scaled by w[j].
-static int sht_inverse_adjoint(dino_plan* p, const float* nodal_ct,
-                               float* modal_ct, int nf, cudaStream_t st) {
+// contraction, then the inverse Fourier synthesis scaled by w[j].  Chunked
+// like the transforms themselves (work holds work_fields x M x J floats).
+int sht_inverse_adjoint_to(dino_plan* p, const float* nodal_ct, float* modal_ct,
+                           int nf, float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
-  for (int f0 = 0; f0 < nf; f0 += p->max_fields) {
-    int n = nf - f0 < p->max_fields ? nf - f0 : p->max_fields;
-    DINO_TRY(fourier_forward(p, nodal_ct + f0 * ns, p->d_work, n, false, st));
-    DINO_TRY(legendre_forward(p, p->d_work, modal_ct + f0 * ms, n, st));
+  const int chunk = l2_chunk(p, nf, work_fields);
+  for (int f0 = 0; f0 < nf; f0 += chunk) {
+    int n = nf - f0 < chunk ? nf - f0 : chunk;
+    DINO_TRY(fourier_forward(p, nodal_ct + f0 * ns, work, n, false, st));
+    DINO_TRY(legendre_forward(p, work, modal_ct + f0 * ms, n, st));
   }
   return DINO_OK;
 }
 
-static int sht_forward_adjoint(dino_plan* p, const float* modal_ct,
-                               float* nodal_ct, int nf, cudaStream_t st) {
+int sht_forward_adjoint_to(dino_plan* p, const float* modal_ct, float* nodal_ct,
+                           int nf, float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
-  for (int f0 = 0; f0 < nf; f0 += p->max_fields) {
-    int n = nf - f0 < p->max_fields ? nf - f0 : p->max_fields;
-    DINO_TRY(legendre_inverse(p, one_seg(modal_ct + f0 * ms, n), p->d_work, n, st));
-    DINO_TRY(fourier_inverse(p, p->d_work, nodal_ct + f0 * ns, n, true, st));
+  const int chunk = l2_chunk(p, nf, work_fields);
+  for (int f0 = 0; f0 < nf; f0 += chunk) {
+    int n = nf - f0 < chunk ? nf - f0 : chunk;
+    DINO_TRY(legendre_inverse(p, one_seg(modal_ct + f0 * ms, n), work, n, st));
+    DINO_TRY(fourier_inverse(p, work, nodal_ct + f0 * ns, n, true, st));
   }
   return DINO_OK;
+}
+
+static int sht_inverse_adjoint(dino_plan* p, const float* nodal_ct,
+                               float* modal_ct, int nf, cudaStream_t st) {
+  return sht_inverse_adjoint_to(p, nodal_ct, modal_ct, nf, p->d_work,
+                                p->max_fields, st);
+}
+
+static int sht_forward_adjoint(dino_plan* p, const float* modal_ct,
+                               float* nodal_ct, int nf, cudaStream_t st) {
+  return sht_forward_adjoint_to(p, modal_ct, nodal_ct, nf, p->d_work,
+                                p->max_fields, st);
 }
 
 // ---------------------------------------------------------------------------

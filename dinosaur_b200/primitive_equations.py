@@ -303,17 +303,122 @@ class _Engine:
                'implicit_inverse')
     return out
 
+  def _filter_ptr(self, filt):
+    if filt is None:
+      return None
+    self._filt = np.ascontiguousarray(filt, np.float64)
+    if self._filt.shape != (self.L,):
+      raise ValueError(f'filter scaling must have shape ({self.L},)')
+    return _lib.dptr(self._filt)
+
   def step_(self, buf, dt, filt, n_steps, graph=False):
-    fptr = None
-    if filt is not None:
-      self._filt = np.ascontiguousarray(filt, np.float64)
-      if self._filt.shape != (self.L,):
-        raise ValueError(f'filter scaling must have shape ({self.L},)')
-      fptr = _lib.dptr(self._filt)
+    fptr = self._filter_ptr(filt)
     fn = (_lib.lib().dino_pe_step_graph if graph else _lib.lib().dino_pe_step)
     _lib.check(fn(self.handle, sh.ptr(buf), float(dt), fptr, int(n_steps),
                   sh.stream_handle()), 'step')
     return buf
+
+  # -- reverse mode ----------------------------------------------------------
+  def explicit_vjp(self, buf, ct):
+    out = self._out()
+    _lib.check(_lib.lib().dino_pe_explicit_vjp(
+        self.handle, sh.ptr(buf), sh.ptr(ct), sh.ptr(out), sh.stream_handle()),
+               'explicit_terms vjp')
+    return out
+
+  def implicit_vjp(self, ct):
+    out = self._out()
+    _lib.check(_lib.lib().dino_pe_implicit_vjp(
+        self.handle, sh.ptr(ct), sh.ptr(out), sh.stream_handle()),
+               'implicit_terms vjp')
+    return out
+
+  def inverse_vjp(self, ct, eta):
+    out = self._out()
+    _lib.check(_lib.lib().dino_pe_implicit_inverse_vjp(
+        self.handle, sh.ptr(ct), sh.ptr(out), float(eta), sh.stream_handle()),
+               'implicit_inverse vjp')
+    return out
+
+  def step_vjp_(self, buf, ct, dt, filt):
+    """Overwrites ct with the VJP of one filtered step taken from buf."""
+    fptr = self._filter_ptr(filt)
+    _lib.check(_lib.lib().dino_pe_step_vjp(
+        self.handle, sh.ptr(buf), sh.ptr(ct), sh.ptr(ct), float(dt), fptr,
+        sh.stream_handle()), 'step vjp')
+    return ct
+
+
+# ---------------------------------------------------------------------------
+# Reverse mode on packed buffers
+# ---------------------------------------------------------------------------
+
+
+class _ExplicitFn(torch.autograd.Function):
+
+  @staticmethod
+  def forward(ctx, buf, eng):
+    ctx.eng = eng
+    ctx.save_for_backward(buf)
+    return eng.explicit(buf)
+
+  @staticmethod
+  def backward(ctx, g):
+    (buf,) = ctx.saved_tensors
+    return ctx.eng.explicit_vjp(buf, g.contiguous()), None
+
+
+class _ImplicitFn(torch.autograd.Function):
+
+  @staticmethod
+  def forward(ctx, buf, eng):
+    ctx.eng = eng
+    return eng.implicit(buf)
+
+  @staticmethod
+  def backward(ctx, g):
+    return ctx.eng.implicit_vjp(g.contiguous()), None
+
+
+class _InverseFn(torch.autograd.Function):
+
+  @staticmethod
+  def forward(ctx, buf, eng, eta):
+    ctx.eng, ctx.eta = eng, eta
+    return eng.inverse(buf, eta)
+
+  @staticmethod
+  def backward(ctx, g):
+    return ctx.eng.inverse_vjp(g.contiguous(), ctx.eta), None, None
+
+
+class _RolloutFn(torch.autograd.Function):
+  """n filtered SIL3 steps; the backward pass recomputes each step from its
+  saved input state (per-step checkpointing, the role of
+  nested_checkpoint_scan in time_integration.py:573-637)."""
+
+  @staticmethod
+  def forward(ctx, buf, eng, dt, filt, n_steps):
+    ckpts = []
+    y = buf.detach().clone()
+    for _ in range(n_steps):
+      ckpts.append(y.clone())
+      eng.step_(y, dt, filt, 1)
+    ctx.eng, ctx.dt, ctx.filt = eng, dt, filt
+    ctx.ckpts = ckpts
+    return y
+
+  @staticmethod
+  def backward(ctx, g):
+    ct = g.detach().clone().contiguous()
+    for y in reversed(ctx.ckpts):
+      ctx.eng.step_vjp_(y, ct, ctx.dt, ctx.filt)
+    ctx.ckpts = None
+    return ct, None, None, None, None
+
+
+def _needs_grad(buf):
+  return torch.is_grad_enabled() and buf.requires_grad
 
 
 # ---------------------------------------------------------------------------
@@ -390,14 +495,16 @@ class PrimitiveEquationsSigma(time_integration.ImplicitExplicitODE):
   def explicit_terms(self, state: State) -> State:
     """primitive_equations.py:1126-1194."""
     eng = self.engine(state)
-    out = eng.explicit(eng.pack(state))
+    buf = eng.pack(state)
+    out = _ExplicitFn.apply(buf, eng) if _needs_grad(buf) else eng.explicit(buf)
     return eng.unpack(out, state,
                       None if state.sim_time is None else 1.0)
 
   def implicit_terms(self, state: State) -> State:
     """primitive_equations.py:1196-1249."""
     eng = self.engine(state)
-    out = eng.implicit(eng.pack(state))
+    buf = eng.pack(state)
+    out = _ImplicitFn.apply(buf, eng) if _needs_grad(buf) else eng.implicit(buf)
     return eng.unpack(out, state, None if state.sim_time is None else 0.0)
 
   def implicit_inverse(self, state: State, step_size: float) -> State:
@@ -406,7 +513,10 @@ class PrimitiveEquationsSigma(time_integration.ImplicitExplicitODE):
       raise TypeError(
           f'`step_size` must be concrete but a tensor was passed: {step_size}.')
     eng = self.engine(state)
-    out = eng.inverse(eng.pack(state), float(step_size))
+    buf = eng.pack(state)
+    eta = float(step_size)
+    out = (_InverseFn.apply(buf, eng, eta) if _needs_grad(buf)
+           else eng.inverse(buf, eta))
     return eng.unpack(out, state, state.sim_time)
 
 

@@ -164,10 +164,16 @@ class FusedSIL3Step:
   use_graph: bool = True
 
   def __call__(self, state):
+    from dinosaur_b200 import primitive_equations as pe  # pylint: disable=g-import-not-at-top
     eng = self.equation.engine(state)
     buf = eng.pack(state)  # a fresh buffer: the input state is not modified
-    eng.step_(buf, self.dt, self.filter_scaling, self.n_steps,
-              graph=self.use_graph)
+    if torch.is_grad_enabled() and buf.requires_grad:
+      # Differentiable rollout with hand-written step VJPs.
+      buf = pe._RolloutFn.apply(buf, eng, self.dt, self.filter_scaling,  # pylint: disable=protected-access
+                                self.n_steps)
+    else:
+      eng.step_(buf, self.dt, self.filter_scaling, self.n_steps,
+                graph=self.use_graph)
     sim_time = state.sim_time
     if sim_time is not None:
       sim_time = sim_time + self.dt * self.n_steps

@@ -214,6 +214,34 @@ DINO_API int dino_pe_step_graph(dino_pe* pe, float* d_state, double dt,
                        const double* host_filter, int32_t n_steps,
                        void* stream);
 
+/* ---- Reverse mode (vector-Jacobian products) ----------------------------
+ * The reference differentiates its step with jax.vjp / jax.grad through the
+ * JAX einsums of explicit_terms, implicit_terms and implicit_inverse
+ * (primitive_equations.py:1126-1330) and the imex_rk_sil3 stages
+ * (time_integration.py:329-405); these entries are the hand-written
+ * equivalents on the packed state layout.  Each allocates the adjoint work
+ * buffers of `pe` on first use. */
+
+/* d_state_ct = (d explicit_terms / d state)^T d_tend_ct at d_state.
+ * d_state_ct must not alias the inputs. */
+DINO_API int dino_pe_explicit_vjp(dino_pe* pe, const float* d_state,
+                                  const float* d_tend_ct, float* d_state_ct,
+                                  void* stream);
+/* d_in_ct = G^T d_out_ct for the linear implicit_terms G (buffers differ). */
+DINO_API int dino_pe_implicit_vjp(dino_pe* pe, const float* d_out_ct,
+                                  float* d_in_ct, void* stream);
+/* d_in_ct = ((1 - eta G)^-1)^T d_out_ct (in place allowed). */
+DINO_API int dino_pe_implicit_inverse_vjp(dino_pe* pe, const float* d_out_ct,
+                                          float* d_in_ct, double eta,
+                                          void* stream);
+/* VJP of one filtered SIL3 step taken from d_state (not modified):
+ * d_in_ct = (d step / d state)^T d_out_ct.  The stage states are recomputed
+ * from d_state, so a rollout's backward pass needs only the per-step input
+ * states (per-step checkpointing).  d_in_ct may alias d_out_ct. */
+DINO_API int dino_pe_step_vjp(dino_pe* pe, const float* d_state,
+                              const float* d_out_ct, float* d_in_ct, double dt,
+                              const double* host_filter, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
