@@ -17,6 +17,7 @@ Multi-GPU runs (torchrun) are independent replicas (weak scaling).
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import os
 import statistics
@@ -390,21 +391,34 @@ def run_ours(args):
 
 
 def pe_extras(torch):
-  """Primitive-equation steps/s on the benchmark grids (CUDA-graph replay)."""
+  """Primitive-equation steps/s on the benchmark grids (CUDA-graph replay).
+
+  Synthetic states near rest (seeded small modal noise); the moist case adds
+  specific humidity (5 g/kg mean) and two passive tracers.  Each case runs
+  with the plain FP32 and the split-BF16 Legendre contraction where both are
+  listed."""
   from dinosaur_b200 import coordinate_systems, held_suarez, primitive_equations as pe
   from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
   from dinosaur_b200 import time_integration as ti, units
   out = {}
-  for name, grid_fn, layers, members, hs, dt_min in [
-      ('T42_L24_x16_held_suarez', sh.Grid.T42, 24, 16, True, 15),
-      ('TL255_L32_dry', sh.Grid.TL255, 32, 1, False, 6)]:
-    g = grid_fn()
+  cases = [
+      # name, grid, layers, members, held_suarez, moist, dt [min], precision
+      ('T42_L24_x16_held_suarez', 'T42', 24, 16, True, False, 15, 'fp32'),
+      ('TL255_L32_dry', 'TL255', 32, 1, False, False, 6, 'fp32'),
+      ('TL255_L32_dry_bf16x3', 'TL255', 32, 1, False, False, 6, 'bf16x3'),
+      ('TL255_L32_moist3_x4', 'TL255', 32, 4, False, True, 6, 'fp32'),
+      ('TL255_L32_moist3_x4_bf16x3', 'TL255', 32, 4, False, True, 6, 'bf16x3'),
+  ]
+  for name, grid_name, layers, members, hs, moist, dt_min, precision in cases:
+    impl = functools.partial(sh.CudaSphericalHarmonics, precision=precision)
+    g = getattr(sh.Grid, grid_name)(spherical_harmonics_impl=impl)
     vert = sigma_coordinates.SigmaCoordinates.equidistant(layers)
     coords = coordinate_systems.CoordinateSystem(g, vert)
     ps = units.SimUnits()
     tref = np.full(layers, 285.0) if hs else np.linspace(220.0, 288.0, layers)
-    eq = pe.PrimitiveEquationsSigma(tref, np.zeros(g.modal_shape, np.float32),
-                                    coords, ps)
+    eq = pe.PrimitiveEquationsSigma(
+        tref, np.zeros(g.modal_shape, np.float32), coords, ps,
+        humidity_key='specific_humidity' if moist else None)
     if hs:
       eq = ti.compose_equations([eq, held_suarez.HeldSuarezForcingSigma(coords, ps, tref)])
     dt = units.nondim_time(dt_min * 60.0)
@@ -414,18 +428,27 @@ def pe_extras(torch):
       flt = ti.exponential_step_filter(g, dt)
     step = ti.step_with_filters(ti.imex_rk_sil3(eq, dt), [flt])
     rng = np.random.default_rng(0)
-    shape = (members, layers) + g.modal_shape if members > 1 else (layers,) + g.modal_shape
-    lshape = (members, 1) + g.modal_shape if members > 1 else (1,) + g.modal_shape
+    lead = (members, layers) if members > 1 else (layers,)
+    shape = lead + g.modal_shape
+    lshape = ((members, 1) if members > 1 else (1,)) + g.modal_shape
     _, l = g.modal_mesh
     scale = g.mask / (l + 1.0) ** 2
-    t = lambda s: torch.as_tensor((1e-4 * rng.standard_normal(s) * scale).astype(np.float32),
-                                  device='cuda')
-    state = pe.State(t(shape), t(shape), t(shape), t(lshape))
+    noise = lambda s, a=1e-4: (a * rng.standard_normal(s) * scale).astype(np.float32)
+    t = lambda a: torch.as_tensor(a, device='cuda')
+    tracers = {}
+    if moist:
+      const = np.zeros(shape, np.float32)
+      const[..., 0, 0] = 2.0 * np.sqrt(np.pi)  # the constant field 1
+      tracers = {'specific_humidity': t(5e-3 * const + noise(shape, 1e-6)),
+                 'tracer_a': t(const + noise(shape)),
+                 'tracer_b': t(const + noise(shape))}
+    state = pe.State(t(noise(shape)), t(noise(shape)), t(noise(shape)),
+                     t(noise(lshape)), tracers=tracers)
     eng = eq.engine(state)
     buf = eng.pack(state)
     eng.step_(buf, dt, step.filter_scaling, 3, graph=True)
     torch.cuda.synchronize()
-    n = 20 if name.startswith('TL255') else 60
+    n = 10 if 'moist' in name else (20 if grid_name == 'TL255' else 60)
     a0 = torch.cuda.Event(enable_timing=True)
     a1 = torch.cuda.Event(enable_timing=True)
     a0.record()
@@ -435,7 +458,10 @@ def pe_extras(torch):
     ms = a0.elapsed_time(a1) / n
     out[name] = {'ms_per_step': ms, 'steps_per_s': 1e3 / ms,
                  'member_steps_per_s': members * 1e3 / ms,
+                 'precision': precision,
                  'finite': bool(torch.isfinite(buf).all())}
+    del eng, buf, state, eq
+    torch.cuda.empty_cache()
   return out
 
 

@@ -106,67 +106,100 @@ __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
   }
 }
 
+// Eight consecutive split values as one 16-byte store of each half.
+__device__ __forceinline__ void store_split8(const float (&v)[8], bf16* hi, bf16* lo) {
+  __align__(16) bf16 h[8];
+  __align__(16) bf16 l[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) split_bf16(v[i], h[i], l[i]);
+  *reinterpret_cast<uint4*>(hi) = *reinterpret_cast<const uint4*>(h);
+  *reinterpret_cast<uint4*>(lo) = *reinterpret_cast<const uint4*>(l);
+}
+
 // Modal rows -> A[m][p][r][kk] = x[b][row][m + 2 kk + p], zero-padded to the
-// next multiple of 64 in kk.
+// next multiple of 64 in kk.  A thread converts 8 consecutive kk of both
+// parities (16 consecutive l, read as one contiguous run) and writes them as
+// 16-byte stores.
 __global__ void tc_split_inverse_kernel(Segs in, int nf, int M, int L, int Rp,
                                         int Kp, bf16* __restrict__ Ah,
                                         bf16* __restrict__ Al) {
   const int m = blockIdx.y;
   const int rows = (m == 0) ? nf : 2 * nf;
   const int Lm = L - m;
-  const int kw = round_up((Lm + 1) >> 1, 64);
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (size_t)rows * kw) return;
-  const int kk = idx % kw;
-  const int r = idx / kw;
+  const int gw = round_up((Lm + 1) >> 1, 64) / 8;  // 8-kk groups per row
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)rows * gw) return;
+  const int g = idx % gw;
+  const int r = idx / gw;
   int b, row;
   tc_row_map(m, r, b, row);
   const float* xr = seg_field(in, b, (size_t)M * L) + (size_t)row * L + m;
-  const int k0 = 2 * kk, k1 = 2 * kk + 1;
-  float v0 = (k0 < Lm) ? xr[k0] : 0.f;
-  float v1 = (k1 < Lm) ? xr[k1] : 0.f;
-  bf16 h, l;
-  size_t o0 = ((size_t)(m * 2) * Rp + r) * Kp + kk;
-  size_t o1 = ((size_t)(m * 2 + 1) * Rp + r) * Kp + kk;
-  split_bf16(v0, h, l);
-  Ah[o0] = h;
-  Al[o0] = l;
-  split_bf16(v1, h, l);
-  Ah[o1] = h;
-  Al[o1] = l;
+  const int k0 = 16 * g;
+  float ev[8], od[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int ke = k0 + 2 * i, ko = ke + 1;
+    ev[i] = (ke < Lm) ? xr[ke] : 0.f;
+    od[i] = (ko < Lm) ? xr[ko] : 0.f;
+  }
+  const size_t o0 = ((size_t)(m * 2) * Rp + r) * Kp + 8 * g;
+  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + r) * Kp + 8 * g;
+  store_split8(ev, Ah + o0, Al + o0);
+  store_split8(od, Ah + o1, Al + o1);
 }
 
 // Weighted Fourier coefficients G[b][row][j] -> symmetric (p = 0) and
-// antisymmetric (p = 1) latitude folds, split into A[m][p][r][j].
+// antisymmetric (p = 1) latitude folds, split into A[m][p][r][j].  A thread
+// folds 8 consecutive latitudes against their mirrors and writes 16-byte
+// stores.
 __global__ void tc_fold_forward_kernel(const float* __restrict__ G, int nf, int M,
                                        int J, int Jh, int Rp, int Kj,
                                        bf16* __restrict__ Ah, bf16* __restrict__ Al) {
   const int m = blockIdx.y;
   const int rows = (m == 0) ? nf : 2 * nf;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (size_t)rows * Kj) return;
-  const int j = idx % Kj;
-  const int r = idx / Kj;
+  const int gw = Kj / 8;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)rows * gw) return;
+  const int g = idx % gw;
+  const int r = idx / gw;
   int b, row;
   tc_row_map(m, r, b, row);
-  float s = 0.f, d = 0.f;
-  if (j < Jh) {
-    const float* g = G + ((size_t)b * M + row) * J;
-    float g1 = g[j];
-    int jm = J - 1 - j;
-    float g2 = (jm != j) ? g[jm] : 0.f;
-    s = g1 + g2;
-    d = g1 - g2;
+  const float* gr = G + ((size_t)b * M + row) * J;
+  const int j0 = 8 * g;
+  float sv[8], dv[8];
+  if (j0 + 8 <= Jh && (J & 3) == 0) {
+    // Aligned fast path: j0..j0+7 and J-8-j0..J-1-j0 are float4 pairs.
+    const float4 a0 = *reinterpret_cast<const float4*>(gr + j0);
+    const float4 a1 = *reinterpret_cast<const float4*>(gr + j0 + 4);
+    const float4 b0 = *reinterpret_cast<const float4*>(gr + J - 8 - j0);
+    const float4 b1 = *reinterpret_cast<const float4*>(gr + J - 4 - j0);
+    const float d[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float e[8] = {b1.w, b1.z, b1.y, b1.x, b0.w, b0.z, b0.y, b0.x};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      sv[i] = d[i] + e[i];
+      dv[i] = d[i] - e[i];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int j = j0 + i;
+      float s = 0.f, d = 0.f;
+      if (j < Jh) {
+        const float g1 = gr[j];
+        const int jm = J - 1 - j;
+        const float g2 = (jm != j) ? gr[jm] : 0.f;
+        s = g1 + g2;
+        d = g1 - g2;
+      }
+      sv[i] = s;
+      dv[i] = d;
+    }
   }
-  bf16 h, l;
-  size_t o0 = ((size_t)(m * 2) * Rp + r) * Kj + j;
-  size_t o1 = ((size_t)(m * 2 + 1) * Rp + r) * Kj + j;
-  split_bf16(s, h, l);
-  Ah[o0] = h;
-  Al[o0] = l;
-  split_bf16(d, h, l);
-  Ah[o1] = h;
-  Al[o1] = l;
+  const size_t o0 = ((size_t)(m * 2) * Rp + r) * Kj + j0;
+  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + r) * Kj + j0;
+  store_split8(sv, Ah + o0, Al + o0);
+  store_split8(dv, Ah + o1, Al + o1);
 }
 
 // ---------------------------------------------------------------------------
@@ -675,8 +708,7 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
     const int n = nf - f0 < t->cap ? nf - f0 : t->cap;
     Segs sub = seg_offset(in, f0, n, ms);
     const int max_rows = 2 * n;
-    const int kw = t->Kp;
-    dim3 g1((unsigned)(((size_t)max_rows * kw + 255) / 256), p->lw);
+    dim3 g1((unsigned)(((size_t)max_rows * (t->Kp / 8) + 255) / 256), p->lw);
     tc_split_inverse_kernel<<<g1, 256, 0, st>>>(sub, n, p->M, p->L, t->Rp, t->Kp, t->Aih,
                                                 t->Ail);
     DINO_TRY(check_launch("tc_split_inverse"));
@@ -708,7 +740,7 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
   for (int f0 = 0; f0 < nf; f0 += t->cap) {
     const int n = nf - f0 < t->cap ? nf - f0 : t->cap;
     const int max_rows = 2 * n;
-    dim3 g1((unsigned)(((size_t)max_rows * t->Kj + 255) / 256), p->lw);
+    dim3 g1((unsigned)(((size_t)max_rows * (t->Kj / 8) + 255) / 256), p->lw);
     tc_fold_forward_kernel<<<g1, 256, 0, st>>>(G + f0 * fs, n, p->M, p->J, p->Jh, t->Rp, t->Kj,
                                                t->Afh, t->Afl);
     DINO_TRY(check_launch("tc_fold_forward"));
