@@ -469,6 +469,36 @@ __device__ __forceinline__ void fft_passes(float2* a, float2* b,
   }
 }
 
+// Copies a rows x kFftJS tile (row stride J floats) into shared memory
+// (row stride kFftJS) with every thread's loads issued before its stores:
+// float4 loads when rows start 16-byte aligned and the tile is full, else
+// scalar loads with zero fill past ncol.
+template <int kMaxRows>
+__device__ __forceinline__ void stage_tile(const float* __restrict__ src, int rows,
+                                           int J, int ncol, float* dst) {
+  if ((J & 3) == 0 && ncol == kFftJS) {
+    constexpr int kChunks = (kMaxRows * 4 + kFftThreads - 1) / kFftThreads;
+    float4 v[kChunks];
+#pragma unroll
+    for (int i = 0; i < kChunks; ++i) {
+      const int t = threadIdx.x + i * kFftThreads;
+      const int r = t >> 2, q = t & 3;
+      v[i] = (r < rows) ? *reinterpret_cast<const float4*>(src + (size_t)r * J + 4 * q)
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < kChunks; ++i) {
+      const int t = threadIdx.x + i * kFftThreads;
+      if ((t >> 2) < rows) reinterpret_cast<float4*>(dst)[t] = v[i];
+    }
+  } else {
+    for (int t = threadIdx.x; t < rows * kFftJS; t += kFftThreads) {
+      const int r = t / kFftJS, c = t % kFftJS;
+      dst[t] = (c < ncol) ? src[(size_t)r * J + c] : 0.f;
+    }
+  }
+}
+
 // Fourier coefficients F[b][row][j] -> nodal[b][i][j] (optionally scaled by
 // wq[j], which gives the adjoint of the weighted forward transform).
 // Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]) is formed from
@@ -498,11 +528,23 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
   const float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
   const float half_inv_sqrt_pi = 0.28209479177387814f;
+  // With two or more buffers, the coefficient tile (M <= 2N - 1 rows) is
+  // first staged in A, which the passes overwrite only after Zs is formed.
+  constexpr bool kStaged = kBufs > 1;
+  const float* src = Fb;
+  int sJ = J;
+  if constexpr (kStaged) {
+    const int rows = min(M, 2 * min(lw, N) - 1);  // rows X() reads; <= 2N - 1
+    stage_tile<2 * N>(Fb, rows, J, ncol, reinterpret_cast<float*>(A));
+    __syncthreads();
+    src = reinterpret_cast<const float*>(A);
+    sJ = kFftJS;
+  }
   auto X = [&](int k, int c) -> float2 {
     if (c >= ncol || k >= lw || k >= N) return make_float2(0.f, 0.f);
-    if (k == 0) return make_float2(Fb[c] * inv_sqrt_2pi, 0.f);
-    return make_float2(Fb[(size_t)(2 * k - 1) * J + c] * half_inv_sqrt_pi,
-                       -Fb[(size_t)(2 * k) * J + c] * half_inv_sqrt_pi);
+    if (k == 0) return make_float2(src[c] * inv_sqrt_2pi, 0.f);
+    return make_float2(src[(size_t)(2 * k - 1) * sJ + c] * half_inv_sqrt_pi,
+                       -src[(size_t)(2 * k) * sJ + c] * half_inv_sqrt_pi);
   };
   // Pairs (k, N - k), k = 0..N/2; k = 0 pairs with the (zero) Nyquist term.
   for (int item = tid; item < (N / 2 + 1) * kFftJS; item += kFftThreads) {
@@ -556,12 +598,20 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
   }
   __syncthreads();
   const float* xb = x + (size_t)b * (2 * N) * J + j0;
+  // The first pass reads the nodal tile straight from global memory, which
+  // overlaps the loads with its butterflies.
   auto first = [xb, ncol, J](int n, int c) {
     if (c >= ncol) return make_float2(0.f, 0.f);
     return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
   };
   auto last = [Zs](int n, int c, float2 v) { Zs[n * kFftJS + c] = v; };
-  fft_passes<N, -1>(A, Bf, twn, first, last);
+  fft_passes<N, -1>(A, Bf, twn, first, last); else {
+    auto first = [xb, ncol, J](int n, int c) {
+      if (c >= ncol) return make_float2(0.f, 0.f);
+      return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
+    };
+    fft_passes<N, -1>(A, Bf, twn, first, last);
+  }
   __syncthreads();
   float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
