@@ -605,13 +605,7 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
     return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
   };
   auto last = [Zs](int n, int c, float2 v) { Zs[n * kFftJS + c] = v; };
-  fft_passes<N, -1>(A, Bf, twn, first, last); else {
-    auto first = [xb, ncol, J](int n, int c) {
-      if (c >= ncol) return make_float2(0.f, 0.f);
-      return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
-    };
-    fft_passes<N, -1>(A, Bf, twn, first, last);
-  }
+  fft_passes<N, -1>(A, Bf, twn, first, last);
   __syncthreads();
   float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
