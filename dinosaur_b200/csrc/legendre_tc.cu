@@ -43,6 +43,8 @@ struct TcTables {
   int* d_err = nullptr;
   int stages_inv = 0, stages_fwd = 0;
   size_t smem_inv = 0, smem_fwd = 0;
+  // N sub-ranges per (m, row tile) CTA and their width (B tile rows).
+  int nsplit_inv = 1, nsplit_fwd = 1, Nsub_inv = 0, Nsub_fwd = 0;
 };
 
 __host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m - 1) / m * m; }
@@ -327,7 +329,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 struct TcArgs {
   int nf, M, L, J, Jh;
   int Rp;        // A slab rows
-  int Nrows;     // B tile rows (Np or Nf)
+  int Nrows;     // rows of one (m, parity) B table (Np or Nf)
+  int Nsub;      // B tile rows = N columns of this CTA (blockIdx.z-th range)
   int stages;
   int tmem_cols; // allocated TMEM columns (power of two)
   float* out;    // inverse: Fourier [nf][M][J]; forward: modal [nf][M][L]
@@ -335,7 +338,7 @@ struct TcArgs {
 };
 
 template <bool kForward>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kTcThreads, 2)
 legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
                    const __grid_constant__ CUtensorMap tAl,
                    const __grid_constant__ CUtensorMap tBh,
@@ -353,22 +356,29 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
 
   const int Lm = a.L - m;
   const int n_par[2] = {(Lm + 1) >> 1, Lm >> 1};
-  int kblk[2], ksteps[2], ncols[2];
+  // This CTA's N range: latitudes (inverse) or l' (forward) lo .. lo+Nsub-1.
+  const int lo = blockIdx.z * a.Nsub;
+  int kblk[2], ksteps[2], ncols[2], cnt[2];
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     if (!kForward) {
       kblk[p] = (n_par[p] + 63) / 64;
       ksteps[p] = (n_par[p] + 15) / 16;
-      ncols[p] = a.Nrows;
+      ncols[p] = a.Nsub;
+      cnt[p] = n_par[p];
     } else {
-      kblk[p] = n_par[p] ? (a.Jh + 63) / 64 : 0;
+      cnt[p] = max(0, min(n_par[p] - lo, a.Nsub));
+      kblk[p] = cnt[p] ? (a.Jh + 63) / 64 : 0;
       ksteps[p] = (a.Jh + 15) / 16;
-      ncols[p] = round_up(n_par[p] > 0 ? n_par[p] : 16, 16);
+      ncols[p] = round_up(cnt[p] > 0 ? cnt[p] : 16, 16);
     }
   }
+  // Uniform early exits: no output column in this range.
+  if (kForward && cnt[0] == 0) return;
+  if (!kForward && lo >= a.Jh) return;
   const int nblocks = kblk[0] + kblk[1];
-  const uint32_t tile_a = 128u * 128u;              // 128 rows x 64 bf16
-  const uint32_t tile_b = (uint32_t)a.Nrows * 128u;  // Nrows x 64 bf16
+  const uint32_t tile_a = 128u * 128u;             // 128 rows x 64 bf16
+  const uint32_t tile_b = (uint32_t)a.Nsub * 128u;  // Nsub rows x 64 bf16
   const uint32_t stage_bytes = 2 * tile_a + 2 * tile_b;
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
   uint8_t* base = smem_raw + pad;
@@ -395,7 +405,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
-  const int acc_cols = a.Nrows;  // parity p accumulates at column p * Nrows
+  const int acc_cols = a.Nsub;  // parity p accumulates at column p * Nsub
 
   if (threadIdx.x == 0) {
     // TMA producer.
@@ -408,7 +418,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
       uint8_t* st = base + (size_t)s * stage_bytes;
       mbar_expect_tx(&full_bar[s], stage_bytes);
       const int ya = (m * 2 + p) * a.Rp + tile * 128;
-      const int yb = (m * 2 + p) * a.Nrows;
+      const int yb = (m * 2 + p) * a.Nrows + lo;
       tma_load_2d(st, &tAh, &full_bar[s], k * 64, ya);
       tma_load_2d(st + tile_a, &tAl, &full_bar[s], k * 64, ya);
       tma_load_2d(st + 2 * tile_a, &tBh, &full_bar[s], k * 64, yb);
@@ -459,7 +469,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
     const int row0 = tile * 128 + warp * 32;  // first row of this warp
     if (!kForward) {
       const bool vec = (a.J & 3) == 0;
-      for (int c = 0; c < a.Nrows / 16; ++c) {
+      for (int c = 0; c < a.Nsub / 16; ++c) {
         float e[16], od[16];
         tmem_ld16(lane_base + c * 16, e);
         if (n_par[1] > 0) {
@@ -476,8 +486,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
           stage[lane * kStride + 16 + (15 - t)] = e[t] - od[t];
         }
         __syncwarp();
-        const int jb = 16 * c;
-        const int jm = a.J - 16 * (c + 1);
+        const int jb = lo + 16 * c;
+        const int jm = a.J - jb - 16;
         // 4 threads per row, 8 rows per pass, 4 passes; two half-blocks.
         for (int pass = 0; pass < 8; ++pass) {
           const int half = pass >> 2;                 // 0: direct, 1: mirror
@@ -512,8 +522,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
         __syncwarp();
       }
     } else {
-      // Structural zeros l < m, one row at a time across the warp.
-      for (int r = 0; r < 32; ++r) {
+      // Structural zeros l < m (first N range only), one row at a time.
+      for (int r = 0; r < 32 && lo == 0; ++r) {
         const int rr = row0 + r;
         if (rr >= rows) break;
         int b, row;
@@ -521,11 +531,11 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
         float* o = a.out + ((size_t)b * a.M + row) * a.L;
         for (int l = lane; l < m; l += 32) o[l] = 0.f;
       }
-      const int nchunks = (max(n_par[0], n_par[1]) + 15) / 16;
+      const int nchunks = (max(cnt[0], cnt[1]) + 15) / 16;
       for (int c = 0; c < nchunks; ++c) {
         float e[16], od[16];
         tmem_ld16(lane_base + c * 16, e);
-        if (n_par[1] > 0) {
+        if (cnt[1] > 0) {
           tmem_ld16(lane_base + acc_cols + c * 16, od);
         } else {
 #pragma unroll
@@ -538,12 +548,12 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
           stage[lane * kStride + 2 * t + 1] = od[t];
         }
         __syncwarp();
-        const int lbase = m + 32 * c;
+        const int lbase = m + 2 * (lo + 16 * c);
         for (int r = 0; r < 32; ++r) {
           const int rr = row0 + r;
           if (rr >= rows) break;
           const int l = lbase + lane;
-          const int lp = 16 * c + (lane >> 1);
+          const int lp = lo + 16 * c + (lane >> 1);
           const bool keep = (lane & 1) ? (lp < n_par[1]) : (lp < n_par[0]);
           if (keep && l < a.L) {
             int b, row;
@@ -602,9 +612,11 @@ static int make_map(CUtensorMap* tm, const bf16* ptr, int inner, long long rows,
   return DINO_OK;
 }
 
+// Pipeline depth within ~104 KB of shared memory, so that two CTAs share an
+// SM (each also holds up to 256 TMEM columns).
 static int pick_stages(int nrows, size_t* smem) {
   const size_t stage = 2 * 128 * 128 + 2 * (size_t)nrows * 128;
-  int s = (int)((200 * 1024) / stage);
+  int s = (int)((104 * 1024) / stage);
   if (s > kMaxStages) s = kMaxStages;
   if (s < 2) s = 2;
   *smem = stage * s + 1024;
@@ -657,17 +669,22 @@ int tc_tables_build(dino_plan* p) {
   tc_table_kernel<<<grid, 128>>>(p->lw, p->L, p->Jh, p->d_x64, t->Kp, t->Np, t->Kj, t->Nf,
                                  t->Bih, t->Bil, t->Bfh, t->Bfl);
   DINO_TRY(check_launch("tc_table"));
+  // Two N ranges per (m, row tile) once a table has 64 or more rows.
+  t->nsplit_inv = t->Np >= 64 ? 2 : 1;
+  t->nsplit_fwd = t->Nf >= 64 ? 2 : 1;
+  t->Nsub_inv = round_up((t->Np + t->nsplit_inv - 1) / t->nsplit_inv, 16);
+  t->Nsub_fwd = round_up((t->Nf + t->nsplit_fwd - 1) / t->nsplit_fwd, 16);
   const long long rowsA = (long long)lw2 * t->Rp;
   DINO_TRY(make_map(&t->tAih, t->Aih, t->Kp, rowsA, 128));
   DINO_TRY(make_map(&t->tAil, t->Ail, t->Kp, rowsA, 128));
-  DINO_TRY(make_map(&t->tBih, t->Bih, t->Kp, (long long)lw2 * t->Np, t->Np));
-  DINO_TRY(make_map(&t->tBil, t->Bil, t->Kp, (long long)lw2 * t->Np, t->Np));
+  DINO_TRY(make_map(&t->tBih, t->Bih, t->Kp, (long long)lw2 * t->Np, t->Nsub_inv));
+  DINO_TRY(make_map(&t->tBil, t->Bil, t->Kp, (long long)lw2 * t->Np, t->Nsub_inv));
   DINO_TRY(make_map(&t->tAfh, t->Afh, t->Kj, rowsA, 128));
   DINO_TRY(make_map(&t->tAfl, t->Afl, t->Kj, rowsA, 128));
-  DINO_TRY(make_map(&t->tBfh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, t->Nf));
-  DINO_TRY(make_map(&t->tBfl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, t->Nf));
-  t->stages_inv = pick_stages(t->Np, &t->smem_inv);
-  t->stages_fwd = pick_stages(t->Nf, &t->smem_fwd);
+  DINO_TRY(make_map(&t->tBfh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, t->Nsub_fwd));
+  DINO_TRY(make_map(&t->tBfl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, t->Nsub_fwd));
+  t->stages_inv = pick_stages(t->Nsub_inv, &t->smem_inv);
+  t->stages_fwd = pick_stages(t->Nsub_fwd, &t->smem_fwd);
   DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)t->smem_inv));
@@ -720,11 +737,12 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
     a.Jh = p->Jh;
     a.Rp = t->Rp;
     a.Nrows = t->Np;
+    a.Nsub = t->Nsub_inv;
     a.stages = t->stages_inv;
-    a.tmem_cols = tmem_cols_for(2 * t->Np);
+    a.tmem_cols = tmem_cols_for(2 * t->Nsub_inv);
     a.out = out + f0 * fs;
     a.err = t->d_err;
-    dim3 g2(ceil_div(max_rows, 128), p->lw);
+    dim3 g2(ceil_div(max_rows, 128), p->lw, t->nsplit_inv);
     legendre_tc_kernel<false><<<g2, kTcThreads, t->smem_inv, st>>>(t->tAih, t->tAil, t->tBih,
                                                                    t->tBil, a);
     DINO_TRY(check_launch("legendre_tc_inverse"));
@@ -752,11 +770,12 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
     a.Jh = p->Jh;
     a.Rp = t->Rp;
     a.Nrows = t->Nf;
+    a.Nsub = t->Nsub_fwd;
     a.stages = t->stages_fwd;
-    a.tmem_cols = tmem_cols_for(2 * t->Nf);
+    a.tmem_cols = tmem_cols_for(2 * t->Nsub_fwd);
     a.out = out + f0 * ms;
     a.err = t->d_err;
-    dim3 g2(ceil_div(max_rows, 128), p->lw);
+    dim3 g2(ceil_div(max_rows, 128), p->lw, t->nsplit_fwd);
     legendre_tc_kernel<true><<<g2, kTcThreads, t->smem_fwd, st>>>(t->tAfh, t->tAfl, t->tBfh,
                                                                   t->tBfl, a);
     DINO_TRY(check_launch("legendre_tc_forward"));
