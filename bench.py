@@ -261,8 +261,10 @@ def run_ours(args):
       dist.barrier()
 
   fields = FIELDS
-  grid = sh.Grid.TL255(spherical_harmonics_impl=lambda **kw: sh.CudaSphericalHarmonics(
-      precision=args.precision, **kw))
+  make_grid = lambda precision: sh.Grid.TL255(
+      spherical_harmonics_impl=functools.partial(sh.CudaSphericalHarmonics,
+                                                 precision=precision))
+  grid = make_grid(args.precision)
   plan = grid.plan
   x_host = torch.from_numpy(modal_input(fields, seed=replica_seed(rank))).pin_memory()
   x = x_host.cuda()
@@ -356,7 +358,27 @@ def run_ours(args):
 
   extra = {}
   if not args.no_extra and world == 1:
-    extra = pe_extras(torch)
+    # The other Legendre form on the same workload, for the split-BF16 vs
+    # FP32 comparison.
+    other = 'fp32' if args.precision == 'bf16x3' else 'bf16x3'
+    g2 = make_grid(other)
+    for _ in range(args.warmup):
+      y2 = g2.plan.forward(g2.plan.inverse(x))
+    torch.cuda.synchronize()
+    rt2 = float(torch.linalg.vector_norm(y2 - x) / torch.linalg.vector_norm(x))
+    b0 = torch.cuda.Event(enable_timing=True)
+    b1 = torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    for _ in range(args.steps):
+      y2 = g2.plan.forward(g2.plan.inverse(x))
+    b1.record(stream)
+    torch.cuda.synchronize()
+    ms2 = b0.elapsed_time(b1) / args.steps
+    extra['sht_' + other] = {'value': aggregate_tflops(sht_flops(fields), 1, ms2),
+                             'unit': 'TFLOP/s', 'ms_per_step': ms2,
+                             'round_trip_rel_l2': rt2}
+    del g2, y2
+    extra.update(pe_extras(torch))
 
   if rank == 0:
     line = {
@@ -471,7 +493,7 @@ def main():
   ap.add_argument('--steps', type=int, default=20)
   ap.add_argument('--warmup', type=int, default=5)
   ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-  ap.add_argument('--precision', default=os.environ.get('DINO_BENCH_PRECISION', 'fp32'),
+  ap.add_argument('--precision', default=os.environ.get('DINO_BENCH_PRECISION', 'bf16x3'),
                   choices=['fp32', 'bf16x3'])
   ap.add_argument('--no-extra', action='store_true')
   ap.add_argument('--no-cpu-baseline', action='store_true')
