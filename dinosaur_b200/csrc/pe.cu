@@ -86,6 +86,10 @@ struct dino_pe {
   float* d_g[2] = {nullptr, nullptr};
   float* d_Y = nullptr;
   float* d_ystar = nullptr;  // Y* of the current stage (implicit planes)
+  // l-major operands of the per-l implicit products: [L][2n][Cp].
+  int Cp = 0;
+  float* d_lm_in = nullptr;
+  float* d_lm_out = nullptr;
   // Adjoint work (allocated by the first VJP call).
   float* d_xbar_n = nullptr;  // nodal cotangents, n_inv planes
   float* d_xbar_m = nullptr;  // their modal adjoint, n_inv planes
@@ -100,7 +104,7 @@ namespace dino {
 
 // Offsets into d_lev (floats); every array has K entries (c2ci has K-1).
 struct LevOff {
-  int dsig, c2ci, alpha, tref, sumsig, sigma, kv, trefdiff;
+  int dsig, c2ci, alpha, tref, sumsig, sigma, kv, trefdiff, logsp0;
   int total;
 };
 
@@ -114,7 +118,8 @@ static LevOff lev_offsets(int K) {
   o.sigma = 5 * K;
   o.kv = 6 * K;
   o.trefdiff = 7 * K;  // (Tref[k+1]-Tref[k]) * c2ci[k]
-  o.total = 8 * K;
+  o.logsp0 = 8 * K;    // log(sigma_k / p0) (Held-Suarez)
+  o.total = 9 * K;
   return o;
 }
 
@@ -221,7 +226,7 @@ struct NodalArgs {
 
 __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
   const size_t IJ = (size_t)a.I * a.J;
-  size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= IJ) return;
   const int mb = blockIdx.y;
   const int K = a.K;
@@ -233,21 +238,28 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
   const float* alpha = a.lev + a.lo.alpha;
   const float* tref = a.lev + a.lo.tref;
   const float* sumsig = a.lev + a.lo.sumsig;
-  const float* nod = a.nod;
-  float* fwd = a.fwd;
-#define NOD(p, k) nod[pl(p, mb, K, k) * IJ + col]
-#define FWD(p, k) fwd[pl(p, mb, K, k) * IJ + col]
-  const float gx = nod[((size_t)a.p_gx + mb) * IJ + col];
-  const float gy = nod[((size_t)a.p_gy + mb) * IJ + col];
+  // Level-0 pointers of this column for each kind; level k is at [k * IJ].
+  auto in = [&](int p) { return a.nod + pl(p, mb, K, 0) * IJ + col; };
+  auto out = [&](int p) { return a.fwd + pl(p, mb, K, 0) * IJ + col; };
+  const float* Pu = in(a.p_u);
+  const float* Pv = in(a.p_v);
+  const float* Pd = in(a.p_div);
+  const float* Pz = in(a.p_vort);
+  const float* PT = in(a.p_temp);
+  const float gx = a.nod[((size_t)a.p_gx + mb) * IJ + col];
+  const float gy = a.nod[((size_t)a.p_gy + mb) * IJ + col];
+  // Tracer planes are a.mem * K apart.
+  const size_t tstride = (size_t)a.mem * K * IJ;
+  const float* Pq = in(a.p_tr);
 
   // Pass 1: column totals of u.grad(ln ps) and of (div + u.grad ln ps), both
   // weighted by the layer thickness (cumulative_sigma_integral, last level).
   float Fe = 0.f, Ff = 0.f;
   for (int k = 0; k < K; ++k) {
-    float u = NOD(a.p_u, k), v = NOD(a.p_v, k), d = NOD(a.p_div, k);
-    float ugl = (u * gx + v * gy) * sec2;
+    const size_t o = (size_t)k * IJ;
+    const float ugl = (Pu[o] * gx + Pv[o] * gy) * sec2;
     Fe += ugl * dsig[k];
-    Ff += (d + ugl) * dsig[k];
+    Ff += (Pd[o] + ugl) * dsig[k];
   }
 
   // Moist: geopotential of the virtual-temperature difference, G @ td with
@@ -255,51 +267,59 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
   // sum evaluated bottom-up (get_geopotential_weights_sigma, :306-338).
   if (a.hum >= 0) {
     float suffix = 0.f;
-    const int ph = a.p_tr + a.hum * a.mem * K;
+    const float* Ph = Pq + a.hum * tstride;
+    float* Ogh = out(a.o_gh);
     for (int k = K - 1; k >= 0; --k) {
-      float q = NOD(ph, k), T = NOD(a.p_temp, k);
-      float td = q * (T + tref[k]) * (a.Rv_over_R - 1.f);
-      FWD(a.o_gh, k) = a.R * (alpha[k] * td + suffix);
+      const size_t o = (size_t)k * IJ;
+      const float td = Ph[o] * (PT[o] + tref[k]) * (a.Rv_over_R - 1.f);
+      Ogh[o] = a.R * (alpha[k] * td + suffix);
       if (k > 0) suffix += (alpha[k] + alpha[k - 1]) * td;
     }
   }
 
+  float* OAu = out(a.o_Au);
+  float* OAv = out(a.o_Av);
+  float* OKE = out(a.o_KE);
+  float* OuT = out(a.o_uT);
+  float* OvT = out(a.o_vT);
+  float* OTn = out(a.o_Tn);
+  float* Otr = out(a.o_tr);
   // Pass 2: everything else, streaming over levels top-down with a window
   // of (k-1, k, k+1) for the vertically advected fields.
   float u_p = 0.f, v_p = 0.f, T_p = 0.f;
-  float u_c = NOD(a.p_u, 0), v_c = NOD(a.p_v, 0), T_c = NOD(a.p_temp, 0);
+  float u_c = Pu[0], v_c = Pv[0], T_c = PT[0];
   float q_p[kMaxTracers], q_c[kMaxTracers], q_n[kMaxTracers];
 #pragma unroll
   for (int t = 0; t < kMaxTracers; ++t) {
     q_p[t] = 0.f;
-    q_c[t] = (t < a.nT) ? NOD(a.p_tr + t * a.mem * K, 0) : 0.f;
+    q_c[t] = (t < a.nT) ? Pq[t * tstride] : 0.f;
     q_n[t] = 0.f;
   }
   float fe = 0.f, ff = 0.f, fe_prev = 0.f, ff_prev = 0.f;
   float sd_up_f = 0.f, sd_up_e = 0.f;  // sigma-dot at k - 1/2
-  float hs_ps = 0.f, sin2 = 0.f, cos2 = 0.f, lnps_n = 0.f;
+  float lnps_n = 0.f, sin2 = 0.f, cos2 = 0.f;
   if (a.hs) {
-    lnps_n = nod[((size_t)a.p_lnps + mb) * IJ + col];
-    hs_ps = expf(lnps_n);
+    lnps_n = a.nod[((size_t)a.p_lnps + mb) * IJ + col];
     sin2 = a.lat[2 * a.J + j];
     cos2 = a.lat[3 * a.J + j];
   }
-  float gqx = 0.f, gqy = 0.f, laplnps = 0.f;
-  if (a.hum >= 0) laplnps = nod[((size_t)a.p_laplnps + mb) * IJ + col];
+  float laplnps = 0.f;
+  if (a.hum >= 0) laplnps = a.nod[((size_t)a.p_laplnps + mb) * IJ + col];
 
   for (int k = 0; k < K; ++k) {
+    const size_t o = (size_t)k * IJ;
     const bool has_next = k + 1 < K;
     float u_n = 0.f, v_n = 0.f, T_n = 0.f;
     if (has_next) {
-      u_n = NOD(a.p_u, k + 1);
-      v_n = NOD(a.p_v, k + 1);
-      T_n = NOD(a.p_temp, k + 1);
+      u_n = Pu[o + IJ];
+      v_n = Pv[o + IJ];
+      T_n = PT[o + IJ];
     }
 #pragma unroll
     for (int t = 0; t < kMaxTracers; ++t)
-      if (t < a.nT) q_n[t] = has_next ? NOD(a.p_tr + t * a.mem * K, k + 1) : 0.f;
-    const float zeta = NOD(a.p_vort, k);
-    const float div = NOD(a.p_div, k);
+      if (t < a.nT) q_n[t] = has_next ? Pq[t * tstride + o + IJ] : 0.f;
+    const float zeta = Pz[o];
+    const float div = Pd[o];
     const float ugl = (u_c * gx + v_c * gy) * sec2;
     fe += ugl * dsig[k];
     ff += (div + ugl) * dsig[k];
@@ -340,11 +360,11 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
       Au += kv * u_c * sec2;
       Av += kv * v_c * sec2;
     }
-    FWD(a.o_Au, k) = Au;
-    FWD(a.o_Av, k) = Av;
-    FWD(a.o_KE, k) = (u_c * u_c + v_c * v_c) * sec2 * 0.5f;
-    FWD(a.o_uT, k) = u_c * T_c * sec2;
-    FWD(a.o_vT, k) = v_c * T_c * sec2;
+    OAu[o] = Au;
+    OAv[o] = Av;
+    OKE[o] = (u_c * u_c + v_c * v_c) * sec2 * 0.5f;
+    OuT[o] = u_c * T_c * sec2;
+    OvT[o] = v_c * T_c * sec2;
     // Temperature: horizontal nodal term, vertical advection, adiabatic.
     float Tn = T_c * div;
     if (a.vadv) Tn += vadv(T_p, T_c, T_n, sd_dn_f, sd_up_f);
@@ -368,36 +388,36 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
       var_part = (tv_var + tv_ref) * (ugl - gf);
     }
     Tn += a.kappa * (mean_part + var_part);
-    FWD(a.o_Tn, k) = Tn;
+    OTn[o] = Tn;
     // Tracers: u q, v q (times sec^2) and q div + vertical advection.
 #pragma unroll
     for (int t = 0; t < kMaxTracers; ++t) {
       if (t >= a.nT) break;
-      const int ob = a.o_tr + 3 * t * a.mem * K;
-      FWD(ob, k) = u_c * q_c[t] * sec2;
-      FWD(ob + a.mem * K, k) = v_c * q_c[t] * sec2;
+      float* ob = Otr + 3 * t * tstride;
+      ob[o] = u_c * q_c[t] * sec2;
+      ob[tstride + o] = v_c * q_c[t] * sec2;
       float qn = q_c[t] * div;
       if (a.vadv) qn += vadv(q_p[t], q_c[t], q_n[t], sd_dn_f, sd_up_f);
-      FWD(ob + 2 * a.mem * K, k) = qn;
+      ob[2 * tstride + o] = qn;
     }
     if (a.hum >= 0) {
-      gqx = NOD(a.p_gqx, k);
-      gqy = NOD(a.p_gqy, k);
+      const float gqx = a.nod[pl(a.p_gqx, mb, K, k) * IJ + col];
+      const float gqy = a.nod[pl(a.p_gqy, mb, K, k) * IJ + col];
       const float coef = tref[k] * a.Rv_minus_R;
-      FWD(a.o_vh, k) = coef * sec2 * (gx * gqy - gy * gqx);
-      FWD(a.o_dh, k) = coef * sec2 * (gqx * gx + gqy * gy) +
-                       q_h * laplnps * tref[k] * a.Rv_minus_R;
+      a.fwd[pl(a.o_vh, mb, K, k) * IJ + col] = coef * sec2 * (gx * gqy - gy * gqx);
+      a.fwd[pl(a.o_dh, mb, K, k) * IJ + col] =
+          coef * sec2 * (gqx * gx + gqy * gy) + q_h * laplnps * tref[k] * a.Rv_minus_R;
     }
     if (a.hs) {
-      // held_suarez.py:105-120, :138-151
+      // held_suarez.py:105-120, :138-151, with log(p / p0) = log(sigma / p0)
+      // + ln ps and (p / p0)^kappa = exp(kappa log(p / p0)).
       const float sig = a.lev[a.lo.sigma + k];
       const float cutoff = fmaxf(0.f, (sig - a.hs_sigma_b) / (1.f - a.hs_sigma_b));
       const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (cutoff * cos2 * cos2);
-      const float pp0 = sig * hs_ps / a.hs_p0;
-      float teq = powf(pp0, a.kappa) *
-                  (a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * logf(pp0) * cos2);
+      const float lp = a.lev[a.lo.logsp0 + k] + lnps_n;
+      float teq = expf(a.kappa * lp) * (a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * lp * cos2);
       teq = fmaxf(a.hs_minT, teq);
-      FWD(a.o_hsT, k) = -kt * (tref[k] + T_c - teq);
+      a.fwd[pl(a.o_hsT, mb, K, k) * IJ + col] = -kt * (tref[k] + T_c - teq);
     }
     // Advance the window.
     fe_prev = fe;
@@ -412,9 +432,7 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
       q_c[t] = q_n[t];
     }
   }
-  fwd[((size_t)a.o_lnps + mb) * IJ + col] = -Fe;
-#undef NOD
-#undef FWD
+  a.fwd[((size_t)a.o_lnps + mb) * IJ + col] = -Fe;
 }
 
 // ---------------------------------------------------------------------------
@@ -634,9 +652,9 @@ __global__ void __launch_bounds__(128) pe_nodal_adjoint_kernel(NodalAdjArgs A) {
   }
   float laplnps = 0.f;
   if (moist) laplnps = nod[((size_t)a.p_laplnps + mb) * IJ + col];
-  float hs_ps = 0.f, sin2 = 0.f, cos2 = 0.f;
+  float lnps_n = 0.f, sin2 = 0.f, cos2 = 0.f;
   if (a.hs) {
-    hs_ps = expf(nod[((size_t)a.p_lnps + mb) * IJ + col]);
+    lnps_n = nod[((size_t)a.p_lnps + mb) * IJ + col];
     sin2 = a.lat[2 * a.J + j];
     cos2 = a.lat[3 * a.J + j];
   }
@@ -750,9 +768,9 @@ __global__ void __launch_bounds__(128) pe_nodal_adjoint_kernel(NodalAdjArgs A) {
       const float sig = a.lev[a.lo.sigma + k];
       const float cutoff = fmaxf(0.f, (sig - a.hs_sigma_b) / (1.f - a.hs_sigma_b));
       const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (cutoff * cos2 * cos2);
-      const float pp0 = sig * hs_ps / a.hs_p0;
-      const float pk = powf(pp0, kap);
-      const float B = a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * logf(pp0) * cos2;
+      const float lp = a.lev[a.lo.logsp0 + k] + lnps_n;  // log(p / p0)
+      const float pk = expf(kap * lp);
+      const float B = a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * lp * cos2;
       Tb += -kt * hsTb;
       if (pk * B > a.hs_minT) lnpsb += kt * hsTb * pk * (kap * B - a.hs_dThz * cos2);
     }
@@ -1119,39 +1137,103 @@ __global__ void pe_combine_kernel(CombineArgs a) {
 // Per-(l, column) application of an implicit operator: for every total
 // wavenumber l, Out[R x C] = A_l[R x nin] Ys[nin x C], where the C = members * M
 // columns are the (member, m-row) pairs and Ys stacks the n = 2K+1 implicit
-// planes (div, T', ln ps) of src (and, for nin = 2n, those of src2).  A CTA takes one l, 64 columns and 16*TR rows of
-// A_l: it stages A_l^T and the gathered Ys in shared memory and each thread
-// accumulates a TR x 4 register tile (broadcast A reads, float4 Ys reads).
-// Rows [0, n) go to `out`, rows [n, 2n) (kMatInvG) to `out2`.  Every element
-// is read and written by one CTA, with a barrier in between, so src may
-// alias out.
-struct ApplyArgs {
-  const float* src;   // inputs [0, n), scaled by s1
-  const float* src2;  // inputs [n, 2n) when nin = 2n, scaled by s2
+// planes (div, T', ln ps) of src (and, for nin = 2n, those of src2).
+//
+// The state keeps l fastest ([plane][row][l]), so the operands go through an
+// l-major copy Y[l][k][c] (columns padded to Cp, a multiple of 64): a tiled
+// shared-memory transpose in (pe_lm_gather_kernel), the per-l product on
+// contiguous rows (pe_apply_kernel), and a tiled transpose out
+// (pe_lm_scatter_kernel) -- every global access is a full 128-byte row.
+
+struct LmArgs {
+  const float* src;   // gather: stacked planes [0, n), scaled by s1
+  const float* src2;  // gather: stacked planes [n, 2n), scaled by s2
   float s1, s2;
-  const float* A;
-  float* out;
-  float* out2;
-  int R, n, nin, RP;
-  int K, M, L, C;
+  float* out;         // scatter: rows [0, n)
+  float* out2;        // scatter: rows [n, 2n)
+  float* lm;          // gather output / scatter input: [L][nk][Cp]
+  int nk, n, K, M, L, C, Cp;
   int p_div, p_temp, p_lnps;
   size_t ML;
 };
 
-constexpr int kApplyCols = 64;
-constexpr int kApplyMaxTR = 13;
-
-__device__ __forceinline__ size_t stacked_plane(const ApplyArgs& a, int i, int mb) {
+__device__ __forceinline__ size_t stacked_plane(const LmArgs& a, int i, int mb) {
   if (i < a.K) return pl(a.p_div, mb, a.K, i);
   if (i < 2 * a.K) return pl(a.p_temp, mb, a.K, i - a.K);
   return (size_t)a.p_lnps + mb;
 }
 
+// One 32 (columns) x 32 (l) tile of stacked plane k per CTA (256 threads).
+__global__ void __launch_bounds__(256) pe_lm_gather_kernel(LmArgs a) {
+  __shared__ float tile[32][33];
+  const int k = blockIdx.z;
+  const int l0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const bool first = k < a.n;
+  const float* base = first ? a.src : a.src2;
+  const int kk = first ? k : k - a.n;
+  const float sc = first ? a.s1 : a.s2;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int cc = ty + 8 * i, c = c0 + cc, l = l0 + tx;
+    float v = 0.f;
+    if (c < a.C && l < a.L) {
+      const int mb = c / a.M, row = c - mb * a.M;
+      v = sc * base[stacked_plane(a, kk, mb) * a.ML + (size_t)row * a.L + l];
+    }
+    tile[cc][tx] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int ll = ty + 8 * i, l = l0 + ll, c = c0 + tx;
+    if (l < a.L) a.lm[((size_t)l * a.nk + k) * a.Cp + c] = tile[tx][ll];
+  }
+}
+
+// Row r of the l-major product back into the state layout (rows [0, n) to
+// out, [n, 2n) to out2).
+__global__ void __launch_bounds__(256) pe_lm_scatter_kernel(LmArgs a) {
+  __shared__ float tile[32][33];
+  const int r = blockIdx.z;
+  const int l0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int ll = ty + 8 * i, l = l0 + ll, c = c0 + tx;
+    tile[ll][tx] = (l < a.L) ? a.lm[((size_t)l * a.nk + r) * a.Cp + c] : 0.f;
+  }
+  __syncthreads();
+  float* dst = r < a.n ? a.out : a.out2;
+  const int rr = r < a.n ? r : r - a.n;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int cc = ty + 8 * i, c = c0 + cc, l = l0 + tx;
+    if (c < a.C && l < a.L) {
+      const int mb = c / a.M, row = c - mb * a.M;
+      dst[stacked_plane(a, rr, mb) * a.ML + (size_t)row * a.L + l] = tile[tx][cc];
+    }
+  }
+}
+
+struct ApplyArgs {
+  const float* A;     // [L][nin][RP]: operator^T per l
+  const float* ylm;   // [L][nin][Cp]
+  float* olm;         // [L][R][Cp]
+  int R, nin, RP, Cp;
+};
+
+constexpr int kApplyCols = 64;
+constexpr int kApplyMaxTR = 13;
+
+// A CTA takes one l, 64 columns and 16*TR rows of A_l: it stages A_l^T and
+// the operand rows in shared memory and each thread accumulates a TR x 4
+// register tile (broadcast A reads, float4 operand reads and stores).
 template <int TR>
 __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
   constexpr int RPT = 16 * TR;
   extern __shared__ __align__(16) float smem[];
-  const int n = a.n, nin = a.nin;
+  const int nin = a.nin;
   float* At = smem;                    // [nin][RPT]
   float* Ys = At + (size_t)nin * RPT;  // [nin][kApplyCols]
   const int tid = threadIdx.x;
@@ -1166,26 +1248,12 @@ __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
       reinterpret_cast<float4*>(At)[e] =
           reinterpret_cast<const float4*>(Ag + (size_t)k * a.RP)[q];
     }
-  }
-  {
-    // Each thread gathers one column at every 4th stacked index; the column
-    // is decoded once and four loads are kept in flight.
-    constexpr int kLanes = 256 / kApplyCols;
-    const int cc = tid % kApplyCols, k0 = tid / kApplyCols;
-    const int c = c0 + cc;
-    const bool ok = c < a.C;
-    const int mb = ok ? c / a.M : 0;
-    const size_t off = (size_t)(ok ? c - mb * a.M : 0) * a.L + l;
-    const float* base = a.src + off;
-#pragma unroll 4
-    for (int k = k0; k < n; k += kLanes)
-      Ys[k * kApplyCols + cc] = ok ? a.s1 * base[stacked_plane(a, k, mb) * a.ML] : 0.f;
-    if (nin > n) {
-      const float* base2 = a.src2 + off;
-#pragma unroll 4
-      for (int k = k0; k < n; k += kLanes)
-        Ys[(n + k) * kApplyCols + cc] =
-            ok ? a.s2 * base2[stacked_plane(a, k, mb) * a.ML] : 0.f;
+    const float* Yg = a.ylm + (size_t)l * nin * a.Cp + c0;
+    constexpr int QC = kApplyCols / 4;
+    for (int e = tid; e < nin * QC; e += 256) {
+      const int k = e / QC, q = e - k * QC;
+      reinterpret_cast<float4*>(Ys)[e] =
+          reinterpret_cast<const float4*>(Yg + (size_t)k * a.Cp)[q];
     }
   }
   __syncthreads();
@@ -1207,20 +1275,13 @@ __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
       acc[i][3] = fmaf(av, y.w, acc[i][3]);
     }
   }
+  float* og = a.olm + (size_t)l * a.R * a.Cp + c0 + cg * 4;
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = c0 + cg * 4 + j;
-    if (c >= a.C) continue;
-    const int mb = c / a.M, row = c - mb * a.M;
-    const size_t off = (size_t)row * a.L + l;
-#pragma unroll
-    for (int i = 0; i < TR; ++i) {
-      const int r = r0 + rg * TR + i;
-      if (r >= a.R) continue;
-      float* dst = r < n ? a.out + stacked_plane(a, r, mb) * a.ML
-                         : a.out2 + stacked_plane(a, r - n, mb) * a.ML;
-      dst[off] = acc[i][j];
-    }
+  for (int i = 0; i < TR; ++i) {
+    const int r = r0 + rg * TR + i;
+    if (r < a.R)
+      *reinterpret_cast<float4*>(og + (size_t)r * a.Cp) =
+          make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
   }
 }
 
@@ -1272,29 +1333,39 @@ static void apply_launch(dim3 grid, size_t smem, cudaStream_t st, const ApplyArg
 static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
                         float* out, float* out2, cudaStream_t st,
                         const float* src2 = nullptr, float s1 = 1.f, float s2 = 1.f) {
+  LmArgs g{};
+  g.src = src;
+  g.src2 = src2;
+  g.s1 = s1;
+  g.s2 = s2;
+  g.out = out;
+  g.out2 = out2;
+  g.n = 2 * pe->K + 1;
+  g.K = pe->K;
+  g.M = pe->M;
+  g.L = pe->L;
+  g.C = pe->mem * pe->M;
+  g.Cp = pe->Cp;
+  g.p_div = pe->mem * pe->K;
+  g.p_temp = 2 * pe->mem * pe->K;
+  g.p_lnps = (3 + pe->nT) * pe->mem * pe->K;
+  g.ML = pe->ML;
+  const dim3 tiles(ceil_div(pe->L, 32), g.Cp / 32);
+  g.lm = pe->d_lm_in;
+  g.nk = m->nin;
+  pe_lm_gather_kernel<<<dim3(tiles.x, tiles.y, m->nin), 256, 0, st>>>(g);
+  DINO_TRY(check_launch("pe_lm_gather"));
   ApplyArgs a{};
-  a.src = src;
-  a.src2 = src2;
-  a.s1 = s1;
-  a.s2 = s2;
   a.A = m->d;
-  a.out = out;
-  a.out2 = out2;
+  a.ylm = pe->d_lm_in;
+  a.olm = pe->d_lm_out;
   a.R = m->R;
-  a.n = 2 * pe->K + 1;
   a.nin = m->nin;
   a.RP = m->RP;
-  a.K = pe->K;
-  a.M = pe->M;
-  a.L = pe->L;
-  a.C = pe->mem * pe->M;
-  a.p_div = pe->mem * pe->K;
-  a.p_temp = 2 * pe->mem * pe->K;
-  a.p_lnps = (3 + pe->nT) * pe->mem * pe->K;
-  a.ML = pe->ML;
+  a.Cp = pe->Cp;
   const int tr = apply_tr(m->R);
   const int rpt = 16 * tr;
-  dim3 grid(ceil_div(a.C, kApplyCols), pe->L, ceil_div(m->R, rpt));
+  dim3 grid(pe->Cp / kApplyCols, pe->L, ceil_div(m->R, rpt));
   const size_t smem = apply_smem(a.nin, tr);
   switch (tr) {
     case 1: apply_launch<1>(grid, smem, st, a); break;
@@ -1311,7 +1382,11 @@ static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
     case 12: apply_launch<12>(grid, smem, st, a); break;
     default: apply_launch<13>(grid, smem, st, a); break;
   }
-  return check_launch("pe_apply");
+  DINO_TRY(check_launch("pe_apply"));
+  g.lm = pe->d_lm_out;
+  g.nk = m->R;
+  pe_lm_scatter_kernel<<<dim3(tiles.x, tiles.y, m->R), 256, 0, st>>>(g);
+  return check_launch("pe_lm_scatter");
 }
 
 struct Term {
@@ -1908,6 +1983,8 @@ static void pe_free(dino_pe* pe) {
   for (auto* g : pe->d_g) cudaFree(g);
   cudaFree(pe->d_Y);
   cudaFree(pe->d_ystar);
+  cudaFree(pe->d_lm_in);
+  cudaFree(pe->d_lm_out);
   cudaFree(pe->d_xbar_n);
   cudaFree(pe->d_xbar_m);
   for (auto* b : pe->d_adj) cudaFree(b);
@@ -1947,6 +2024,7 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
     lev[lo.sigma + k] = (float)pe->sigma[k];
     double cut = (pe->sigma[k] - pe->hs_sigma_b) / (1.0 - pe->hs_sigma_b);
     lev[lo.kv + k] = (float)(pe->hs_kf * (cut > 0 ? cut : 0.0));
+    if (pe->hs_p0 > 0) lev[lo.logsp0 + k] = (float)std::log(pe->sigma[k] / pe->hs_p0);
     if (k + 1 < K) {
       // center_to_center arrives already as the reference's 1/x operand.
       lev[lo.c2ci + k] = (float)pe->c2c[k];
@@ -2024,6 +2102,14 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
   for (auto*& g : pe->d_g) DINO_CHECK_CUDA(cudaMalloc(&g, sizeof(float) * pe->n_state * ML));
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_Y, sizeof(float) * pe->n_state * ML));
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_ystar, sizeof(float) * pe->n_state * ML));
+  pe->Cp = ceil_div(pe->mem * pe->M, kApplyCols) * kApplyCols;
+  {
+    const size_t lm = (size_t)pe->L * 2 * (2 * K + 1) * pe->Cp;
+    DINO_CHECK_CUDA(cudaMalloc(&pe->d_lm_in, sizeof(float) * lm));
+    DINO_CHECK_CUDA(cudaMalloc(&pe->d_lm_out, sizeof(float) * lm));
+    DINO_CHECK_CUDA(cudaMemset(pe->d_lm_in, 0, sizeof(float) * lm));
+    DINO_CHECK_CUDA(cudaMemset(pe->d_lm_out, 0, sizeof(float) * lm));
+  }
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_flag, sizeof(int)));
   DINO_CHECK_CUDA(cudaDeviceSynchronize());
   return DINO_OK;
