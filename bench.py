@@ -484,6 +484,66 @@ def pe_extras(torch):
                  'finite': bool(torch.isfinite(buf).all())}
     del eng, buf, state, eq
     torch.cuda.empty_cache()
+  out.update(small_and_gradient_cases(torch))
+  return out
+
+
+def small_and_gradient_cases(torch):
+  """T21 / 12 levels, 72 filtered steps (one day at dt = 20 min) from a
+  near-rest state; and the gradient of a tracking loss through 24 steps of
+  T42 / 20 levels (forward with per-step checkpoints + reverse sweep)."""
+  from dinosaur_b200 import coordinate_systems, primitive_equations as pe
+  from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
+  from dinosaur_b200 import time_integration as ti, units
+  out = {}
+  for name, grid_name, layers, steps, grad in [('T21_L12_72_steps', 'T21', 12, 72, False),
+                                                ('T42_L20_grad_24_steps', 'T42', 20, 24, True)]:
+    g = getattr(sh.Grid, grid_name)()
+    coords = coordinate_systems.CoordinateSystem(
+        g, sigma_coordinates.SigmaCoordinates.equidistant(layers))
+    tref = np.linspace(220.0, 288.0, layers)
+    eq = pe.PrimitiveEquationsSigma(tref, np.zeros(g.modal_shape, np.float32), coords,
+                                    units.SimUnits())
+    dt = units.nondim_time(20 * 60.0)
+    step = ti.repeated(ti.step_with_filters(ti.imex_rk_sil3(eq, dt),
+                                            [ti.exponential_step_filter(g, dt)]), steps)
+    rng = np.random.default_rng(1)
+    _, l = g.modal_mesh
+    scale = g.mask / (l + 1.0) ** 2
+    shape = (layers,) + g.modal_shape
+    t = lambda s: torch.as_tensor((1e-4 * rng.standard_normal(s) * scale).astype(np.float32),
+                                  device='cuda')
+    leaves = [t(shape), t(shape), t(shape), t((1,) + g.modal_shape)]
+    target = [t(shape) for _ in range(2)]
+
+    def run():
+      x = pe.State(*[v.clone().requires_grad_(grad) for v in leaves])
+      y = step(x)
+      if grad:
+        loss = (((y.temperature_variation - target[0]) ** 2).mean() +
+                ((y.vorticity - target[1]) ** 2).mean())
+        loss.backward()
+      return y
+
+    for _ in range(2):
+      run()
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    reps = 3
+    a0.record()
+    for _ in range(reps):
+      y = run()
+    a1.record()
+    torch.cuda.synchronize()
+    ms = a0.elapsed_time(a1) / reps
+    entry = {'ms_per_rollout': ms, 'steps': steps, 'precision': 'fp32',
+             'finite': bool(torch.isfinite(y.vorticity).all())}
+    if grad:
+      entry['what'] = 'forward (checkpointed) + reverse sweep'
+    else:
+      entry['steps_per_s'] = steps * 1e3 / ms
+    out[name] = entry
   return out
 
 
