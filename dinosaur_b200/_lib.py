@@ -54,6 +54,17 @@ class GridDesc(ctypes.Structure):
 _DP = ctypes.POINTER(ctypes.c_double)
 
 
+class SWEDesc(ctypes.Structure):
+  _fields_ = [
+      ('layers', ctypes.c_int32),
+      ('members', ctypes.c_int32),
+      ('reference_potential', ctypes.POINTER(ctypes.c_double)),
+      ('densities', ctypes.POINTER(ctypes.c_double)),
+      ('orography_modal', ctypes.POINTER(ctypes.c_float)),
+      ('angular_velocity', ctypes.c_double),
+  ]
+
+
 class PEDesc(ctypes.Structure):
   _fields_ = [
       ('layers', ctypes.c_int32),
@@ -120,6 +131,14 @@ SIGNATURES = {
     'dino_pe_step': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32, _vp]),
     'dino_pe_step_graph': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32,
                                           _vp]),
+    'dino_swe_create': (ctypes.c_int, [_vp, ctypes.POINTER(SWEDesc),
+                                       ctypes.POINTER(_vp)]),
+    'dino_swe_destroy': (ctypes.c_int, [_vp]),
+    'dino_swe_state_size': (ctypes.c_int64, [_vp]),
+    'dino_swe_explicit': (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    'dino_swe_implicit': (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    'dino_swe_implicit_inverse': (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double,
+                                                 _vp]),
     'dino_pe_explicit_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     'dino_pe_implicit_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     'dino_pe_implicit_inverse_vjp': (ctypes.c_int, [_vp, _vp, _vp,

@@ -147,29 +147,6 @@ struct PrepArgs {
   float inv_radius;
 };
 
-__device__ __forceinline__ float d_dlon_at(const float* x, int row, int l,
-                                           int L) {
-  if (row == 0) return 0.f;
-  int m = (row + 1) >> 1;
-  return (row & 1) ? m * x[(size_t)(row + 1) * L + l]
-                   : -m * x[(size_t)(row - 1) * L + l];
-}
-
-// cos_lat_d_dlat (tab = 0) or sec_lat_d_dlat_cos2 (tab = 2) at (row, l) of a
-// plane x scaled elementwise by s[l] (s = nullptr: no scaling).
-__device__ __forceinline__ float dlat_at(const float* x, const float* s,
-                                         int row, int l, int L, int lw,
-                                         const float* deriv, int tab) {
-  int m = (row + 1) >> 1;
-  const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
-  const float* tb = ta + (size_t)lw * L;
-  const float* xr = x + (size_t)row * L;
-  float v = 0.f;
-  if (l + 1 < L) v += ta[l + 1] * (s ? s[l + 1] * xr[l + 1] : xr[l + 1]);
-  if (l >= 1) v += tb[l - 1] * (s ? s[l - 1] * xr[l - 1] : xr[l - 1]);
-  return v;
-}
-
 __global__ void pe_prep_kernel(PrepArgs a) {
   const size_t ML = (size_t)a.M * a.L;
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -516,22 +493,6 @@ __global__ void pe_post_kernel(PostArgs a) {
 // transform's adjoint, the VJP of the nodal column kernel (recomputing its
 // inputs), the inverse transform's adjoint and the transposed pre-pass.
 // ---------------------------------------------------------------------------
-
-// Transposed cos_lat_d_dlat (tab 0) / sec_lat_d_dlat_cos2 (tab 2) at (row, l)
-// of a plane y whose entries at l >= lclip count as zero:
-//   (D^T y)[l] = ta[l] y[l-1] + tb[l] y[l+1].
-__device__ __forceinline__ float dlat_t_at(const float* y, int row, int l, int L,
-                                           int lclip, int lw, const float* deriv,
-                                           int tab) {
-  const int m = (row + 1) >> 1;
-  const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
-  const float* tb = ta + (size_t)lw * L;
-  const float* yr = y + (size_t)row * L;
-  float v = 0.f;
-  if (l >= 1 && l - 1 < lclip) v += ta[l] * yr[l - 1];
-  if (l + 1 < lclip) v += tb[l] * yr[l + 1];
-  return v;
-}
 
 // Transposed post-pass: tendency cotangents (packed state layout) ->
 // cotangents of the forward-transform outputs.  d/dlon is antisymmetric

@@ -214,6 +214,37 @@ DINO_API int dino_pe_step_graph(dino_pe* pe, float* d_state, double dt,
                        const double* host_filter, int32_t n_steps,
                        void* stream);
 
+/* ---- Shallow-water equations (shallow_water.py:121-230) ------------------
+ * Packed state, kind-major: [vorticity: members*layers][divergence]
+ * [potential] planes of [M][L] in the plan's real modal layout. */
+typedef struct dino_swe dino_swe;
+
+typedef struct dino_swe_desc {
+  int32_t layers;                    /* K */
+  int32_t members;                   /* ensemble members, >= 1 */
+  const double* reference_potential; /* [K] mean geopotential per layer */
+  const double* densities;           /* [K] from the top, or NULL (all 1) */
+  const float* orography_modal;      /* [M][L] or NULL */
+  double angular_velocity;           /* nondimensional Omega */
+} dino_swe_desc;
+
+/* ShallowWaterEquations(coords, physics_specs, orography,
+ * reference_potential, densities) (shallow_water.py:121-140). */
+DINO_API int dino_swe_create(dino_plan* plan, const dino_swe_desc* desc,
+                             dino_swe** out);
+DINO_API int dino_swe_destroy(dino_swe* swe);
+DINO_API int64_t dino_swe_state_size(const dino_swe* swe);
+/* explicit_terms (shallow_water.py:158-205); out must not alias state. */
+DINO_API int dino_swe_explicit(dino_swe* swe, const float* d_state,
+                               float* d_out, void* stream);
+/* implicit_terms (:207-213). */
+DINO_API int dino_swe_implicit(dino_swe* swe, const float* d_state,
+                               float* d_out, void* stream);
+/* implicit_inverse(state, eta), closed form per l (:215-230); in place
+ * allowed. */
+DINO_API int dino_swe_implicit_inverse(dino_swe* swe, const float* d_state,
+                                       float* d_out, double eta, void* stream);
+
 /* ---- Reverse mode (vector-Jacobian products) ----------------------------
  * The reference differentiates its step with jax.vjp / jax.grad through the
  * JAX einsums of explicit_terms, implicit_terms and implicit_inverse

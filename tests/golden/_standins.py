@@ -146,7 +146,7 @@ def _strip(kw):
 
 def _einsum(*args, **kw):
   args = [list(a) if isinstance(a, range) else a for a in args]
-  return np.einsum(*args, **_strip(kw))
+  return _at(np.einsum(*args, **_strip(kw)))
 
 
 class _JnpModule(types.ModuleType):
@@ -227,10 +227,18 @@ def _decorator_or_identity(fn=None, *a, **k):
   return fn
 
 
-def _vmap(fn, *a, **k):
-  def _unsupported(*args, **kwargs):
-    raise NotImplementedError('vmap is not provided by the stand-in')
-  return _unsupported
+def _vmap(fn, in_axes=0, out_axes=0, *a, **k):
+  """jax.vmap over axis 0 of every positional argument (the only form the
+  reference's state constructors use): maps a Python loop and stacks each
+  output leaf."""
+  def mapped(*args):
+    if in_axes != 0 or out_axes != 0:
+      raise NotImplementedError('the stand-in vmap maps axis 0 only')
+    n = len(np.asarray(tree_flatten(args[0])[0][0]))
+    outs = [fn(*[tree_map(lambda x, i=i: np.asarray(x)[i], arg) for arg in args])
+            for i in range(n)]
+    return tree_map(lambda *xs: np.stack([np.asarray(x) for x in xs]), *outs)
+  return mapped
 
 
 class _Dummy:

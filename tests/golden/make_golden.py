@@ -207,6 +207,47 @@ def main(reference_root='/root/reference'):
   _save('hs_T21_L6.npz', **pack('in', hs_state), **pack('forcing', hs_expl),
         **pack('step1', hs1))
 
+  # -- shallow water (two layers) --------------------------------------
+  from dinosaur import layer_coordinates
+  from dinosaur import shallow_water
+  from dinosaur import shallow_water_states
+  swe_coords = coordinate_systems.CoordinateSystem(
+      spherical_harmonic.Grid.T21(), layer_coordinates.LayerCoordinates(2))
+  swe_grid = swe_coords.horizontal
+  _, l = swe_grid.modal_mesh
+  smooth = lambda n, a: a * rng.standard_normal((n,) + swe_grid.modal_shape) * (
+      swe_grid.mask / (l + 1.0) ** 2)
+  densities = np.array([0.9, 1.0])
+  ref_potential = np.array([0.1, 0.12])
+  swe_orog = smooth(1, 1e-3)[0]
+  lat = np.arccos(swe_grid.cos_lat)
+  u_layers = np.stack([np.cos(lat) / 5, np.cos(lat) ** 2 / 6])
+  steady = shallow_water_states.multi_layer(u_layers, densities, swe_coords)
+  swe_state = shallow_water.State(
+      vorticity=np.asarray(steady.vorticity) + smooth(2, 1e-2),
+      divergence=np.asarray(steady.divergence) + smooth(2, 1e-2),
+      potential=np.asarray(steady.potential) + smooth(2, 1e-2))
+  swe_eq = shallow_water.ShallowWaterEquations(
+      swe_coords, physics_specs, swe_orog, ref_potential, densities=densities)
+  swe_dt = 1e-3 * 20
+  swe_step = time_integration.step_with_filters(
+      time_integration.imex_rk_sil3(swe_eq, swe_dt),
+      [time_integration.exponential_step_filter(swe_grid, swe_dt)])
+  w1 = swe_step(swe_state)
+  w2 = swe_step(w1)
+
+  def swe_pack(prefix, st):
+    return {f'{prefix}_{k}': np.asarray(getattr(st, k)) for k in
+            ('vorticity', 'divergence', 'potential')}
+
+  _save('swe_T21_L2.npz', densities=densities, ref_potential=ref_potential,
+        orography=swe_orog, u_layers=u_layers, dt=swe_dt,
+        **swe_pack('steady', steady), **swe_pack('in', swe_state),
+        **swe_pack('explicit', swe_eq.explicit_terms(swe_state)),
+        **swe_pack('implicit', swe_eq.implicit_terms(swe_state)),
+        **swe_pack('inverse', swe_eq.implicit_inverse(swe_state, 0.03)),
+        **swe_pack('step1', w1), **swe_pack('step2', w2))
+
   # -- nondimensional constants ----------------------------------------
   _save('units.npz', radius=physics_specs.radius,
         angular_velocity=physics_specs.angular_velocity,

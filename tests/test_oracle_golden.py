@@ -197,3 +197,35 @@ def test_held_suarez_matches_reference():
       [dycore.exponential_step_filter(grid, dt, tau=0.0087504, order=1.5,
                                       cutoff=0.8)])
   assert_state_close(step(s), unpack(g, 'step1'), atol=1e-10)
+
+
+SWE_KEYS = ('vorticity', 'divergence', 'potential')
+
+
+def test_shallow_water_matches_reference():
+  from oracle import swe
+  g = load('swe_T21_L2.npz')
+  grid = sht.Grid.T21()
+  steady = swe.multi_layer(g['u_layers'], g['densities'], grid)
+  for k in SWE_KEYS:
+    scale = max(np.abs(g[f'steady_{k}']).max(), 1e-300)
+    close(steady[k] / scale, g[f'steady_{k}'] / scale, atol=1e-11)
+  eq = swe.ShallowWaterEquations(grid, dycore.SimUnits(), g['orography'],
+                                 g['ref_potential'], g['densities'])
+  s = {k: g[f'in_{k}'] for k in SWE_KEYS}
+
+  def check(got, prefix, atol):
+    for k in SWE_KEYS:
+      ref = g[f'{prefix}_{k}']
+      scale = max(np.abs(ref).max(), 1e-300)
+      close(got[k] / scale, ref / scale, atol=atol)
+
+  check(eq.explicit_terms(s), 'explicit', 1e-10)
+  check(eq.implicit_terms(s), 'implicit', 1e-12)
+  check(eq.implicit_inverse(s, 0.03), 'inverse', 1e-12)
+  dt = float(g['dt'])
+  step = swe.filtered_step(swe.imex_rk_sil3(eq, dt),
+                           sht.exponential_filter_scaling(grid, dt / 0.010938, 18, 0))
+  s1 = step(s)
+  check(s1, 'step1', 1e-10)
+  check(step(s1), 'step2', 1e-10)

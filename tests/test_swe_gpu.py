@@ -1,0 +1,127 @@
+"""GPU parity of the shallow-water equations (dino_swe_* through the C ABI).
+
+Against the FP64 oracle (pinned to the reference's outputs in
+tests/golden/swe_T21_L2.npz): explicit / implicit terms and the implicit
+inverse <= 2e-5 max-abs relative to each field's max; two filtered SIL3
+steps <= 5e-5; the steady multi-layer state <= 2e-5.  The reference's own
+steady geostrophic-flow test (shallow_water_test.py:100-203) with its
+tolerances: mean potential < 1e-8 and relative L2 drift < 1e-5 over 10 x 1000
+steps.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import dycore as od
+from oracle import sht as osht
+from oracle import swe as oswe
+
+pytestmark = pytest.mark.gpu
+
+from dinosaur_b200 import coordinate_systems  # noqa: E402
+from dinosaur_b200 import layer_coordinates  # noqa: E402
+from dinosaur_b200 import shallow_water as sw  # noqa: E402
+from dinosaur_b200 import shallow_water_states as sws  # noqa: E402
+from dinosaur_b200 import spherical_harmonic as sh  # noqa: E402
+from dinosaur_b200 import time_integration as ti  # noqa: E402
+from dinosaur_b200 import units  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
+KEYS = oswe.SWE_KEYS
+
+
+def rel(a, b):
+  a = a.detach().double().cpu().numpy()
+  return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+def case():
+  g = np.load(os.path.join(GOLDEN, 'swe_T21_L2.npz'))
+  og = osht.Grid.T21()
+  grid = sh.Grid.T21()
+  coords = coordinate_systems.CoordinateSystem(
+      grid, layer_coordinates.LayerCoordinates(2))
+  eq = sw.ShallowWaterEquations(coords, units.SimUnits(), g['orography'],
+                                g['ref_potential'], densities=g['densities'])
+  oeq = oswe.ShallowWaterEquations(og, od.SimUnits(), g['orography'],
+                                   g['ref_potential'], g['densities'])
+  st = {k: np.asarray(g[f'in_{k}'], np.float32).astype(np.float64) for k in KEYS}
+  return g, og, grid, eq, oeq, st
+
+
+def to_state(d):
+  return sw.State(*[torch.as_tensor(d[k], device='cuda', dtype=torch.float32)
+                    for k in KEYS])
+
+
+def assert_close(got, ref, tol):
+  for k in KEYS:
+    e = rel(getattr(got, k), ref[k])
+    assert e < tol, (k, e)
+
+
+def test_terms_and_inverse_match_oracle():
+  _, _, _, eq, oeq, st = case()
+  s = to_state(st)
+  assert_close(eq.explicit_terms(s), oeq.explicit_terms(st), 2e-5)
+  assert_close(eq.implicit_terms(s), oeq.implicit_terms(st), 2e-6)
+  for eta in (0.03, 0.2):
+    assert_close(eq.implicit_inverse(s, eta), oeq.implicit_inverse(st, eta), 2e-6)
+
+
+def test_filtered_sil3_steps_match_oracle():
+  g, og, grid, eq, oeq, st = case()
+  dt = float(g['dt'])
+  step = ti.step_with_filters(ti.imex_rk_sil3(eq, dt),
+                              [ti.exponential_step_filter(grid, dt)])
+  ostep = oswe.filtered_step(oswe.imex_rk_sil3(oeq, dt),
+                             osht.exponential_filter_scaling(og, dt / 0.010938))
+  got = step(step(to_state(st)))
+  ref = ostep(ostep(st))
+  assert_close(got, ref, 5e-5)
+
+
+def test_multi_layer_steady_state_matches_oracle():
+  g, og, grid, _, _, _ = case()
+  coords = coordinate_systems.CoordinateSystem(
+      grid, layer_coordinates.LayerCoordinates(2))
+  got = sws.multi_layer(g['u_layers'], g['densities'], coords)
+  ref = oswe.multi_layer(g['u_layers'], g['densities'], og)
+  assert_close(got, ref, 2e-5)
+
+
+@pytest.mark.parametrize('params', [
+    dict(wavenumbers=64, layers=1, velocity=lambda lat: np.cos(3 * lat) / 5,
+         dt=1e-3),
+    dict(wavenumbers=64, layers=4, velocity=lambda lat: np.cos(lat) / 5,
+         dt=1e-3),
+])
+def test_reference_steady_geostrophic_flow(params):
+  # shallow_water_test.py:100-203 (density ratio 0.9, mean potential 1/10,
+  # 10 x 1000 filtered SIL3 steps).
+  grid = sh.Grid.with_wavenumbers(params['wavenumbers'])
+  layers = params['layers']
+  coords = coordinate_systems.CoordinateSystem(
+      grid, layer_coordinates.LayerCoordinates(layers))
+  density = np.array([0.9 ** n for n in range(layers)][::-1])
+  mean_potential = np.ones(layers) / 10
+  dt = params['dt']
+  eq = sw.ShallowWaterEquations(coords, units.SimUnits(), None, mean_potential,
+                                densities=density)
+  step = ti.repeated(ti.step_with_filters(
+      ti.imex_rk_sil3(eq, dt), [ti.exponential_step_filter(grid, dt)]), 1000)
+  lat = np.arccos(grid.cos_lat)
+  velocity = np.stack([params['velocity'](lat)] * layers)
+  state = sws.multi_layer(velocity, density, coords)
+  init = grid.to_nodal(state.potential).double().cpu().numpy()
+  init_l2 = np.sqrt(np.square(init).sum())
+  w = osht.gauss_legendre_nodes(grid.latitude_nodes)[1]
+  for _ in range(10):
+    state = step(state)
+    pot = grid.to_nodal(state.potential).double().cpu().numpy()
+    mean = np.mean(w * pot / np.sum(w), axis=(-1, -2))
+    assert np.all(np.abs(mean) < 1e-8), mean
+    assert np.sqrt(np.square(pot - init).sum()) / init_l2 < 1e-5
