@@ -821,6 +821,38 @@ static int sht_forward_adjoint(dino_plan* p, const float* modal_ct,
 }
 
 // ---------------------------------------------------------------------------
+// FastSphericalHarmonics modal layout (spherical_harmonic.py:411-621)
+// ---------------------------------------------------------------------------
+
+// Rows of the Fast layout are m = 0, 0 (imaginary, always zero), 1, -1, 2,
+// -2, ... (:486-497): the Real layout [M = 2 lw - 1][L] with a zero row
+// inserted at index 1.  to_fast: [M][L] -> [M + 1][L]; else the inverse
+// (which drops row 1).
+__global__ void modal_relayout_kernel(const float* __restrict__ in,
+                                      float* __restrict__ out, int M, int L,
+                                      int to_fast) {
+  const int rows_in = to_fast ? M : M + 1, rows_out = to_fast ? M + 1 : M;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)rows_out * L) return;
+  const int r = idx / L, l = idx % L;
+  const float* src = in + (size_t)blockIdx.y * rows_in * L;
+  float v;
+  if (to_fast)
+    v = (r == 0) ? src[l] : (r == 1 ? 0.f : src[(size_t)(r - 1) * L + l]);
+  else
+    v = src[(size_t)(r == 0 ? 0 : r + 1) * L + l];
+  out[(size_t)blockIdx.y * rows_out * L + idx] = v;
+}
+
+int modal_relayout(dino_plan* p, bool to_fast, const float* in, float* out, int nf,
+                   cudaStream_t st) {
+  const int rows_out = to_fast ? p->M + 1 : p->M;
+  dim3 grid(ceil_div(rows_out * p->L, 256), nf);
+  modal_relayout_kernel<<<grid, 256, 0, st>>>(in, out, p->M, p->L, to_fast ? 1 : 0);
+  return check_launch("modal_relayout");
+}
+
+// ---------------------------------------------------------------------------
 // Spectral operators (spherical_harmonic.py:1033-1102)
 // ---------------------------------------------------------------------------
 
@@ -963,6 +995,15 @@ int dino_modal_op(dino_plan* p, int32_t op, const float* in, float* out,
   DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_modal_op: null argument");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
   return modal_op(p, op, in, out, nf, arg, (cudaStream_t)stream);
+}
+
+int dino_modal_relayout(dino_plan* p, int32_t to_fast, const float* in, float* out,
+                        int32_t nfields, void* stream) {
+  DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_modal_relayout: null argument");
+  DINO_REQUIRE(in != out, DINO_ERR_ARG, "dino_modal_relayout: in and out must differ");
+  DINO_REQUIRE(nfields >= 0 && nfields <= 65535, DINO_ERR_SHAPE, "nfields out of range");
+  if (nfields == 0) return DINO_OK;
+  return modal_relayout(p, to_fast != 0, in, out, nfields, (cudaStream_t)stream);
 }
 
 }  // extern "C"

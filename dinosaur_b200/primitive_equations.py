@@ -175,7 +175,9 @@ class _Engine:
     self.members = members
     self.tracer_names = tracer_names
     self.K = vert.layers
-    self.M, self.L = grid.modal_shape
+    # The engine works in the Real modal layout; a Fast-layout grid's arrays
+    # are converted in pack() / unpack().
+    self.M, self.L = 2 * grid.longitude_wavenumbers - 1, grid.total_wavenumbers
     hum = -1
     if eq.humidity_key is not None:
       if eq.humidity_key not in tracer_names:
@@ -198,6 +200,10 @@ class _Engine:
         alpha=np.ascontiguousarray(get_sigma_ratios(vert), np.float64),
     )
     orog = eq.orography
+    if sh.is_fast_layout(grid):
+      orog = sh.to_real_layout(grid, torch.as_tensor(np.asarray(orog, np.float32)
+                                                     if not isinstance(orog, torch.Tensor)
+                                                     else orog))
     if isinstance(orog, torch.Tensor):
       orog = orog.detach().cpu().numpy()
     self._orog = np.ascontiguousarray(np.asarray(orog, np.float32).reshape(
@@ -250,14 +256,13 @@ class _Engine:
   # -- packing -------------------------------------------------------------
   def pack(self, state: State) -> torch.Tensor:
     mK = self.members * self.K
-    parts = [sh.as_device_tensor(state.vorticity).reshape(mK, self.M, self.L),
-             sh.as_device_tensor(state.divergence).reshape(mK, self.M, self.L),
-             sh.as_device_tensor(state.temperature_variation).reshape(
-                 mK, self.M, self.L)]
+    real = lambda x: sh.to_real_layout(self.grid, x)
+    parts = [real(state.vorticity).reshape(mK, self.M, self.L),
+             real(state.divergence).reshape(mK, self.M, self.L),
+             real(state.temperature_variation).reshape(mK, self.M, self.L)]
     for name in self.tracer_names:
-      parts.append(sh.as_device_tensor(state.tracers[name]).reshape(
-          mK, self.M, self.L))
-    parts.append(sh.as_device_tensor(state.log_surface_pressure).reshape(
+      parts.append(real(state.tracers[name]).reshape(mK, self.M, self.L))
+    parts.append(real(state.log_surface_pressure).reshape(
         self.members, self.M, self.L))
     buf = torch.cat(parts).reshape(-1).contiguous()
     assert buf.numel() == self.size
@@ -266,16 +271,22 @@ class _Engine:
   def unpack(self, buf: torch.Tensor, like: State, sim_time=None) -> State:
     mK = self.members * self.K
     planes = buf.view(-1, self.M, self.L)
-    shape3 = tuple(like.vorticity.shape)
-    lshape = tuple(like.log_surface_pressure.shape)
+
+    def leaf(p0, p1, like_leaf):
+      shape = tuple(like_leaf.shape)
+      x = planes[p0:p1]
+      if sh.is_fast_layout(self.grid):
+        return sh.from_real_layout(self.grid, x).view(shape)
+      return x.view(shape)
+
+    nT = len(self.tracer_names)
     out = State(
-        vorticity=planes[0:mK].view(shape3),
-        divergence=planes[mK:2 * mK].view(shape3),
-        temperature_variation=planes[2 * mK:3 * mK].view(shape3),
-        log_surface_pressure=planes[(3 + len(self.tracer_names)) * mK:].view(
-            lshape),
-        tracers={name: planes[(3 + t) * mK:(4 + t) * mK].view(
-            tuple(like.tracers[name].shape))
+        vorticity=leaf(0, mK, like.vorticity),
+        divergence=leaf(mK, 2 * mK, like.divergence),
+        temperature_variation=leaf(2 * mK, 3 * mK, like.temperature_variation),
+        log_surface_pressure=leaf((3 + nT) * mK, (3 + nT) * mK + self.members,
+                                  like.log_surface_pressure),
+        tracers={name: leaf((3 + t) * mK, (4 + t) * mK, like.tracers[name])
                  for t, name in enumerate(self.tracer_names)},
         sim_time=sim_time)
     return out

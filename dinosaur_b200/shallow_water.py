@@ -86,14 +86,18 @@ class _Engine:
 
   def __init__(self, eq: 'ShallowWaterEquations', members: int):
     grid = eq.coords.horizontal
+    self.grid = grid
     self.K = eq.coords.vertical.layers
-    self.M, self.L = grid.modal_shape
+    # Real modal layout inside; Fast-layout arrays are converted at the edges.
+    self.M, self.L = 2 * grid.longitude_wavenumbers - 1, grid.total_wavenumbers
     self.members = members
     self._ref = np.ascontiguousarray(np.broadcast_to(
         np.asarray(eq.reference_potential, np.float64), (self.K,)))
     self._dens = np.ascontiguousarray(np.broadcast_to(
         np.asarray(eq.densities, np.float64), (self.K,)))
     orog = eq.orography
+    if orog is not None and sh.is_fast_layout(grid):
+      orog = sh.to_real_layout(grid, orog)
     if isinstance(orog, torch.Tensor):
       orog = orog.detach().cpu().numpy()
     self._orog = None if orog is None else np.ascontiguousarray(
@@ -122,7 +126,7 @@ class _Engine:
 
   def pack(self, state: State) -> torch.Tensor:
     n = self.members * self.K
-    parts = [sh.as_device_tensor(getattr(state, k)).reshape(n, self.M, self.L)
+    parts = [sh.to_real_layout(self.grid, getattr(state, k)).reshape(n, self.M, self.L)
              for k in ('vorticity', 'divergence', 'potential')]
     return torch.cat(parts).reshape(-1).contiguous()
 
@@ -130,8 +134,8 @@ class _Engine:
     n = self.members * self.K
     planes = buf.view(-1, self.M, self.L)
     shape = tuple(like.vorticity.shape)
-    return State(planes[0:n].view(shape), planes[n:2 * n].view(shape),
-                 planes[2 * n:].view(shape))
+    conv = lambda x: sh.from_real_layout(self.grid, x).view(shape)
+    return State(conv(planes[0:n]), conv(planes[n:2 * n]), conv(planes[2 * n:]))
 
   def call(self, name, buf, *extra):
     out = torch.empty(self.size, device='cuda', dtype=torch.float32)
@@ -171,7 +175,7 @@ class ShallowWaterEquations(time_integration.ImplicitExplicitODE):
 
   def _engine(self, state: State) -> _Engine:
     K = self.coords.vertical.layers
-    M, L = self.coords.horizontal.modal_shape
+    M, L = self.coords.horizontal.modal_shape  # in the grid's own layout
     shape = tuple(state.vorticity.shape)
     if shape[-3:] != (K, M, L) or len(shape) not in (3, 4):
       raise ValueError(f'expected state arrays of shape [members,] {(K, M, L)}; '

@@ -219,6 +219,22 @@ class Plan:
     n = int(np.prod(lead)) if lead else 1
     return self._call('dino_sht_forward_adjoint', g, lead + (self.I, self.J), n)
 
+  def relayout(self, x: torch.Tensor, to_fast: bool) -> torch.Tensor:
+    """Real <-> FastSphericalHarmonics modal rows (dino_modal_relayout)."""
+    rows_in = self.M + (0 if to_fast else 1)
+    rows_out = self.M + (1 if to_fast else 0)
+    if tuple(x.shape[-2:]) != (rows_in, self.L):
+      raise ValueError(f'expected [..., {rows_in}, {self.L}] modal array; got '
+                       f'{tuple(x.shape)}')
+    x = x.contiguous()
+    nf = x.numel() // (rows_in * self.L)
+    out = torch.empty(x.shape[:-2] + (rows_out, self.L), device=x.device,
+                      dtype=torch.float32)
+    _lib.check(_lib.lib().dino_modal_relayout(self.handle, int(to_fast), ptr(x),
+                                              ptr(out), nf, stream_handle()),
+               'modal_relayout')
+    return out
+
   def modal_op(self, op: str, x: torch.Tensor, arg: int = 0,
                transpose: bool = False) -> torch.Tensor:
     self._check(x, (self.M, self.L), op)
@@ -367,6 +383,106 @@ class CudaSphericalHarmonics(SphericalHarmonics):
 
 # The reference's default implementation name maps to the CUDA one.
 RealSphericalHarmonics = CudaSphericalHarmonics
+
+
+class _Relayout(torch.autograd.Function):
+  """Real <-> Fast modal layout (a row insertion / deletion: its transpose is
+  the opposite conversion)."""
+
+  @staticmethod
+  def forward(ctx, x, plan, to_fast):
+    ctx.plan, ctx.to_fast = plan, to_fast
+    return plan.relayout(x, to_fast)
+
+  @staticmethod
+  def backward(ctx, g):
+    return ctx.plan.relayout(g.contiguous(), not ctx.to_fast), None, None
+
+
+def relayout(plan: Plan, x: torch.Tensor, to_fast: bool) -> torch.Tensor:
+  if torch.is_grad_enabled() and x.requires_grad:
+    return _Relayout.apply(x, plan, to_fast)
+  return plan.relayout(x, to_fast)
+
+
+@dataclasses.dataclass(frozen=True)
+class FastSphericalHarmonics(CudaSphericalHarmonics):
+  """The m-stacked modal layout of FastSphericalHarmonics
+  (spherical_harmonic.py:411-621) on one GPU: rows m = 0, 0 (imaginary, always
+  zero), 1, -1, 2, -2, ... of shape (2 lw, L).  Transforms and operators run
+  in the Real layout; modal arrays are converted at this boundary by
+  ``dino_modal_relayout``.  The reference's sharding and einsum-ordering
+  options are accepted and have no effect on one GPU.
+  """
+
+  spmd_mesh: Any = None
+  base_shape_multiple: int | None = None
+  reverse_einsum_arg_order: bool | None = None
+  stacked_fourier_transforms: bool | None = None
+  transform_precision: str = 'tensorfloat32'
+
+  @functools.cached_property
+  def modal_axes(self):
+    m_pos = np.arange(1, self.longitude_wavenumbers)
+    m_pos_neg = np.stack([m_pos, -m_pos], axis=1).ravel()
+    return (np.concatenate([[0, 0], m_pos_neg]),
+            np.arange(self.total_wavenumbers))
+
+  @property
+  def modal_shape(self):
+    return (2 * self.longitude_wavenumbers, self.total_wavenumbers)
+
+  @functools.cached_property
+  def mask(self):
+    m, l = np.meshgrid(*self.modal_axes, indexing='ij')
+    rows = np.arange(self.modal_shape[0])[:, None]
+    return (abs(m) <= l) & (rows != 1)
+
+  @functools.cached_property
+  def basis(self) -> _SphericalHarmonicBasis:
+    """f with the zero imaginary m = 0 column, p per m (not repeated)."""
+    f = _real_basis(self.longitude_wavenumbers, self.longitude_nodes)
+    f = np.insert(f, 1, 0.0, axis=1)
+    x = self.nodal_axes[1]
+    w = (2 * np.pi / self.longitude_nodes) * self.quadrature_weights_lat
+    p = _legendre_host(self.longitude_wavenumbers, self.total_wavenumbers, x)
+    return _SphericalHarmonicBasis(f=f, p=p, w=w)
+
+  def to_real(self, x):
+    return relayout(self.plan, as_device_tensor(x), False)
+
+  def from_real(self, x):
+    return relayout(self.plan, as_device_tensor(x), True)
+
+  def inverse_transform(self, x):
+    return super().inverse_transform(self.to_real(x))
+
+  def transform(self, x):
+    return self.from_real(super().transform(x))
+
+  def longitudinal_derivative(self, x):
+    return self.from_real(super().longitudinal_derivative(self.to_real(x)))
+
+
+RealSphericalHarmonicsWithZeroImag = FastSphericalHarmonics
+
+
+def is_fast_layout(grid) -> bool:
+  return isinstance(grid.spherical_harmonics, FastSphericalHarmonics)
+
+
+def to_real_layout(grid, x):
+  """Modal array of `grid`'s layout -> the Real layout (identity for Real)."""
+  if is_fast_layout(grid):
+    return grid.spherical_harmonics.to_real(x)
+  return as_device_tensor(x)
+
+
+def from_real_layout(grid, x):
+  """Real-layout modal array -> `grid`'s layout (identity for Real)."""
+  if is_fast_layout(grid):
+    return grid.spherical_harmonics.from_real(x)
+  return x
 
 SphericalHarmonicsImpl = Callable[..., SphericalHarmonics]
 
@@ -528,23 +644,19 @@ class Grid:
 
   @functools.cached_property
   def modal_axes(self):
-    m_pos = np.arange(1, self.longitude_wavenumbers)
-    m_pos_neg = np.stack([m_pos, -m_pos], axis=1).ravel()
-    return (np.concatenate([[0], m_pos_neg]),
-            np.arange(self.total_wavenumbers))
+    return self.spherical_harmonics.modal_axes
 
   @property
   def modal_shape(self):
-    return (2 * self.longitude_wavenumbers - 1, self.total_wavenumbers)
+    return self.spherical_harmonics.modal_shape
 
   @property
   def modal_padding(self):
-    return (0, 0)
+    return self.spherical_harmonics.modal_padding
 
   @functools.cached_property
   def mask(self):
-    m, l = self.modal_mesh
-    return abs(m) <= l
+    return self.spherical_harmonics.mask
 
   @functools.cached_property
   def modal_mesh(self):
@@ -578,8 +690,9 @@ class Grid:
   # -- operators -------------------------------------------------------------
   def _op(self, name, x, arg=0):
     from dinosaur_b200 import autograd  # pylint: disable=g-import-not-at-top
-    return autograd.modal_op(self.plan, name, as_device_tensor(x), arg,
-                             radius=1.0)
+    out = autograd.modal_op(self.plan, name, to_real_layout(self, x), arg,
+                            radius=1.0)
+    return from_real_layout(self, out)
 
   def laplacian(self, x):
     """x * -l(l+1)/r^2 (spherical_harmonic.py:1033-1036)."""

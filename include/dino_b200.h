@@ -214,6 +214,14 @@ DINO_API int dino_pe_step_graph(dino_pe* pe, float* d_state, double dt,
                        const double* host_filter, int32_t n_steps,
                        void* stream);
 
+/* Converts modal arrays between the Real layout ([M = 2 lw - 1][L], rows
+ * m = 0, 1, -1, ...) and the FastSphericalHarmonics layout ([2 lw][L], rows
+ * m = 0, 0 (imaginary, zero), 1, -1, ...; spherical_harmonic.py:411-621):
+ * to_fast = 1 inserts the zero row, 0 drops it.  in and out must differ. */
+DINO_API int dino_modal_relayout(dino_plan* plan, int32_t to_fast,
+                                 const float* d_in, float* d_out,
+                                 int32_t nfields, void* stream);
+
 /* ---- Shallow-water equations (shallow_water.py:121-230) ------------------
  * Packed state, kind-major: [vorticity: members*layers][divergence]
  * [potential] planes of [M][L] in the plan's real modal layout. */

@@ -382,3 +382,15 @@ def horizontal_diffusion_scaling(grid: Grid, scale, order=1) -> np.ndarray:
   """filtering.py:92-100."""
   eigenvalues = grid.laplacian_eigenvalues
   return np.exp(-scale * (-eigenvalues) ** order)
+
+
+def fast_to_real(x):
+  """FastSphericalHarmonics modal rows (m = 0, 0i, 1, -1, 2, -2, ...;
+  spherical_harmonic.py:486-497) -> the Real layout (drops the always-zero
+  imaginary m = 0 row)."""
+  return np.delete(np.asarray(x), 1, axis=-2)
+
+
+def real_to_fast(x):
+  """The Real layout -> FastSphericalHarmonics rows (inserts the zero row)."""
+  return np.insert(np.asarray(x), 1, 0.0, axis=-2)

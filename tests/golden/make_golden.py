@@ -248,6 +248,19 @@ def main(reference_root='/root/reference'):
         **swe_pack('inverse', swe_eq.implicit_inverse(swe_state, 0.03)),
         **swe_pack('step1', w1), **swe_pack('step2', w2))
 
+  # -- Fast (m-stacked, zero imaginary m = 0 row) layout ----------------
+  fast = spherical_harmonic.Grid.T21(
+      spherical_harmonics_impl=spherical_harmonic.FastSphericalHarmonics)
+  fx = rng.standard_normal((3,) + fast.modal_shape) * fast.mask
+  fz = rng.standard_normal((3,) + fast.nodal_shape)
+  _save('fast_T21.npz', modal_axes_m=fast.modal_axes[0],
+        modal_axes_l=fast.modal_axes[1], mask=fast.mask, modal_in=fx,
+        nodal_out=fast.to_nodal(fx), nodal_in=fz, modal_out=fast.to_modal(fz),
+        d_dlon=fast.d_dlon(fx), laplacian=fast.laplacian(fx),
+        cos_lat_d_dlat=fast.cos_lat_d_dlat(fx),
+        sec_lat_d_dlat_cos2=fast.sec_lat_d_dlat_cos2(fx),
+        clip=fast.clip_wavenumbers(fx))
+
   # -- nondimensional constants ----------------------------------------
   _save('units.npz', radius=physics_specs.radius,
         angular_velocity=physics_specs.angular_velocity,

@@ -229,3 +229,20 @@ def test_shallow_water_matches_reference():
   s1 = step(s)
   check(s1, 'step1', 1e-10)
   check(step(s1), 'step2', 1e-10)
+
+
+def test_fast_layout_is_the_real_layout_with_a_zero_row():
+  g = load('fast_T21.npz')
+  grid = sht.Grid.T21()
+  m = g['modal_axes_m']
+  np.testing.assert_array_equal(m[:2], [0, 0])
+  np.testing.assert_array_equal(np.delete(m, 1), grid.modal_axes[0])
+  np.testing.assert_array_equal(g['modal_axes_l'], grid.modal_axes[1])
+  assert not g['mask'][1].any()
+  np.testing.assert_array_equal(sht.fast_to_real(g['mask']), grid.mask)
+  x = sht.fast_to_real(g['modal_in'])
+  close(grid.to_nodal(x), g['nodal_out'])
+  close(sht.real_to_fast(grid.to_modal(g['nodal_in'])), g['modal_out'])
+  for name in ('d_dlon', 'laplacian', 'cos_lat_d_dlat', 'sec_lat_d_dlat_cos2'):
+    close(sht.real_to_fast(getattr(grid, name)(x)), g[name], atol=1e-12)
+  close(sht.real_to_fast(grid.clip_wavenumbers(x)), g['clip'], atol=0)
