@@ -937,35 +937,39 @@ extern "C" {
 
 int dino_sht_inverse(dino_plan* p, const float* modal, float* nodal, int32_t nf,
                      void* stream) {
-  DINO_REQUIRE(p && modal && nodal, DINO_ERR_ARG, "dino_sht_inverse: null argument");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "dino_sht_inverse: null plan");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
-  if (nf == 0) return DINO_OK;
+  if (nf == 0) return DINO_OK;  // buffers may be null for an empty batch
+  DINO_REQUIRE(modal && nodal, DINO_ERR_ARG, "dino_sht_inverse: null argument");
   return sht_inverse_segs(p, one_seg(modal, nf), nodal, nf, p->d_work,
                           p->max_fields, (cudaStream_t)stream);
 }
 
 int dino_sht_forward(dino_plan* p, const float* nodal, float* modal, int32_t nf,
                      void* stream) {
-  DINO_REQUIRE(p && modal && nodal, DINO_ERR_ARG, "dino_sht_forward: null argument");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "dino_sht_forward: null plan");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
   if (nf == 0) return DINO_OK;
+  DINO_REQUIRE(modal && nodal, DINO_ERR_ARG, "dino_sht_forward: null argument");
   return sht_forward_to(p, nodal, modal, nf, p->d_work, p->max_fields,
                         (cudaStream_t)stream);
 }
 
 int dino_sht_inverse_adjoint(dino_plan* p, const float* nodal_ct,
                              float* modal_ct, int32_t nf, void* stream) {
-  DINO_REQUIRE(p && nodal_ct && modal_ct, DINO_ERR_ARG, "null argument");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "null plan");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
   if (nf == 0) return DINO_OK;
+  DINO_REQUIRE(nodal_ct && modal_ct, DINO_ERR_ARG, "null argument");
   return sht_inverse_adjoint(p, nodal_ct, modal_ct, nf, (cudaStream_t)stream);
 }
 
 int dino_sht_forward_adjoint(dino_plan* p, const float* modal_ct,
                              float* nodal_ct, int32_t nf, void* stream) {
-  DINO_REQUIRE(p && nodal_ct && modal_ct, DINO_ERR_ARG, "null argument");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "null plan");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
   if (nf == 0) return DINO_OK;
+  DINO_REQUIRE(nodal_ct && modal_ct, DINO_ERR_ARG, "null argument");
   return sht_forward_adjoint(p, modal_ct, nodal_ct, nf, (cudaStream_t)stream);
 }
 
@@ -992,17 +996,20 @@ int dino_sht_phase(dino_plan* p, int32_t phase, const float* in, float* out,
 
 int dino_modal_op(dino_plan* p, int32_t op, const float* in, float* out,
                   int32_t nf, int32_t arg, void* stream) {
-  DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_modal_op: null argument");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "dino_modal_op: null plan");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  if (nf == 0) return DINO_OK;
+  DINO_REQUIRE(in && out, DINO_ERR_ARG, "dino_modal_op: null argument");
   return modal_op(p, op, in, out, nf, arg, (cudaStream_t)stream);
 }
 
 int dino_modal_relayout(dino_plan* p, int32_t to_fast, const float* in, float* out,
                         int32_t nfields, void* stream) {
-  DINO_REQUIRE(p && in && out, DINO_ERR_ARG, "dino_modal_relayout: null argument");
-  DINO_REQUIRE(in != out, DINO_ERR_ARG, "dino_modal_relayout: in and out must differ");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "dino_modal_relayout: null plan");
   DINO_REQUIRE(nfields >= 0 && nfields <= 65535, DINO_ERR_SHAPE, "nfields out of range");
   if (nfields == 0) return DINO_OK;
+  DINO_REQUIRE(in && out, DINO_ERR_ARG, "dino_modal_relayout: null argument");
+  DINO_REQUIRE(in != out, DINO_ERR_ARG, "dino_modal_relayout: in and out must differ");
   return modal_relayout(p, to_fast != 0, in, out, nfields, (cudaStream_t)stream);
 }
 

@@ -136,7 +136,8 @@ DINO_API int dino_sht_inverse_noalloc(dino_plan* plan, const float* d_modal,
                                       float* d_nodal, int32_t nfields,
                                       void* stream);
 
-/* modal [nfields][M][L] -> nodal [nfields][I][J]. */
+/* modal [nfields][M][L] -> nodal [nfields][I][J].  For every batch entry
+ * point, nfields = 0 is a no-op and its buffers may then be NULL. */
 DINO_API int dino_sht_inverse(dino_plan* plan, const float* d_modal, float* d_nodal,
                      int32_t nfields, void* stream);
 /* nodal [nfields][I][J] -> modal [nfields][M][L]. */
