@@ -419,6 +419,7 @@ def run_ours(args):
         'data': 'synthetic',
         'config': {'workload': 'SHT pair TL255 x 128 fields', 'grid': 'TL255',
                    'fields': fields, 'precision': args.precision,
+                   'plan': plan.describe(),
                    'parallelism': f'replicas x{world}',
                    'l2': 'working set ~0.3 GB per step > 126 MB L2 (no flush)'},
         'e2e': {'value': e2e_value, 'unit': 'TFLOP/s',

@@ -132,6 +132,7 @@ SIGNATURES = {
     'dino_pe_step_graph': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32,
                                           _vp]),
     'dino_modal_relayout': (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
+    'dino_plan_describe': (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_size_t]),
     'dino_swe_create': (ctypes.c_int, [_vp, ctypes.POINTER(SWEDesc),
                                        ctypes.POINTER(_vp)]),
     'dino_swe_destroy': (ctypes.c_int, [_vp]),

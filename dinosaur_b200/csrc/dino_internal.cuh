@@ -184,6 +184,7 @@ int modal_op(dino_plan* p, int op, const float* in, float* out, int nfields,
 // Sets kernel attributes ahead of stream capture.
 int sht_prepare(dino_plan* p);
 // FP32 SIMT inverse Legendre contraction for any plan (no precision dispatch).
+std::string tc_describe(dino_plan* p);  // legendre_tc.cu
 int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
                           cudaStream_t st);
 

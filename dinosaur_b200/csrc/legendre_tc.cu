@@ -22,7 +22,10 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cstdio>
 #include <cstring>
+#include <string>
+#include <vector>
 
 #include "dino_internal.cuh"
 
@@ -45,6 +48,9 @@ struct TcTables {
   size_t smem_inv = 0, smem_fwd = 0;
   // N sub-ranges per (m, row tile) CTA and their width (B tile rows).
   int nsplit_inv = 1, nsplit_fwd = 1, Nsub_inv = 0, Nsub_fwd = 0;
+  // Autotuning record: candidates tried and the chosen launch time.
+  int tuned_fields = 0, tried_inv = 0, tried_fwd = 0;
+  float us_inv = 0.f, us_fwd = 0.f;
 };
 
 __host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m - 1) / m * m; }
@@ -612,15 +618,151 @@ static int make_map(CUtensorMap* tm, const bf16* ptr, int inner, long long rows,
   return DINO_OK;
 }
 
-// Pipeline depth within ~104 KB of shared memory, so that two CTAs share an
-// SM (each also holds up to 256 TMEM columns).
-static int pick_stages(int nrows, size_t* smem) {
-  const size_t stage = 2 * 128 * 128 + 2 * (size_t)nrows * 128;
-  int s = (int)((104 * 1024) / stage);
-  if (s > kMaxStages) s = kMaxStages;
-  if (s < 2) s = 2;
-  *smem = stage * s + 1024;
-  return s;
+// ---------------------------------------------------------------------------
+// Autotuning of the tensor-core launch shape
+// ---------------------------------------------------------------------------
+
+constexpr size_t kTcSmemLimit = 220 * 1024;
+
+int tc_status(dino_plan* p);
+
+static int tmem_cols_for(int cols);
+
+// One candidate shape for a direction: the (m, row tile) CTA's N range is
+// split into nsplit ranges of Nsub rows, with a pipeline `stages` deep.
+struct TcShape {
+  int nsplit, Nsub, stages;
+  size_t smem;
+};
+
+static void tc_candidates(int nfull, std::vector<TcShape>* out) {
+  int last_nsub = -1;
+  for (int nsplit : {1, 2, 4}) {
+    const int nsub = round_up((nfull + nsplit - 1) / nsplit, 16);
+    if (nsub == last_nsub || (nsplit > 1 && nsub * (nsplit - 1) >= nfull)) continue;
+    last_nsub = nsub;
+    if (tmem_cols_for(2 * nsub) > 512) continue;
+    const size_t stage = 2 * 128 * 128 + 2 * (size_t)nsub * 128;
+    for (int stages = 2; stages <= kMaxStages; ++stages) {
+      const size_t smem = stage * stages + 1024;
+      if (smem > kTcSmemLimit) break;
+      out->push_back({nsplit, nsub, stages, smem});
+    }
+  }
+}
+
+template <bool kForward>
+static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf, float* out,
+                         cudaEvent_t e0, cudaEvent_t e1, float* us) {
+  const size_t lw2 = (size_t)p->lw * 2;
+  CUtensorMap bh, bl;
+  if (!kForward) {
+    DINO_TRY(make_map(&bh, t->Bih, t->Kp, (long long)lw2 * t->Np, c.Nsub));
+    DINO_TRY(make_map(&bl, t->Bil, t->Kp, (long long)lw2 * t->Np, c.Nsub));
+  } else {
+    DINO_TRY(make_map(&bh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
+    DINO_TRY(make_map(&bl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
+  }
+  TcArgs a{};
+  a.nf = nf;
+  a.M = p->M;
+  a.L = p->L;
+  a.J = p->J;
+  a.Jh = p->Jh;
+  a.Rp = t->Rp;
+  a.Nrows = kForward ? t->Nf : t->Np;
+  a.Nsub = c.Nsub;
+  a.stages = c.stages;
+  a.tmem_cols = tmem_cols_for(2 * c.Nsub);
+  a.out = out;
+  a.err = t->d_err;
+  dim3 grid(ceil_div(2 * nf, 128), p->lw, c.nsplit);
+  const CUtensorMap& ah = kForward ? t->tAfh : t->tAih;
+  const CUtensorMap& al = kForward ? t->tAfl : t->tAil;
+  constexpr int kReps = 3;
+  for (int r = 0; r <= kReps; ++r) {
+    if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
+    legendre_tc_kernel<kForward><<<grid, kTcThreads, c.smem, 0>>>(ah, al, bh, bl, a);
+    DINO_TRY(check_launch("legendre_tc (autotune)"));
+  }
+  DINO_CHECK_CUDA(cudaEventRecord(e1, 0));
+  DINO_CHECK_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  DINO_CHECK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  *us = 1e3f * ms / kReps;
+  return DINO_OK;
+}
+
+// Times every candidate shape of both directions on this plan's tables with
+// an L2-sized batch (the chunk the transforms launch) and keeps the fastest.
+static int tc_autotune(dino_plan* p, TcTables* t) {
+  const size_t per_field = (size_t)p->M * p->J * sizeof(float);
+  int nf = (int)((48ull << 20) / (per_field ? per_field : 1));
+  nf = nf < 1 ? 1 : nf;
+  nf = nf > t->cap ? t->cap : nf;
+  t->tuned_fields = nf;
+  float* fwd_out = nullptr;
+  DINO_CHECK_CUDA(cudaMalloc(&fwd_out, sizeof(float) * (size_t)nf * p->M * p->L));
+  cudaEvent_t e0, e1;
+  DINO_CHECK_CUDA(cudaEventCreate(&e0));
+  DINO_CHECK_CUDA(cudaEventCreate(&e1));
+  auto tune = [&](bool forward) -> int {
+    std::vector<TcShape> cands;
+    tc_candidates(forward ? t->Nf : t->Np, &cands);
+    float best = 1e30f;
+    TcShape pick = cands.front();
+    for (const TcShape& c : cands) {
+      float us = 0.f;
+      const int rc = forward ? tc_time_shape<true>(p, t, c, nf, fwd_out, e0, e1, &us)
+                             : tc_time_shape<false>(p, t, c, nf, p->d_work, e0, e1, &us);
+      if (rc != DINO_OK) return rc;
+      if (us < best) {
+        best = us;
+        pick = c;
+      }
+    }
+    const size_t lw2 = (size_t)p->lw * 2;
+    if (forward) {
+      t->nsplit_fwd = pick.nsplit;
+      t->Nsub_fwd = pick.Nsub;
+      t->stages_fwd = pick.stages;
+      t->smem_fwd = pick.smem;
+      t->us_fwd = best;
+      t->tried_fwd = (int)cands.size();
+      DINO_TRY(make_map(&t->tBfh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
+      DINO_TRY(make_map(&t->tBfl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
+    } else {
+      t->nsplit_inv = pick.nsplit;
+      t->Nsub_inv = pick.Nsub;
+      t->stages_inv = pick.stages;
+      t->smem_inv = pick.smem;
+      t->us_inv = best;
+      t->tried_inv = (int)cands.size();
+      DINO_TRY(make_map(&t->tBih, t->Bih, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
+      DINO_TRY(make_map(&t->tBil, t->Bil, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
+    }
+    return DINO_OK;
+  };
+  int rc = tune(false);
+  if (rc == DINO_OK) rc = tune(true);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(fwd_out);
+  if (rc != DINO_OK) return rc;
+  return tc_status(p);
+}
+
+std::string tc_describe(dino_plan* p) {
+  TcTables* t = p->tc;
+  if (!t) return "";
+  char buf[512];
+  snprintf(buf, sizeof(buf),
+           "tcgen05 split-BF16 Legendre autotuned on %d fields: inverse %d N ranges of "
+           "%d rows, %d stages (%.1f us, %d shapes tried); forward %d N ranges of %d rows, "
+           "%d stages (%.1f us, %d shapes tried)",
+           t->tuned_fields, t->nsplit_inv, t->Nsub_inv, t->stages_inv, t->us_inv,
+           t->tried_inv, t->nsplit_fwd, t->Nsub_fwd, t->stages_fwd, t->us_fwd, t->tried_fwd);
+  return buf;
 }
 
 int tc_tables_build(dino_plan* p) {
@@ -669,29 +811,19 @@ int tc_tables_build(dino_plan* p) {
   tc_table_kernel<<<grid, 128>>>(p->lw, p->L, p->Jh, p->d_x64, t->Kp, t->Np, t->Kj, t->Nf,
                                  t->Bih, t->Bil, t->Bfh, t->Bfl);
   DINO_TRY(check_launch("tc_table"));
-  // Two N ranges per (m, row tile) once a table has 64 or more rows.
-  t->nsplit_inv = t->Np >= 64 ? 2 : 1;
-  t->nsplit_fwd = t->Nf >= 64 ? 2 : 1;
-  t->Nsub_inv = round_up((t->Np + t->nsplit_inv - 1) / t->nsplit_inv, 16);
-  t->Nsub_fwd = round_up((t->Nf + t->nsplit_fwd - 1) / t->nsplit_fwd, 16);
   const long long rowsA = (long long)lw2 * t->Rp;
   DINO_TRY(make_map(&t->tAih, t->Aih, t->Kp, rowsA, 128));
   DINO_TRY(make_map(&t->tAil, t->Ail, t->Kp, rowsA, 128));
-  DINO_TRY(make_map(&t->tBih, t->Bih, t->Kp, (long long)lw2 * t->Np, t->Nsub_inv));
-  DINO_TRY(make_map(&t->tBil, t->Bil, t->Kp, (long long)lw2 * t->Np, t->Nsub_inv));
   DINO_TRY(make_map(&t->tAfh, t->Afh, t->Kj, rowsA, 128));
   DINO_TRY(make_map(&t->tAfl, t->Afl, t->Kj, rowsA, 128));
-  DINO_TRY(make_map(&t->tBfh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, t->Nsub_fwd));
-  DINO_TRY(make_map(&t->tBfl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, t->Nsub_fwd));
-  t->stages_inv = pick_stages(t->Nsub_inv, &t->smem_inv);
-  t->stages_fwd = pick_stages(t->Nsub_fwd, &t->smem_fwd);
   DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)t->smem_inv));
+                                       (int)kTcSmemLimit));
   DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)t->smem_fwd));
-  return DINO_OK;
+                                       (int)kTcSmemLimit));
+  DINO_CHECK_CUDA(cudaDeviceSynchronize());
+  return tc_autotune(p, t);
 }
 
 void tc_tables_free(dino_plan* p) {
@@ -795,6 +927,21 @@ int tc_status(dino_plan* p) {
 }
 
 }  // namespace dino
+
+extern "C" int dino_plan_describe(dino_plan* p, char* buf, size_t len) {
+  DINO_REQUIRE(p && buf && len > 0, DINO_ERR_ARG, "dino_plan_describe: null argument");
+  char head[256];
+  snprintf(head, sizeof(head),
+           "grid %d x %d nodes, %d x %d modal, Legendre %s, batch capacity %d fields",
+           p->I, p->J, p->M, p->L,
+           p->precision == DINO_PREC_BF16X3 ? "split-BF16 (tcgen05)" : "FP32 (SIMT)",
+           p->max_fields);
+  std::string s = head;
+  const std::string tc = dino::tc_describe(p);
+  if (!tc.empty()) s += "; " + tc;
+  snprintf(buf, len, "%s", s.c_str());
+  return DINO_OK;
+}
 
 extern "C" int dino_plan_status(dino_plan* p) {
   DINO_REQUIRE(p, DINO_ERR_ARG, "dino_plan_status: null argument");

@@ -219,6 +219,12 @@ class Plan:
     n = int(np.prod(lead)) if lead else 1
     return self._call('dino_sht_forward_adjoint', g, lead + (self.I, self.J), n)
 
+  def describe(self) -> str:
+    """Shapes, Legendre form and (split-BF16) the autotuned launch shapes."""
+    buf = ctypes.create_string_buffer(1024)
+    _lib.check(_lib.lib().dino_plan_describe(self.handle, buf, len(buf)), 'describe')
+    return buf.value.decode()
+
   def relayout(self, x: torch.Tensor, to_fast: bool) -> torch.Tensor:
     """Real <-> FastSphericalHarmonics modal rows (dino_modal_relayout)."""
     rows_in = self.M + (0 if to_fast else 1)

@@ -112,6 +112,12 @@ DINO_API int dino_plan_nodes(const dino_plan* plan, double* host_sin_lat,
 DINO_API int dino_plan_legendre_column(const dino_plan* plan, int32_t m, int32_t l,
                               double* host_out);
 
+/* A one-line description of the plan (shapes, Legendre form, and for the
+ * split-BF16 form the launch shapes its autotuner chose at creation and
+ * their measured times), NUL-terminated and truncated to len bytes.  No
+ * counterpart in the reference. */
+DINO_API int dino_plan_describe(dino_plan* plan, char* buf, size_t len);
+
 /* Synchronizes the device and reports whether any bounded device-side wait
  * of this plan's kernels gave up (DINO_ERR_TIMEOUT); DINO_OK otherwise. */
 DINO_API int dino_plan_status(dino_plan* plan);

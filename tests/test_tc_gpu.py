@@ -112,3 +112,13 @@ def test_tc_primitive_equations_match_fp64_oracle():
   lhs = tree_dot(gpu_vjp(step, st, w), v)
   rhs = central_dot(ostep, st, w, v)
   assert abs(lhs - rhs) <= 1e-4 * abs(rhs), (lhs, rhs)
+
+
+def test_autotuner_records_its_choice():
+  """The split-BF16 plan times its candidate launch shapes at creation and
+  keeps the fastest; the choice and its time are reported."""
+  g = tc_grid('TL255')
+  d = g.plan.describe()
+  assert 'autotuned' in d and 'shapes tried' in d, d
+  assert 'split-BF16' in d
+  assert 'FP32 (SIMT)' in sh.Grid.T21().plan.describe()
