@@ -458,6 +458,7 @@ def pe_extras(torch):
   cases = [
       # name, grid, layers, members, held_suarez, moist, dt [min], precision
       ('T42_L24_x16_held_suarez', 'T42', 24, 16, True, False, 15, 'fp32'),
+      ('T42_L24_x16_held_suarez_bf16x3', 'T42', 24, 16, True, False, 15, 'bf16x3'),
       ('TL255_L32_dry', 'TL255', 32, 1, False, False, 6, 'fp32'),
       ('TL255_L32_dry_bf16x3', 'TL255', 32, 1, False, False, 6, 'bf16x3'),
       ('TL255_L32_moist3_x4', 'TL255', 32, 4, False, True, 6, 'fp32'),
@@ -517,7 +518,63 @@ def pe_extras(torch):
     del eng, buf, state, eq
     torch.cuda.empty_cache()
   out.update(small_and_gradient_cases(torch))
+  out.update(large_gradient_case(torch))
   return out
+
+
+def large_gradient_case(torch):
+  """The reverse pass of the large configuration: 12 filtered SIL3 steps of
+  TL255 / 32 levels, moist with two passive tracers, 4 members, split-BF16
+  Legendre -- forward with per-step checkpoints, then the step VJPs."""
+  from dinosaur_b200 import coordinate_systems, primitive_equations as pe
+  from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
+  from dinosaur_b200 import time_integration as ti, units
+  layers, members, steps = 32, 4, 12
+  impl = functools.partial(sh.CudaSphericalHarmonics, precision='bf16x3')
+  g = sh.Grid.TL255(spherical_harmonics_impl=impl)
+  coords = coordinate_systems.CoordinateSystem(
+      g, sigma_coordinates.SigmaCoordinates.equidistant(layers))
+  eq = pe.PrimitiveEquationsSigma(np.linspace(220.0, 288.0, layers),
+                                  np.zeros(g.modal_shape, np.float32), coords,
+                                  units.SimUnits(), humidity_key='specific_humidity')
+  dt = units.nondim_time(6 * 60.0)
+  step = ti.repeated(ti.step_with_filters(ti.imex_rk_sil3(eq, dt),
+                                          [ti.exponential_step_filter(g, dt)]), steps)
+  rng = np.random.default_rng(2)
+  _, l = g.modal_mesh
+  scale = g.mask / (l + 1.0) ** 2
+  shape = (members, layers) + g.modal_shape
+  noise = lambda s, a=1e-4: torch.as_tensor((a * rng.standard_normal(s) * scale)
+                                            .astype(np.float32), device='cuda')
+  const = np.zeros(shape, np.float32)
+  const[..., 0, 0] = 2.0 * np.sqrt(np.pi)
+  const = torch.as_tensor(const, device='cuda')
+
+  def run():
+    x = pe.State(noise(shape), noise(shape), noise(shape), noise((members, 1) + g.modal_shape),
+                 tracers={'specific_humidity': 5e-3 * const + noise(shape, 1e-6),
+                          'tracer_a': const + noise(shape), 'tracer_b': const + noise(shape)})
+    leaves = [x.vorticity, x.divergence, x.temperature_variation, x.log_surface_pressure]
+    for t in leaves:
+      t.requires_grad_(True)
+    y = step(x)
+    loss = (y.temperature_variation ** 2).mean() + (y.vorticity ** 2).mean()
+    loss.backward()
+    return bool(all(torch.isfinite(t.grad).all() for t in leaves))
+
+  run()
+  torch.cuda.synchronize()
+  a0 = torch.cuda.Event(enable_timing=True)
+  a1 = torch.cuda.Event(enable_timing=True)
+  a0.record()
+  finite = run()
+  a1.record()
+  torch.cuda.synchronize()
+  ms = a0.elapsed_time(a1)
+  return {'TL255_L32_moist3_x4_bf16x3_grad_12_steps': {
+      'ms_per_rollout': ms, 'steps': steps, 'members': members,
+      'precision': 'bf16x3', 'what': 'forward (checkpointed) + reverse sweep',
+      'finite': finite}}
 
 
 def small_and_gradient_cases(torch):
