@@ -113,6 +113,9 @@ struct dino_plan {
   // Workspace: intermediate Fourier coefficients [max_fields][M][J].
   float* d_work = nullptr;
   dino::TcTables* tc = nullptr;
+  // Second stream for alternating L2-sized chunks, with fork/join events.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace dino {
@@ -171,10 +174,12 @@ int sht_inverse_adjoint_to(dino_plan* p, const float* nodal_ct, float* modal_ct,
                            int nfields, float* work, int work_fields, cudaStream_t st);
 int sht_forward_adjoint_to(dino_plan* p, const float* modal_ct, float* nodal_ct,
                            int nfields, float* work, int work_fields, cudaStream_t st);
+// slot: -1 uses the whole tensor-core operand slabs; 0 / 1 one half each, so
+// that two chunks can run at once on different streams.
 int legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
-                     int nfields, cudaStream_t st);
+                     int nfields, cudaStream_t st, int slot = -1);
 int legendre_forward(dino_plan* p, const float* fourier, float* out_modal,
-                     int nfields, cudaStream_t st);
+                     int nfields, cudaStream_t st, int slot = -1);
 int fourier_inverse(dino_plan* p, const float* fourier, float* nodal,
                     int nfields, bool weighted_adjoint, cudaStream_t st);
 int fourier_forward(dino_plan* p, const float* nodal, float* fourier,
@@ -192,9 +197,11 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 int tc_tables_build(dino_plan* p);
 void tc_tables_free(dino_plan* p);
 int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
-                        int nfields, cudaStream_t st);
+                        int nfields, cudaStream_t st, int slot);
 int tc_legendre_forward(dino_plan* p, const float* fourier, float* out_modal,
-                        int nfields, cudaStream_t st);
+                        int nfields, cudaStream_t st, int slot);
+// Fields one operand-slab half holds (any count for the FP32 path).
+int tc_slot_fields(dino_plan* p);
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 

@@ -129,7 +129,7 @@ __device__ __forceinline__ void store_split8(const float (&v)[8], bf16* hi, bf16
 // parities (16 consecutive l, read as one contiguous run) and writes them as
 // 16-byte stores.
 __global__ void tc_split_inverse_kernel(Segs in, int nf, int M, int L, int Rp,
-                                        int Kp, bf16* __restrict__ Ah,
+                                        int Kp, int roff, bf16* __restrict__ Ah,
                                         bf16* __restrict__ Al) {
   const int m = blockIdx.y;
   const int rows = (m == 0) ? nf : 2 * nf;
@@ -150,8 +150,8 @@ __global__ void tc_split_inverse_kernel(Segs in, int nf, int M, int L, int Rp,
     ev[i] = (ke < Lm) ? xr[ke] : 0.f;
     od[i] = (ko < Lm) ? xr[ko] : 0.f;
   }
-  const size_t o0 = ((size_t)(m * 2) * Rp + r) * Kp + 8 * g;
-  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + r) * Kp + 8 * g;
+  const size_t o0 = ((size_t)(m * 2) * Rp + roff + r) * Kp + 8 * g;
+  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + roff + r) * Kp + 8 * g;
   store_split8(ev, Ah + o0, Al + o0);
   store_split8(od, Ah + o1, Al + o1);
 }
@@ -161,7 +161,7 @@ __global__ void tc_split_inverse_kernel(Segs in, int nf, int M, int L, int Rp,
 // folds 8 consecutive latitudes against their mirrors and writes 16-byte
 // stores.
 __global__ void tc_fold_forward_kernel(const float* __restrict__ G, int nf, int M,
-                                       int J, int Jh, int Rp, int Kj,
+                                       int J, int Jh, int Rp, int Kj, int roff,
                                        bf16* __restrict__ Ah, bf16* __restrict__ Al) {
   const int m = blockIdx.y;
   const int rows = (m == 0) ? nf : 2 * nf;
@@ -204,8 +204,8 @@ __global__ void tc_fold_forward_kernel(const float* __restrict__ G, int nf, int 
       dv[i] = d;
     }
   }
-  const size_t o0 = ((size_t)(m * 2) * Rp + r) * Kj + j0;
-  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + r) * Kj + j0;
+  const size_t o0 = ((size_t)(m * 2) * Rp + roff + r) * Kj + j0;
+  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + roff + r) * Kj + j0;
   store_split8(sv, Ah + o0, Al + o0);
   store_split8(dv, Ah + o1, Al + o1);
 }
@@ -335,6 +335,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 struct TcArgs {
   int nf, M, L, J, Jh;
   int Rp;        // A slab rows
+  int roff;      // first A slab row of this launch (operand-slab half)
   int Nrows;     // rows of one (m, parity) B table (Np or Nf)
   int Nsub;      // B tile rows = N columns of this CTA (blockIdx.z-th range)
   int stages;
@@ -423,7 +424,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
       const int k = (p == 0) ? i : i - kblk[0];
       uint8_t* st = base + (size_t)s * stage_bytes;
       mbar_expect_tx(&full_bar[s], stage_bytes);
-      const int ya = (m * 2 + p) * a.Rp + tile * 128;
+      const int ya = (m * 2 + p) * a.Rp + a.roff + tile * 128;
       const int yb = (m * 2 + p) * a.Nrows + lo;
       tma_load_2d(st, &tAh, &full_bar[s], k * 64, ya);
       tma_load_2d(st + tile_a, &tAl, &full_bar[s], k * 64, ya);
@@ -848,18 +849,28 @@ static int tmem_cols_for(int cols) {
   return c;
 }
 
+// Rows of one operand-slab half (a multiple of the 128-row MMA tile).
+static int tc_slot_rows(const TcTables* t) { return (t->Rp / 2) / 128 * 128; }
+
+int tc_slot_fields(dino_plan* p) {
+  return p->tc ? tc_slot_rows(p->tc) / 2 : (1 << 30);
+}
+
 int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
-                        cudaStream_t st) {
+                        cudaStream_t st, int slot) {
   TcTables* t = p->tc;
   DINO_REQUIRE(t, DINO_ERR_ARG, "plan has no tensor-core tables");
   const size_t ms = (size_t)p->M * p->L, fs = (size_t)p->M * p->J;
-  for (int f0 = 0; f0 < nf; f0 += t->cap) {
-    const int n = nf - f0 < t->cap ? nf - f0 : t->cap;
+  const int cap = slot < 0 ? t->cap : tc_slot_rows(t) / 2;
+  const int roff = slot > 0 ? tc_slot_rows(t) : 0;
+  DINO_REQUIRE(cap >= 1, DINO_ERR_UNSUPPORTED, "operand slab too small for two slots");
+  for (int f0 = 0; f0 < nf; f0 += cap) {
+    const int n = nf - f0 < cap ? nf - f0 : cap;
     Segs sub = seg_offset(in, f0, n, ms);
     const int max_rows = 2 * n;
     dim3 g1((unsigned)(((size_t)max_rows * (t->Kp / 8) + 255) / 256), p->lw);
-    tc_split_inverse_kernel<<<g1, 256, 0, st>>>(sub, n, p->M, p->L, t->Rp, t->Kp, t->Aih,
-                                                t->Ail);
+    tc_split_inverse_kernel<<<g1, 256, 0, st>>>(sub, n, p->M, p->L, t->Rp, t->Kp, roff,
+                                                t->Aih, t->Ail);
     DINO_TRY(check_launch("tc_split_inverse"));
     TcArgs a{};
     a.nf = n;
@@ -868,6 +879,7 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
     a.J = p->J;
     a.Jh = p->Jh;
     a.Rp = t->Rp;
+    a.roff = roff;
     a.Nrows = t->Np;
     a.Nsub = t->Nsub_inv;
     a.stages = t->stages_inv;
@@ -883,16 +895,19 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
 }
 
 int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
-                        cudaStream_t st) {
+                        cudaStream_t st, int slot) {
   TcTables* t = p->tc;
   DINO_REQUIRE(t, DINO_ERR_ARG, "plan has no tensor-core tables");
   const size_t ms = (size_t)p->M * p->L, fs = (size_t)p->M * p->J;
-  for (int f0 = 0; f0 < nf; f0 += t->cap) {
-    const int n = nf - f0 < t->cap ? nf - f0 : t->cap;
+  const int cap = slot < 0 ? t->cap : tc_slot_rows(t) / 2;
+  const int roff = slot > 0 ? tc_slot_rows(t) : 0;
+  DINO_REQUIRE(cap >= 1, DINO_ERR_UNSUPPORTED, "operand slab too small for two slots");
+  for (int f0 = 0; f0 < nf; f0 += cap) {
+    const int n = nf - f0 < cap ? nf - f0 : cap;
     const int max_rows = 2 * n;
     dim3 g1((unsigned)(((size_t)max_rows * (t->Kj / 8) + 255) / 256), p->lw);
     tc_fold_forward_kernel<<<g1, 256, 0, st>>>(G + f0 * fs, n, p->M, p->J, p->Jh, t->Rp, t->Kj,
-                                               t->Afh, t->Afl);
+                                               roff, t->Afh, t->Afl);
     DINO_TRY(check_launch("tc_fold_forward"));
     TcArgs a{};
     a.nf = n;
@@ -901,6 +916,7 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
     a.J = p->J;
     a.Jh = p->Jh;
     a.Rp = t->Rp;
+    a.roff = roff;
     a.Nrows = t->Nf;
     a.Nsub = t->Nsub_fwd;
     a.stages = t->stages_fwd;

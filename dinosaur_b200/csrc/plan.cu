@@ -148,6 +148,12 @@ static int upload(T** dst, const std::vector<T>& src) {
 
 static void plan_free(dino_plan* p) {
   if (!p) return;
+  if (p->side) {
+    cudaStreamSynchronize(p->side);
+    cudaStreamDestroy(p->side);
+  }
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   tc_tables_free(p);
   cudaFree(p->d_x64);
   cudaFree(p->d_w64);
@@ -287,6 +293,10 @@ static int plan_build(dino_plan* p, const dino_grid_desc* d) {
 
   // Workspace for the intermediate Fourier coefficients.
   DINO_CHECK_CUDA(cudaMalloc(&p->d_work, sizeof(float) * (size_t)p->max_fields * M * J));
+  // Side stream and fork/join events for alternating chunks.
+  DINO_CHECK_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+  DINO_CHECK_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+  DINO_CHECK_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
 
   if (p->precision == DINO_PREC_BF16X3) DINO_TRY(tc_tables_build(p));
   DINO_CHECK_CUDA(cudaDeviceSynchronize());

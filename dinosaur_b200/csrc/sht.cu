@@ -306,9 +306,9 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 }
 
 int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
-                     cudaStream_t st) {
+                     cudaStream_t st, int slot) {
   if (p->precision == DINO_PREC_BF16X3)
-    return tc_legendre_inverse(p, in, out, nf, st);
+    return tc_legendre_inverse(p, in, out, nf, st, slot);
   dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
       in, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
@@ -316,9 +316,9 @@ int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
 }
 
 int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
-                     cudaStream_t st) {
+                     cudaStream_t st, int slot) {
   if (p->precision == DINO_PREC_BF16X3)
-    return tc_legendre_forward(p, G, out, nf, st);
+    return tc_legendre_forward(p, G, out, nf, st, slot);
   dim3 grid(ceil_div(p->L, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_forward_simt<<<grid, kLegThreads, 0, st>>>(
       G, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
@@ -755,29 +755,69 @@ static int l2_chunk(dino_plan* p, int nf, int work_fields) {
   return (nf + chunks - 1) / chunks;
 }
 
+// Chunks alternate between the caller's stream and the plan's side stream
+// when two of them fit in the workspace (and in the tensor-core operand
+// slabs): each stream has its own half, both chunks' intermediates stay in
+// L2, and one chunk's kernels fill the SMs the other leaves idle in its
+// waves' tails.  The side stream forks from and joins back into the
+// caller's stream with events, so the pattern also records into CUDA graphs.
+struct ChunkRun {
+  dino_plan* p;
+  cudaStream_t st;
+  float* work;
+  size_t work_stride;  // floats per half
+  bool dual = false;
+
+  ChunkRun(dino_plan* p_, cudaStream_t st_, float* work_, int chunk, int nf,
+           int work_fields)
+      : p(p_), st(st_), work(work_), work_stride((size_t)chunk * p_->M * p_->J) {
+    dual = p->side && nf > chunk && 2 * chunk <= work_fields &&
+           chunk <= tc_slot_fields(p);
+  }
+  int begin() {
+    if (!dual) return DINO_OK;
+    DINO_CHECK_CUDA(cudaEventRecord(p->ev_fork, st));
+    DINO_CHECK_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    return DINO_OK;
+  }
+  int slot(int c) const { return dual ? (c & 1) : -1; }
+  cudaStream_t stream(int c) const { return slot(c) == 1 ? p->side : st; }
+  float* buf(int c) const { return work + (slot(c) == 1 ? work_stride : 0); }
+  int end() {
+    if (!dual) return DINO_OK;
+    DINO_CHECK_CUDA(cudaEventRecord(p->ev_join, p->side));
+    DINO_CHECK_CUDA(cudaStreamWaitEvent(st, p->ev_join, 0));
+    return DINO_OK;
+  }
+};
+
 int sht_inverse_segs(dino_plan* p, const Segs& in, float* out, int nf,
                      float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
   const int chunk = l2_chunk(p, nf, work_fields);
-  for (int f0 = 0; f0 < nf; f0 += chunk) {
+  ChunkRun run(p, st, work, chunk, nf, work_fields);
+  DINO_TRY(run.begin());
+  for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
     Segs sub = seg_offset(in, f0, n, ms);
-    DINO_TRY(legendre_inverse(p, sub, work, n, st));
-    DINO_TRY(fourier_inverse(p, work, out + f0 * ns, n, false, st));
+    DINO_TRY(legendre_inverse(p, sub, run.buf(c), n, run.stream(c), run.slot(c)));
+    DINO_TRY(fourier_inverse(p, run.buf(c), out + f0 * ns, n, false, run.stream(c)));
   }
-  return DINO_OK;
+  return run.end();
 }
 
 int sht_forward_to(dino_plan* p, const float* nodal, float* out, int nf,
                    float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
   const int chunk = l2_chunk(p, nf, work_fields);
-  for (int f0 = 0; f0 < nf; f0 += chunk) {
+  ChunkRun run(p, st, work, chunk, nf, work_fields);
+  DINO_TRY(run.begin());
+  for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
-    DINO_TRY(fourier_forward(p, nodal + f0 * ns, work, n, true, st));
-    DINO_TRY(legendre_forward(p, work, out + f0 * ms, n, st));
+    DINO_TRY(fourier_forward(p, nodal + f0 * ns, run.buf(c), n, true, run.stream(c)));
+    DINO_TRY(legendre_forward(p, run.buf(c), out + f0 * ms, n, run.stream(c), run.slot(c)));
   }
-  return DINO_OK;
+  return run.end();
 }
 
 // Adjoint of the inverse transform: unweighted forward Fourier, then the
@@ -788,24 +828,30 @@ int sht_inverse_adjoint_to(dino_plan* p, const float* nodal_ct, float* modal_ct,
                            int nf, float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
   const int chunk = l2_chunk(p, nf, work_fields);
-  for (int f0 = 0; f0 < nf; f0 += chunk) {
+  ChunkRun run(p, st, work, chunk, nf, work_fields);
+  DINO_TRY(run.begin());
+  for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
-    DINO_TRY(fourier_forward(p, nodal_ct + f0 * ns, work, n, false, st));
-    DINO_TRY(legendre_forward(p, work, modal_ct + f0 * ms, n, st));
+    DINO_TRY(fourier_forward(p, nodal_ct + f0 * ns, run.buf(c), n, false, run.stream(c)));
+    DINO_TRY(legendre_forward(p, run.buf(c), modal_ct + f0 * ms, n, run.stream(c),
+                              run.slot(c)));
   }
-  return DINO_OK;
+  return run.end();
 }
 
 int sht_forward_adjoint_to(dino_plan* p, const float* modal_ct, float* nodal_ct,
                            int nf, float* work, int work_fields, cudaStream_t st) {
   const size_t ms = (size_t)p->M * p->L, ns = (size_t)p->I * p->J;
   const int chunk = l2_chunk(p, nf, work_fields);
-  for (int f0 = 0; f0 < nf; f0 += chunk) {
+  ChunkRun run(p, st, work, chunk, nf, work_fields);
+  DINO_TRY(run.begin());
+  for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
-    DINO_TRY(legendre_inverse(p, one_seg(modal_ct + f0 * ms, n), work, n, st));
-    DINO_TRY(fourier_inverse(p, work, nodal_ct + f0 * ns, n, true, st));
+    DINO_TRY(legendre_inverse(p, one_seg(modal_ct + f0 * ms, n), run.buf(c), n,
+                              run.stream(c), run.slot(c)));
+    DINO_TRY(fourier_inverse(p, run.buf(c), nodal_ct + f0 * ns, n, true, run.stream(c)));
   }
-  return DINO_OK;
+  return run.end();
 }
 
 static int sht_inverse_adjoint(dino_plan* p, const float* nodal_ct,
