@@ -186,11 +186,41 @@ class FusedSIL3Step:
     return buf
 
 
+@dataclasses.dataclass
+class TimeReversedImExODE(ImplicitExplicitODE):
+  """An ImplicitExplicitODE reversed in time (time_integration.py:117-138):
+  dx/dt = -explicit_terms(x) - implicit_terms(x)."""
+
+  forward_eq: Any
+
+  def explicit_terms(self, state):
+    return pytree.tree_map(lambda x: -x if _is_tensor_like(x) else x,
+                           self.forward_eq.explicit_terms(state))
+
+  def implicit_terms(self, state):
+    return pytree.tree_map(lambda x: -x if _is_tensor_like(x) else x,
+                           self.forward_eq.implicit_terms(state))
+
+  def implicit_inverse(self, state, step_size: float):
+    return self.forward_eq.implicit_inverse(state, -step_size)
+
+
+def _is_tensor_like(x):
+  return isinstance(x, (torch.Tensor, np.ndarray, float, int)) and x is not None
+
+
 def imex_rk_sil3(equation, time_step: float):
-  """SIL3 IMEX-RK step (time_integration.py:375-405)."""
+  """SIL3 IMEX-RK step (time_integration.py:375-405).
+
+  The primitive equations take the fused CUDA step; their time-reversed ODE
+  is the same step with -dt (negated explicit and implicit terms, implicit
+  inverse at -eta)."""
   from dinosaur_b200 import primitive_equations as pe  # pylint: disable=g-import-not-at-top
   if isinstance(equation, pe.PrimitiveEquationsSigma):
     return FusedSIL3Step(equation, float(time_step))
+  if (isinstance(equation, TimeReversedImExODE) and
+      isinstance(equation.forward_eq, pe.PrimitiveEquationsSigma)):
+    return FusedSIL3Step(equation.forward_eq, -float(time_step))
   return imex_runge_kutta(SIL3_TABLEAU, equation, time_step)
 
 
@@ -301,3 +331,72 @@ def trajectory_from_step(step_fn, outer_steps: int, inner_steps: int, *,
     return x, _stack(frames)
 
   return multistep
+
+
+# ---------------------------------------------------------------------------
+# Digital filter initialisation (time_integration.py:640-716)
+# ---------------------------------------------------------------------------
+
+
+def accumulate_repeated(step_fn, weights, state, scan_fn=None):
+  """Weighted sum of the states along repeated steps (time_integration.py:645-660)."""
+  del scan_fn
+
+  def zeros(x):
+    return torch.zeros_like(x) if isinstance(x, torch.Tensor) else (
+        np.zeros_like(x) if isinstance(x, np.ndarray) else x)
+
+  averaged = pytree.tree_map(zeros, state)
+  for w in np.asarray(weights):
+    state = step_fn(state)
+    averaged = pytree.tree_map(
+        lambda s, a, w=float(w): a + w * s if _is_array_leaf(s) else a,
+        state, averaged)
+  return averaged
+
+
+def _is_array_leaf(x):
+  return isinstance(x, (torch.Tensor, np.ndarray)) and x.ndim > 0
+
+
+def _dfi_lanczos_weights(time_span: float, cutoff_period: float,
+                         dt: float) -> np.ndarray:
+  """Lanczos weights of the filter window (time_integration.py:663-670)."""
+  n_steps = round(time_span / (2 * dt))
+  n = np.arange(1, n_steps + 1)
+  return (np.sinc(n / (n_steps + 1)) *
+          np.sinc(n * time_span / (cutoff_period * n_steps)))
+
+
+def digital_filter_initialization(equation, ode_solver, filters,
+                                  time_span: float, cutoff_period: float,
+                                  dt: float):
+  """Digital filter initialisation (time_integration.py:673-716; Lynch &
+  Huang 1992): the Lanczos-weighted mean of forward and time-reversed
+  rollouts over [-time_span / 2, time_span / 2]."""
+
+  def f(state):
+    forward_step = step_with_filters(ode_solver(equation, dt), filters)
+    backward_step = step_with_filters(
+        ode_solver(TimeReversedImExODE(equation), dt), filters)
+    weights = _dfi_lanczos_weights(time_span, cutoff_period, dt)
+    init_weight = 1.0
+    total_weight = init_weight + 2 * weights.sum()
+    init_weight /= total_weight
+    weights = weights / total_weight
+    init_term = pytree.tree_map(
+        lambda x: x * init_weight if _is_array_leaf(x) else x, state)
+    forward_term = accumulate_repeated(forward_step, weights, state)
+    backward_term = accumulate_repeated(backward_step, weights, state)
+    return pytree.tree_map(
+        lambda a, b, c: a + b + c if _is_array_leaf(a) else a,
+        init_term, forward_term, backward_term)
+
+  return f
+
+
+def maybe_fix_sim_time_roundoff(state, dt: float):
+  """Rounds sim_time to a multiple of dt (time_integration.py:719-726)."""
+  if getattr(state, 'sim_time', None) is not None:
+    state.sim_time = dt * round(state.sim_time / dt)
+  return state

@@ -725,6 +725,56 @@ def step_with_filters(step_fn, filters):
   return _step
 
 
+class TimeReversedImExODE:
+  """dx/dt = -explicit(x) - implicit(x) (time_integration.py:117-138)."""
+
+  def __init__(self, forward_eq):
+    self.forward_eq = forward_eq
+
+  def explicit_terms(self, state):
+    return tree_map(np.negative, self.forward_eq.explicit_terms(state))
+
+  def implicit_terms(self, state):
+    return tree_map(np.negative, self.forward_eq.implicit_terms(state))
+
+  def implicit_inverse(self, state, step_size):
+    return self.forward_eq.implicit_inverse(state, -step_size)
+
+
+def accumulate_repeated(step_fn, weights, state):
+  """time_integration.py:645-660: sum_n w_n x_n along x_{n+1} = step(x_n)."""
+  averaged = tree_map(np.zeros_like, state)
+  for w in weights:
+    state = step_fn(state)
+    averaged = tree_map(lambda s, a, w=w: a + w * s, state, averaged)
+  return averaged
+
+
+def dfi_lanczos_weights(time_span, cutoff_period, dt):
+  """time_integration.py:663-670."""
+  n_steps = round(time_span / (2 * dt))
+  n = np.arange(1, n_steps + 1)
+  return (np.sinc(n / (n_steps + 1)) *
+          np.sinc(n * time_span / (cutoff_period * n_steps)))
+
+
+def digital_filter_initialization(equation, ode_solver, filters, time_span,
+                                  cutoff_period, dt):
+  """time_integration.py:673-716 (Lynch & Huang 1992)."""
+  def f(state):
+    forward = step_with_filters(ode_solver(equation, dt), filters)
+    backward = step_with_filters(
+        ode_solver(TimeReversedImExODE(equation), dt), filters)
+    weights = dfi_lanczos_weights(time_span, cutoff_period, dt)
+    total = 1.0 + 2 * weights.sum()
+    weights = weights / total
+    init = tree_map(lambda x: x / total, state)
+    fwd = accumulate_repeated(forward, weights, state)
+    bwd = accumulate_repeated(backward, weights, state)
+    return tree_map(lambda *xs: sum(xs), init, fwd, bwd)
+  return f
+
+
 def repeated(fn, steps):
   """time_integration.py:508-520 (a Python loop instead of lax.scan)."""
   def f(x):

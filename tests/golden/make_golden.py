@@ -155,6 +155,19 @@ def main(reference_root='/root/reference'):
         **pack('implicit', impl), **pack('inverse', inv),
         **pack('step1', s1), **pack('step2', s2))
 
+  # -- digital filter initialisation (time_integration.py:645-712) ---------
+  dfi_dt = dt
+  dfi = time_integration.digital_filter_initialization(
+      eq, time_integration.imex_rk_sil3,
+      [time_integration.exponential_step_filter(grid, dfi_dt)],
+      time_span=8 * dfi_dt, cutoff_period=8 * dfi_dt, dt=dfi_dt)
+  dfi_out = dfi(state)
+  reversed_eq = time_integration.TimeReversedImExODE(eq)
+  rev_step = time_integration.imex_rk_sil3(reversed_eq, dfi_dt)
+  _save('dfi_T21_L6.npz', dt=dfi_dt,
+        weights=time_integration._dfi_lanczos_weights(8 * dfi_dt, 8 * dfi_dt, dfi_dt),
+        **pack('dfi', dfi_out), **pack('reversed_step', rev_step(state)))
+
   # -- moist primitive equations with a passive tracer -------------------
   q = 5e-3 * (1 + 0.2 * bump / np.abs(bump).max())
   q_modal = np.asarray(q)

@@ -246,3 +246,17 @@ def test_fast_layout_is_the_real_layout_with_a_zero_row():
   for name in ('d_dlon', 'laplacian', 'cos_lat_d_dlat', 'sec_lat_d_dlat_cos2'):
     close(sht.real_to_fast(getattr(grid, name)(x)), g[name], atol=1e-12)
   close(sht.real_to_fast(grid.clip_wavenumbers(x)), g['clip'], atol=0)
+
+
+def test_digital_filter_initialization_matches_reference(pe_setup):
+  g, grid, _, eq = pe_setup
+  d = load('dfi_T21_L6.npz')
+  dt = float(d['dt'])
+  close(dycore.dfi_lanczos_weights(8 * dt, 8 * dt, dt), d['weights'], atol=0)
+  s = unpack(g, 'in')
+  rev = dycore.imex_rk_sil3(dycore.TimeReversedImExODE(eq), dt)(s)
+  assert_state_close(rev, unpack(d, 'reversed_step'), atol=1e-10)
+  dfi = dycore.digital_filter_initialization(
+      eq, dycore.imex_rk_sil3, [dycore.exponential_step_filter(grid, dt)],
+      8 * dt, 8 * dt, dt)
+  assert_state_close(dfi(s), unpack(d, 'dfi'), atol=1e-10)
