@@ -147,38 +147,94 @@ struct PrepArgs {
   float inv_radius;
 };
 
-__global__ void pe_prep_kernel(PrepArgs a) {
+// The modal-point geometry of (row, l), loaded once and reused for every
+// level: the d/dlon partner row and factor, and the cos_lat_d_dlat (tab 0) or
+// sec_lat_d_dlat_cos2 (tab 2) recurrence coefficients at l + 1 and l - 1
+// (optionally times a per-l scaling s, folded in).
+struct ModalNbr {
+  int row, l, L;
+  int dl_row;
+  float dl_fac;
+  float a1, b1;  // coefficients of x[l + 1] and x[l - 1] (0 when out of range)
+
+  __device__ ModalNbr(int row_, int l_, int L_, int lw, const float* deriv, int tab,
+                      const float* s)
+      : row(row_), l(l_), L(L_) {
+    const int m = (row + 1) >> 1;
+    if (row == 0) {
+      dl_row = 0;
+      dl_fac = 0.f;
+    } else if (row & 1) {
+      dl_row = row + 1;
+      dl_fac = (float)m;
+    } else {
+      dl_row = row - 1;
+      dl_fac = -(float)m;
+    }
+    const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
+    const float* tb = ta + (size_t)lw * L;
+    a1 = (l + 1 < L) ? ta[l + 1] * (s ? s[l + 1] : 1.f) : 0.f;
+    b1 = (l >= 1) ? tb[l - 1] * (s ? s[l - 1] : 1.f) : 0.f;
+  }
+  __device__ float dlon(const float* x) const {
+    return dl_fac * x[(size_t)dl_row * L + l];
+  }
+  __device__ float dlat(const float* x) const {
+    const float* xr = x + (size_t)row * L + l;
+    float v = 0.f;
+    if (l + 1 < L) v += a1 * xr[1];
+    if (l >= 1) v += b1 * xr[-1];
+    return v;
+  }
+};
+
+// Threads cover (row, l) with l fastest; each walks kPlanesPerThread of the
+// (member, level) planes, reusing its operator coefficients.
+constexpr int kModalTX = 32, kModalTY = 8, kPlanesPerThread = 8;
+
+__global__ void __launch_bounds__(kModalTX * kModalTY) pe_prep_kernel(PrepArgs a) {
+  const int l = blockIdx.x * kModalTX + threadIdx.x;
+  const int row = blockIdx.y * kModalTY + threadIdx.y;
+  if (l >= a.L || row >= a.M) return;
   const size_t ML = (size_t)a.M * a.L;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= ML) return;
-  const int l = idx % a.L, row = idx / a.L;
-  const int k = blockIdx.y;
-  const int mb = blockIdx.z;
-  {
+  const size_t idx = (size_t)row * a.L + l;
+  const float ir = a.inv_radius;
+  // u, v from vorticity / divergence through the inverse Laplacian (scaled
+  // coefficients); unscaled ones for the humidity and ln ps gradients.
+  const ModalNbr ns(row, l, a.L, a.lw, a.deriv, 0, a.invlap);
+  const ModalNbr nu(row, l, a.L, a.lw, a.deriv, 0, nullptr);
+  const float il = a.invlap[l];
+  const int q0 = blockIdx.z * kPlanesPerThread;
+  const int q1 = min(q0 + kPlanesPerThread, a.K * a.mem);
+  for (int q = q0; q < q1; ++q) {
+    const int mb = q / a.K, k = q - mb * a.K;
     const float* vort = a.state + pl(a.p_vort, mb, a.K, k) * ML;
     const float* div = a.state + pl(a.p_div, mb, a.K, k) * ML;
     // psi = lap^-1 vort, chi = lap^-1 div (l = 0 -> 0)
-    float dchi = d_dlon_at(div, row, l, a.L) * a.invlap[l];
-    float dpsi = d_dlon_at(vort, row, l, a.L) * a.invlap[l];
-    float cchi = dlat_at(div, a.invlap, row, l, a.L, a.lw, a.deriv, 0);
-    float cpsi = dlat_at(vort, a.invlap, row, l, a.L, a.lw, a.deriv, 0);
-    a.aux[pl(a.a_u, mb, a.K, k) * ML + idx] = (dchi - cpsi) * a.inv_radius;
-    a.aux[pl(a.a_v, mb, a.K, k) * ML + idx] = (cchi + dpsi) * a.inv_radius;
+    const float dchi = ns.dlon(div) * il;
+    const float dpsi = ns.dlon(vort) * il;
+    const float cchi = ns.dlat(div);
+    const float cpsi = ns.dlat(vort);
+    a.aux[pl(a.a_u, mb, a.K, k) * ML + idx] = (dchi - cpsi) * ir;
+    a.aux[pl(a.a_v, mb, a.K, k) * ML + idx] = (cchi + dpsi) * ir;
     if (a.hum >= 0) {
-      const float* q = a.state + pl(a.p_hum, mb, a.K, k) * ML;
-      a.aux[pl(a.a_gqx, mb, a.K, k) * ML + idx] =
-          d_dlon_at(q, row, l, a.L) * a.inv_radius;
-      a.aux[pl(a.a_gqy, mb, a.K, k) * ML + idx] =
-          dlat_at(q, nullptr, row, l, a.L, a.lw, a.deriv, 0) * a.inv_radius;
+      const float* qh = a.state + pl(a.p_hum, mb, a.K, k) * ML;
+      a.aux[pl(a.a_gqx, mb, a.K, k) * ML + idx] = nu.dlon(qh) * ir;
+      a.aux[pl(a.a_gqy, mb, a.K, k) * ML + idx] = nu.dlat(qh) * ir;
+    }
+    if (k == 0) {
+      const float* lnps = a.state + ((size_t)a.p_lnps + mb) * ML;
+      a.aux[((size_t)a.a_gx + mb) * ML + idx] = nu.dlon(lnps) * ir;
+      a.aux[((size_t)a.a_gy + mb) * ML + idx] = nu.dlat(lnps) * ir;
+      if (a.hum >= 0)
+        a.aux[((size_t)a.a_laplnps + mb) * ML + idx] = lnps[idx] * a.lap[l];
     }
   }
-  if (k != 0) return;
-  const float* lnps = a.state + ((size_t)a.p_lnps + mb) * ML;
-  a.aux[((size_t)a.a_gx + mb) * ML + idx] = d_dlon_at(lnps, row, l, a.L) * a.inv_radius;
-  a.aux[((size_t)a.a_gy + mb) * ML + idx] =
-      dlat_at(lnps, nullptr, row, l, a.L, a.lw, a.deriv, 0) * a.inv_radius;
-  if (a.hum >= 0)
-    a.aux[((size_t)a.a_laplnps + mb) * ML + idx] = lnps[idx] * a.lap[l];
+}
+
+static dim3 modal_grid(int M, int L, int planes) {
+  return dim3(ceil_div(L, kModalTX), ceil_div(M, kModalTY),
+              ceil_div(planes, kPlanesPerThread));
 }
 
 // ---------------------------------------------------------------------------
@@ -431,60 +487,56 @@ struct PostArgs {
   float inv_radius, gravity;
 };
 
-__global__ void pe_post_kernel(PostArgs a) {
+__global__ void __launch_bounds__(kModalTX * kModalTY) pe_post_kernel(PostArgs a) {
+  const int l = blockIdx.x * kModalTX + threadIdx.x;
+  const int row = blockIdx.y * kModalTY + threadIdx.y;
+  if (l >= a.L || row >= a.M) return;
   const size_t ML = (size_t)a.M * a.L;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= ML) return;
-  const int l = idx % a.L, row = idx / a.L;
-  const int k = blockIdx.y;
-  const int mb = blockIdx.z;
+  const size_t idx = (size_t)row * a.L + l;
   const int K = a.K;
   const bool clip = (l == a.L - 1);
   const float lam = a.lap[l];
-#define FM(p, k) (a.fm + pl(p, mb, K, k) * ML)
-#define OUT(p, k) a.tend[pl(p, mb, K, k) * ML + idx]
-  {
-    const float* Au = FM(a.o_Au, k);
-    const float* Av = FM(a.o_Av, k);
-    float vort = -(d_dlon_at(Av, row, l, a.L) -
-                   dlat_at(Au, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
-    float div = -(d_dlon_at(Au, row, l, a.L) +
-                  dlat_at(Av, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
-    div += -lam * FM(a.o_KE, k)[idx] - a.gravity * lam * a.orog[idx];
+  const float ir = a.inv_radius;
+  const float orog = a.gravity * lam * a.orog[idx];
+  const ModalNbr nb(row, l, a.L, a.lw, a.deriv, 2, nullptr);
+  const int q0 = blockIdx.z * kPlanesPerThread;
+  const int q1 = min(q0 + kPlanesPerThread, K * a.mem);
+  for (int q = q0; q < q1; ++q) {
+    const int mb = q / K, k = q - mb * K;
+#define FM(p) (a.fm + pl(p, mb, K, k) * ML)
+#define OUT(p) a.tend[pl(p, mb, K, k) * ML + idx]
+    const float* Au = FM(a.o_Au);
+    const float* Av = FM(a.o_Av);
+    float vort = -(nb.dlon(Av) - nb.dlat(Au)) * ir;
+    float div = -(nb.dlon(Au) + nb.dlat(Av)) * ir;
+    div += -lam * FM(a.o_KE)[idx] - orog;
     if (a.hum >= 0) {
-      vort += FM(a.o_vh, k)[idx];
-      div += -lam * FM(a.o_gh, k)[idx] - FM(a.o_dh, k)[idx];
+      vort += FM(a.o_vh)[idx];
+      div += -lam * FM(a.o_gh)[idx] - FM(a.o_dh)[idx];
     }
-    const float* uT = FM(a.o_uT, k);
-    const float* vT = FM(a.o_vT, k);
-    float temp = FM(a.o_Tn, k)[idx] -
-                 (d_dlon_at(uT, row, l, a.L) +
-                  dlat_at(vT, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
+    float temp = FM(a.o_Tn)[idx] - (nb.dlon(FM(a.o_uT)) + nb.dlat(FM(a.o_vT))) * ir;
     if (clip) {
       vort = 0.f;
       div = 0.f;
       temp = 0.f;
     }
-    if (a.hs) temp += FM(a.o_hsT, k)[idx];
-    OUT(a.p_vort, k) = vort;
-    OUT(a.p_div, k) = div;
-    OUT(a.p_temp, k) = temp;
+    if (a.hs) temp += FM(a.o_hsT)[idx];
+    OUT(a.p_vort) = vort;
+    OUT(a.p_div) = div;
+    OUT(a.p_temp) = temp;
     for (int t = 0; t < a.nT; ++t) {
       const int ob = a.o_tr + 3 * t * a.mem * K;
-      const float* uq = FM(ob, k);
-      const float* vq = FM(ob + a.mem * K, k);
-      float q = FM(ob + 2 * a.mem * K, k)[idx] -
-                (d_dlon_at(uq, row, l, a.L) +
-                 dlat_at(vq, nullptr, row, l, a.L, a.lw, a.deriv, 2)) * a.inv_radius;
-      OUT(a.p_tr + t * a.mem * K, k) = clip ? 0.f : q;
+      float qv = FM(ob + 2 * a.mem * K)[idx] -
+                 (nb.dlon(FM(ob)) + nb.dlat(FM(ob + a.mem * K))) * ir;
+      OUT(a.p_tr + t * a.mem * K) = clip ? 0.f : qv;
     }
-  }
-  if (k == 0) {
-    float lnps = a.fm[((size_t)a.o_lnps + mb) * ML + idx];
-    a.tend[((size_t)a.p_lnps + mb) * ML + idx] = clip ? 0.f : lnps;
-  }
+    if (k == 0) {
+      const float lnps = a.fm[((size_t)a.o_lnps + mb) * ML + idx];
+      a.tend[((size_t)a.p_lnps + mb) * ML + idx] = clip ? 0.f : lnps;
+    }
 #undef FM
 #undef OUT
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1519,8 +1571,7 @@ static int pe_nodal_inputs(dino_pe* pe, const float* state, cudaStream_t st) {
     a.lap = p->d_lap;
     a.invlap = p->d_invlap;
     a.inv_radius = (float)(1.0 / p->radius);
-    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
-    pe_prep_kernel<<<grid, 256, 0, st>>>(a);
+    pe_prep_kernel<<<modal_grid(pe->M, pe->L, K * mem), dim3(kModalTX, kModalTY), 0, st>>>(a);
     DINO_TRY(check_launch("pe_prep"));
   }
   // 2. inverse SHT of [state kinds][aux][ln ps (Held-Suarez)]
@@ -1657,8 +1708,7 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
     a.lap = p->d_lap;
     a.inv_radius = (float)(1.0 / p->radius);
     a.gravity = (float)pe->g;
-    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
-    pe_post_kernel<<<grid, 256, 0, st>>>(a);
+    pe_post_kernel<<<modal_grid(pe->M, pe->L, K * mem), dim3(kModalTX, kModalTY), 0, st>>>(a);
     DINO_TRY(check_launch("pe_post"));
   }
   return DINO_OK;
