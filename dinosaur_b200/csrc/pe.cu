@@ -563,51 +563,99 @@ struct PostAdjArgs {
   float inv_radius;
 };
 
-__global__ void pe_post_adjoint_kernel(PostAdjArgs a) {
+// Transposed operators at (row, l): d/dlon^T = -d/dlon, and
+// (D^T y)[l] = ta[l] y[l-1] + tb[l] y[l+1] with y taken as zero at l >= lclip
+// (the clipped top wavenumber of a tendency cotangent).
+struct ModalNbrT {
+  int row, l, L;
+  int dl_row;
+  float dl_fac;
+  float a0, b0;  // coefficients of y[l - 1] and y[l + 1] (0 when out of range)
+
+  __device__ ModalNbrT(int row_, int l_, int L_, int lw, const float* deriv, int tab,
+                       int lclip)
+      : row(row_), l(l_), L(L_) {
+    const int m = (row + 1) >> 1;
+    if (row == 0) {
+      dl_row = 0;
+      dl_fac = 0.f;
+    } else if (row & 1) {
+      dl_row = row + 1;
+      dl_fac = (float)m;
+    } else {
+      dl_row = row - 1;
+      dl_fac = -(float)m;
+    }
+    const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
+    const float* tb = ta + (size_t)lw * L;
+    a0 = (l >= 1 && l - 1 < lclip) ? ta[l] : 0.f;
+    b0 = (l + 1 < lclip) ? tb[l] : 0.f;
+  }
+  // d/dlon (the transpose is its negative).
+  __device__ float dlon(const float* x) const {
+    return dl_fac * x[(size_t)dl_row * L + l];
+  }
+  __device__ float dlat_t(const float* y) const {
+    const float* yr = y + (size_t)row * L + l;
+    float v = 0.f;
+    if (a0 != 0.f) v += a0 * yr[-1];
+    if (b0 != 0.f) v += b0 * yr[1];
+    return v;
+  }
+};
+
+__global__ void __launch_bounds__(kModalTX * kModalTY) pe_post_adjoint_kernel(PostAdjArgs a) {
+  const int l = blockIdx.x * kModalTX + threadIdx.x;
+  const int row = blockIdx.y * kModalTY + threadIdx.y;
+  if (l >= a.L || row >= a.M) return;
   const size_t ML = (size_t)a.M * a.L;
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= ML) return;
-  const int l = idx % a.L, row = idx / a.L;
-  const int k = blockIdx.y, mb = blockIdx.z, K = a.K;
+  const size_t idx = (size_t)row * a.L + l;
+  const int K = a.K;
   const int Lc = a.L - 1;
   const bool keep = l < Lc;
   const float ir = a.inv_radius;
   const float lam = a.lap[l];
+  const ModalNbrT nb(row, l, a.L, a.lw, a.deriv, 2, Lc);
+  const int q0 = blockIdx.z * kPlanesPerThread;
+  const int q1 = min(q0 + kPlanesPerThread, K * a.mem);
+  for (int q = q0; q < q1; ++q) {
+    const int mb = q / K, k = q - mb * K;
 #define TB(p) (a.tbar + pl(p, mb, K, k) * ML)
 #define FB(p) a.fbar[pl(p, mb, K, k) * ML + idx]
-  const float* vb = TB(a.p_vort);
-  const float* db = TB(a.p_div);
-  const float* Tb = TB(a.p_temp);
-  const float vc = keep ? vb[idx] : 0.f;
-  const float dc = keep ? db[idx] : 0.f;
-  const float Tc = keep ? Tb[idx] : 0.f;
-  const float dlon_v = keep ? d_dlon_at(vb, row, l, a.L) : 0.f;
-  const float dlon_d = keep ? d_dlon_at(db, row, l, a.L) : 0.f;
-  const float dlon_T = keep ? d_dlon_at(Tb, row, l, a.L) : 0.f;
-  FB(a.o_Au) = (dlat_t_at(vb, row, l, a.L, Lc, a.lw, a.deriv, 2) + dlon_d) * ir;
-  FB(a.o_Av) = (dlon_v - dlat_t_at(db, row, l, a.L, Lc, a.lw, a.deriv, 2)) * ir;
-  FB(a.o_KE) = -lam * dc;
-  if (a.hum >= 0) {
-    FB(a.o_vh) = vc;
-    FB(a.o_gh) = -lam * dc;
-    FB(a.o_dh) = -dc;
-  }
-  FB(a.o_Tn) = Tc;
-  FB(a.o_uT) = dlon_T * ir;
-  FB(a.o_vT) = -dlat_t_at(Tb, row, l, a.L, Lc, a.lw, a.deriv, 2) * ir;
-  if (a.hs) FB(a.o_hsT) = Tb[idx];
-  for (int t = 0; t < a.nT; ++t) {
-    const int ob = a.o_tr + 3 * t * a.mem * K;
-    const float* qb = TB(a.p_tr + t * a.mem * K);
-    FB(ob) = (keep ? d_dlon_at(qb, row, l, a.L) : 0.f) * ir;
-    FB(ob + a.mem * K) = -dlat_t_at(qb, row, l, a.L, Lc, a.lw, a.deriv, 2) * ir;
-    FB(ob + 2 * a.mem * K) = keep ? qb[idx] : 0.f;
-  }
-  if (k == 0)
-    a.fbar[((size_t)a.o_lnps + mb) * ML + idx] =
-        keep ? a.tbar[((size_t)a.p_lnps + mb) * ML + idx] : 0.f;
+    const float* vb = TB(a.p_vort);
+    const float* db = TB(a.p_div);
+    const float* Tb = TB(a.p_temp);
+    const float vc = keep ? vb[idx] : 0.f;
+    const float dc = keep ? db[idx] : 0.f;
+    const float Tc = keep ? Tb[idx] : 0.f;
+    const float dlon_v = keep ? nb.dlon(vb) : 0.f;
+    const float dlon_d = keep ? nb.dlon(db) : 0.f;
+    const float dlon_T = keep ? nb.dlon(Tb) : 0.f;
+    FB(a.o_Au) = (nb.dlat_t(vb) + dlon_d) * ir;
+    FB(a.o_Av) = (dlon_v - nb.dlat_t(db)) * ir;
+    FB(a.o_KE) = -lam * dc;
+    if (a.hum >= 0) {
+      FB(a.o_vh) = vc;
+      FB(a.o_gh) = -lam * dc;
+      FB(a.o_dh) = -dc;
+    }
+    FB(a.o_Tn) = Tc;
+    FB(a.o_uT) = dlon_T * ir;
+    FB(a.o_vT) = -nb.dlat_t(Tb) * ir;
+    if (a.hs) FB(a.o_hsT) = Tb[idx];
+    for (int t = 0; t < a.nT; ++t) {
+      const int ob = a.o_tr + 3 * t * a.mem * K;
+      const float* qb = TB(a.p_tr + t * a.mem * K);
+      FB(ob) = (keep ? nb.dlon(qb) : 0.f) * ir;
+      FB(ob + a.mem * K) = -nb.dlat_t(qb) * ir;
+      FB(ob + 2 * a.mem * K) = keep ? qb[idx] : 0.f;
+    }
+    if (k == 0)
+      a.fbar[((size_t)a.o_lnps + mb) * ML + idx] =
+          keep ? a.tbar[((size_t)a.p_lnps + mb) * ML + idx] : 0.f;
 #undef TB
 #undef FB
+  }
 }
 
 // VJP of pe_nodal_kernel for one column.  Pass 0 forms the column totals;
@@ -891,44 +939,48 @@ struct PrepAdjArgs {
   float inv_radius;
 };
 
-__global__ void pe_prep_adjoint_kernel(PrepAdjArgs a) {
+__global__ void __launch_bounds__(kModalTX * kModalTY) pe_prep_adjoint_kernel(PrepAdjArgs a) {
+  const int l = blockIdx.x * kModalTX + threadIdx.x;
+  const int row = blockIdx.y * kModalTY + threadIdx.y;
+  if (l >= a.L || row >= a.M) return;
   const size_t ML = (size_t)a.M * a.L;
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= ML) return;
-  const int l = idx % a.L, row = idx / a.L;
-  const int k = blockIdx.y, mb = blockIdx.z, K = a.K;
+  const size_t idx = (size_t)row * a.L + l;
+  const int K = a.K;
   const int mK = a.mem * K;
   const float ir = a.inv_radius;
-  const float* ub = a.xbar + pl(a.p_u, mb, K, k) * ML;
-  const float* vb = a.xbar + pl(a.p_v, mb, K, k) * ML;
   const float s = a.invlap[l] * ir;
-  const size_t pz = pl(0, mb, K, k) * ML + idx;
-  a.sbar[pz] = a.xbar[pz] + s * (-dlat_t_at(ub, row, l, a.L, a.L, a.lw, a.deriv, 0) -
-                                 d_dlon_at(vb, row, l, a.L));
-  const size_t pd = pl(mK, mb, K, k) * ML + idx;
-  a.sbar[pd] = a.xbar[pd] + s * (-d_dlon_at(ub, row, l, a.L) +
-                                 dlat_t_at(vb, row, l, a.L, a.L, a.lw, a.deriv, 0));
-  const size_t pt = pl(2 * mK, mb, K, k) * ML + idx;
-  a.sbar[pt] = a.xbar[pt];
-  for (int t = 0; t < a.nT; ++t) {
-    const size_t pq = pl((3 + t) * mK, mb, K, k) * ML + idx;
-    float v = a.xbar[pq];
-    if (t == a.hum) {
-      const float* gqxb = a.xbar + pl(a.p_gqx, mb, K, k) * ML;
-      const float* gqyb = a.xbar + pl(a.p_gqy, mb, K, k) * ML;
-      v += ir * (-d_dlon_at(gqxb, row, l, a.L) +
-                 dlat_t_at(gqyb, row, l, a.L, a.L, a.lw, a.deriv, 0));
+  const ModalNbrT nb(row, l, a.L, a.lw, a.deriv, 0, a.L);
+  const int q0 = blockIdx.z * kPlanesPerThread;
+  const int q1 = min(q0 + kPlanesPerThread, K * a.mem);
+  for (int q = q0; q < q1; ++q) {
+    const int mb = q / K, k = q - mb * K;
+    const float* ub = a.xbar + pl(a.p_u, mb, K, k) * ML;
+    const float* vb = a.xbar + pl(a.p_v, mb, K, k) * ML;
+    const size_t pz = pl(0, mb, K, k) * ML + idx;
+    a.sbar[pz] = a.xbar[pz] + s * (-nb.dlat_t(ub) - nb.dlon(vb));
+    const size_t pd = pl(mK, mb, K, k) * ML + idx;
+    a.sbar[pd] = a.xbar[pd] + s * (-nb.dlon(ub) + nb.dlat_t(vb));
+    const size_t pt = pl(2 * mK, mb, K, k) * ML + idx;
+    a.sbar[pt] = a.xbar[pt];
+    for (int t = 0; t < a.nT; ++t) {
+      const size_t pq = pl((3 + t) * mK, mb, K, k) * ML + idx;
+      float v = a.xbar[pq];
+      if (t == a.hum) {
+        const float* gqxb = a.xbar + pl(a.p_gqx, mb, K, k) * ML;
+        const float* gqyb = a.xbar + pl(a.p_gqy, mb, K, k) * ML;
+        v += ir * (-nb.dlon(gqxb) + nb.dlat_t(gqyb));
+      }
+      a.sbar[pq] = v;
     }
-    a.sbar[pq] = v;
+    if (k == 0) {
+      const float* gxb = a.xbar + ((size_t)a.p_gx + mb) * ML;
+      const float* gyb = a.xbar + ((size_t)a.p_gy + mb) * ML;
+      float v = a.hs ? a.xbar[((size_t)a.p_lnps + mb) * ML + idx] : 0.f;
+      v += ir * (-nb.dlon(gxb) + nb.dlat_t(gyb));
+      if (a.hum >= 0) v += a.lap[l] * a.xbar[((size_t)a.p_laplnps + mb) * ML + idx];
+      a.sbar[((size_t)a.s_lnps + mb) * ML + idx] = v;
+    }
   }
-  if (k != 0) return;
-  const float* gxb = a.xbar + ((size_t)a.p_gx + mb) * ML;
-  const float* gyb = a.xbar + ((size_t)a.p_gy + mb) * ML;
-  float v = a.hs ? a.xbar[((size_t)a.p_lnps + mb) * ML + idx] : 0.f;
-  v += ir * (-d_dlon_at(gxb, row, l, a.L) +
-             dlat_t_at(gyb, row, l, a.L, a.L, a.lw, a.deriv, 0));
-  if (a.hum >= 0) v += a.lap[l] * a.xbar[((size_t)a.p_laplnps + mb) * ML + idx];
-  a.sbar[((size_t)a.s_lnps + mb) * ML + idx] = v;
 }
 
 // out = sum_t c_t x_t over the packed state, with coefficients ci on the
@@ -1176,56 +1228,63 @@ __device__ __forceinline__ size_t stacked_plane(const LmArgs& a, int i, int mb) 
   return (size_t)a.p_lnps + mb;
 }
 
-// One 32 (columns) x 32 (l) tile of stacked plane k per CTA (256 threads).
+// One 32 (rows of one member) x 32 (l) tile of stacked plane k per CTA (256
+// threads): blockIdx.y enumerates (member, row tile), so a tile never spans
+// two members and the column c = member * M + row needs no division.
 __global__ void __launch_bounds__(256) pe_lm_gather_kernel(LmArgs a) {
   __shared__ float tile[32][33];
   const int k = blockIdx.z;
-  const int l0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int row_tiles = (a.M + 31) / 32;
+  const int mb = blockIdx.y / row_tiles;
+  const int row0 = (blockIdx.y - mb * row_tiles) * 32;
+  const int l0 = blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const bool first = k < a.n;
-  const float* base = first ? a.src : a.src2;
   const int kk = first ? k : k - a.n;
   const float sc = first ? a.s1 : a.s2;
+  const float* src = (first ? a.src : a.src2) + stacked_plane(a, kk, mb) * a.ML;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int cc = ty + 8 * i, c = c0 + cc, l = l0 + tx;
-    float v = 0.f;
-    if (c < a.C && l < a.L) {
-      const int mb = c / a.M, row = c - mb * a.M;
-      v = sc * base[stacked_plane(a, kk, mb) * a.ML + (size_t)row * a.L + l];
-    }
-    tile[cc][tx] = v;
+    const int rr = ty + 8 * i, row = row0 + rr, l = l0 + tx;
+    tile[rr][tx] = (row < a.M && l < a.L) ? sc * src[(size_t)row * a.L + l] : 0.f;
   }
   __syncthreads();
+  const int row = row0 + tx;
+  if (row >= a.M) return;
+  float* dst = a.lm + (size_t)k * a.Cp + (size_t)mb * a.M + row;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int ll = ty + 8 * i, l = l0 + ll, c = c0 + tx;
-    if (l < a.L) a.lm[((size_t)l * a.nk + k) * a.Cp + c] = tile[tx][ll];
+    const int ll = ty + 8 * i, l = l0 + ll;
+    if (l < a.L) dst[(size_t)l * a.nk * a.Cp] = tile[tx][ll];
   }
 }
 
 // Row r of the l-major product back into the state layout (rows [0, n) to
-// out, [n, 2n) to out2).
+// out, [n, 2n) to out2), tiled like the gather.
 __global__ void __launch_bounds__(256) pe_lm_scatter_kernel(LmArgs a) {
   __shared__ float tile[32][33];
   const int r = blockIdx.z;
-  const int l0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int row_tiles = (a.M + 31) / 32;
+  const int mb = blockIdx.y / row_tiles;
+  const int row0 = (blockIdx.y - mb * row_tiles) * 32;
+  const int l0 = blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  {
+    const int row = row0 + tx;
+    const float* srcp = a.lm + (size_t)r * a.Cp + (size_t)mb * a.M + row;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int ll = ty + 8 * i, l = l0 + ll, c = c0 + tx;
-    tile[ll][tx] = (l < a.L) ? a.lm[((size_t)l * a.nk + r) * a.Cp + c] : 0.f;
+    for (int i = 0; i < 4; ++i) {
+      const int ll = ty + 8 * i, l = l0 + ll;
+      tile[ll][tx] = (l < a.L && row < a.M) ? srcp[(size_t)l * a.nk * a.Cp] : 0.f;
+    }
   }
   __syncthreads();
-  float* dst = r < a.n ? a.out : a.out2;
-  const int rr = r < a.n ? r : r - a.n;
+  float* dst = (r < a.n ? a.out : a.out2) +
+               stacked_plane(a, r < a.n ? r : r - a.n, mb) * a.ML;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int cc = ty + 8 * i, c = c0 + cc, l = l0 + tx;
-    if (c < a.C && l < a.L) {
-      const int mb = c / a.M, row = c - mb * a.M;
-      dst[stacked_plane(a, rr, mb) * a.ML + (size_t)row * a.L + l] = tile[tx][cc];
-    }
+    const int rr = ty + 8 * i, row = row0 + rr, l = l0 + tx;
+    if (row < a.M && l < a.L) dst[(size_t)row * a.L + l] = tile[tx][rr];
   }
 }
 
@@ -1363,7 +1422,7 @@ static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
   g.p_temp = 2 * pe->mem * pe->K;
   g.p_lnps = (3 + pe->nT) * pe->mem * pe->K;
   g.ML = pe->ML;
-  const dim3 tiles(ceil_div(pe->L, 32), g.Cp / 32);
+  const dim3 tiles(ceil_div(pe->L, 32), ceil_div(pe->M, 32) * pe->mem);
   g.lm = pe->d_lm_in;
   g.nk = m->nin;
   pe_lm_gather_kernel<<<dim3(tiles.x, tiles.y, m->nin), 256, 0, st>>>(g);
@@ -1814,8 +1873,8 @@ static int pe_explicit_vjp_impl(dino_pe* pe, const float* state, const float* tb
     a.deriv = p->d_deriv;
     a.lap = p->d_lap;
     a.inv_radius = (float)(1.0 / p->radius);
-    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
-    pe_post_adjoint_kernel<<<grid, 256, 0, st>>>(a);
+    pe_post_adjoint_kernel<<<modal_grid(pe->M, pe->L, K * mem), dim3(kModalTX, kModalTY), 0,
+                             st>>>(a);
     DINO_TRY(check_launch("pe_post_adjoint"));
   }
   DINO_TRY(sht_forward_adjoint_to(p, pe->d_fwd_out, pe->d_fwd_in, pe->n_fwd,
@@ -1856,8 +1915,8 @@ static int pe_explicit_vjp_impl(dino_pe* pe, const float* state, const float* tb
     a.lap = p->d_lap;
     a.invlap = p->d_invlap;
     a.inv_radius = (float)(1.0 / p->radius);
-    dim3 grid(ceil_div((int)pe->ML, 256), K, mem);
-    pe_prep_adjoint_kernel<<<grid, 256, 0, st>>>(a);
+    pe_prep_adjoint_kernel<<<modal_grid(pe->M, pe->L, K * mem), dim3(kModalTX, kModalTY), 0,
+                             st>>>(a);
     DINO_TRY(check_launch("pe_prep_adjoint"));
   }
   return DINO_OK;
