@@ -670,7 +670,8 @@ struct NodalAdjArgs {
   float* xbar;        // cotangents of the nodal inputs (nodal-buffer layout)
 };
 
-__global__ void __launch_bounds__(128) pe_nodal_adjoint_kernel(NodalAdjArgs A) {
+// Five CTAs per SM (96 registers, no spills).
+__global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A) {
   const NodalArgs& a = A.f;
   const size_t IJ = (size_t)a.I * a.J;
   const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
