@@ -66,6 +66,8 @@ struct dino_pe {
   std::vector<double> dsig, c2c, alpha, tref, sumsig, sigma, G, H;
   // Device constants.
   float* d_lev = nullptr;   // per-level constants (see LevOff)
+  float* d_levpack = nullptr;  // the same, packed per level (kLevPack)
+  int sms = 148;               // multiprocessors of the device
   float* d_lat = nullptr;   // per-latitude constants: sec2, f, sin2, cos2
   float* d_orog = nullptr;  // modal orography [M][L]
   // Field bookkeeping (planes).
@@ -102,7 +104,8 @@ struct dino_pe {
 
 namespace dino {
 
-// Offsets into d_lev (floats); every array has K entries (c2ci has K-1).
+// Offsets into d_lev (floats); every array has K entries (c2ci and trefdiff
+// hold 0 at K - 1).
 struct LevOff {
   int dsig, c2ci, alpha, tref, sumsig, sigma, kv, trefdiff, logsp0;
   int total;
@@ -252,26 +255,76 @@ struct NodalArgs {
       o_lnps;
   const float* lev;
   LevOff lo;
+  const float* levpack;  // [K][kLevPack] (pe_nodal_kernel)
   const float* lat;  // [4][J]: sec2, coriolis, sin^2, cos^2
   float R, kappa, Rv_over_R, Cpv_over_Cp, Rv_minus_R;
   float hs_p0, hs_ka, hs_ks, hs_sigma_b, hs_minT, hs_maxT, hs_dTy, hs_dThz;
 };
 
-__global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
-  const size_t IJ = (size_t)a.I * a.J;
-  const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= IJ) return;
-  const int mb = blockIdx.y;
+// Packed per-level coefficients (16 floats, four float4 per level):
+//   0 dsig, 1 1/dsig, 2 sumsig, 3 tref,
+//   4 c2ci (0 at K-1), 5 c2ci[k-1] (0 at 0), 6 alpha, 7 alpha[k-1] (0 at 0),
+//   8 Rayleigh kv, 9 Held-Suarez cutoff, 10 (sigma/p0)^kappa, 11 log(sigma/p0),
+//   12 trefdiff (0 at K-1), 13 trefdiff[k-1] (0 at 0), 14-15 unused.
+constexpr int kLevPack = 16;
+
+template <int V>
+__device__ __forceinline__ void ld_vec(float (&x)[V], const float* p) {
+  static_assert(V == 1 || V == 2, "one or two columns per thread");
+  if constexpr (V == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    x[0] = t.x; x[1] = t.y;
+  } else {
+    x[0] = *p;
+  }
+}
+
+template <int V>
+__device__ __forceinline__ void st_vec(float* p, const float (&x)[V]) {
+  if constexpr (V == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(x[0], x[1]);
+  } else {
+    *p = x[0];
+  }
+}
+
+// One thread per (V adjacent columns, chunk of levels): blockDim =
+// (kNodalCols, C), chunk c holding levels [c K / C, (c + 1) K / C).  The
+// column totals and the prefix sums that sigma-dot needs come from per-chunk
+// partial sums exchanged through shared memory, so a thread walks K / C
+// levels.  A chunk's running sums are its partial sum formed in the same
+// order, so the sigma-dot of a half level shared by two chunks is the same in
+// both.  V columns share each address computation and level coefficient (the
+// latitude count J is a multiple of V, so they lie on one meridian).
+// kTracers = false compiles out the tracer windows (dry states).
+constexpr int kNodalCols = 32, kNodalMaxChunks = 4;
+
+template <bool kTracers, int V>
+__global__ void __launch_bounds__(kNodalCols * kNodalMaxChunks)
+    pe_nodal_kernel(NodalArgs a) {
+  extern __shared__ float4 s_lev[];  // [K][kLevPack / 4]
+  __shared__ float s_e[kNodalMaxChunks][kNodalCols * V];
+  __shared__ float s_f[kNodalMaxChunks][kNodalCols * V];
+  __shared__ float s_g[kTracers ? kNodalMaxChunks : 1][kNodalCols * V];
+  const int tx = threadIdx.x, c = threadIdx.y, C = blockDim.y;
   const int K = a.K;
-  const int j = col % a.J;
-  const float sec2 = a.lat[j];
-  const float fcor = a.lat[a.J + j];
-  const float* dsig = a.lev + a.lo.dsig;
-  const float* c2ci = a.lev + a.lo.c2ci;
-  const float* alpha = a.lev + a.lo.alpha;
-  const float* tref = a.lev + a.lo.tref;
-  const float* sumsig = a.lev + a.lo.sumsig;
-  // Level-0 pointers of this column for each kind; level k is at [k * IJ].
+  for (int i = c * kNodalCols + tx; i < K * (kLevPack / 4); i += kNodalCols * C)
+    s_lev[i] = reinterpret_cast<const float4*>(a.levpack)[i];
+  __syncthreads();
+  // Offsets within one kind's planes are 32-bit (K * I * J < 2^31, checked
+  // on the host); tracer kinds stay 64-bit apart.
+  const unsigned IJ = (unsigned)a.I * (unsigned)a.J;
+  const unsigned col = (blockIdx.x * kNodalCols + tx) * V;
+  const bool active = col < IJ;
+  const int mb = blockIdx.y;
+  const int k0 = (c * K) / C, k1 = ((c + 1) * K) / C;
+  const int nT = kTracers ? a.nT : 0;
+  const int hum = kTracers ? a.hum : -1;
+  const int j = active ? (int)(col % (unsigned)a.J) : 0;
+  float sec2[V], fcor[V];
+  ld_vec(sec2, a.lat + j);
+  ld_vec(fcor, a.lat + a.J + j);
+  // Level-0 pointers of these columns for each kind; level k is at [k * IJ].
   auto in = [&](int p) { return a.nod + pl(p, mb, K, 0) * IJ + col; };
   auto out = [&](int p) { return a.fwd + pl(p, mb, K, 0) * IJ + col; };
   const float* Pu = in(a.p_u);
@@ -279,34 +332,97 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
   const float* Pd = in(a.p_div);
   const float* Pz = in(a.p_vort);
   const float* PT = in(a.p_temp);
-  const float gx = a.nod[((size_t)a.p_gx + mb) * IJ + col];
-  const float gy = a.nod[((size_t)a.p_gy + mb) * IJ + col];
   // Tracer planes are a.mem * K apart.
   const size_t tstride = (size_t)a.mem * K * IJ;
   const float* Pq = in(a.p_tr);
+  const float* Ph = Pq + (hum >= 0 ? hum : 0) * tstride;
+  const float rv1 = a.Rv_over_R - 1.f;
+  float gx[V], gy[V];
 
-  // Pass 1: column totals of u.grad(ln ps) and of (div + u.grad ln ps), both
-  // weighted by the layer thickness (cumulative_sigma_integral, last level).
-  float Fe = 0.f, Ff = 0.f;
-  for (int k = 0; k < K; ++k) {
-    const size_t o = (size_t)k * IJ;
-    const float ugl = (Pu[o] * gx + Pv[o] * gy) * sec2;
-    Fe += ugl * dsig[k];
-    Ff += (Pd[o] + ugl) * dsig[k];
+  // Pass 1: this chunk's share of the column totals of u.grad(ln ps) and of
+  // (div + u.grad ln ps), both weighted by the layer thickness
+  // (cumulative_sigma_integral, last level), and (moist) of the geopotential
+  // suffix sum of the virtual-temperature difference.
+  float pe_[V], pf_[V], pg_[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) pe_[i] = pf_[i] = pg_[i] = 0.f;
+  if (active) {
+    ld_vec(gx, a.nod + ((size_t)a.p_gx + mb) * IJ + col);
+    ld_vec(gy, a.nod + ((size_t)a.p_gy + mb) * IJ + col);
+    for (int k = k0; k < k1; ++k) {
+      const unsigned o = (unsigned)k * IJ;
+      const float ds = s_lev[4 * k].x;
+      float u[V], v[V], d[V];
+      ld_vec(u, Pu + o);
+      ld_vec(v, Pv + o);
+      ld_vec(d, Pd + o);
+#pragma unroll
+      for (int i = 0; i < V; ++i) {
+        const float ugl = (u[i] * gx[i] + v[i] * gy[i]) * sec2[i];
+        pe_[i] += ugl * ds;
+        pf_[i] += (d[i] + ugl) * ds;
+      }
+    }
+    if (hum >= 0) {
+      for (int k = max(k0, 1); k < k1; ++k) {
+        const unsigned o = (unsigned)k * IJ;
+        const float4 c1 = s_lev[4 * k + 1];
+        const float tr = s_lev[4 * k].w;
+        float h[V], T[V];
+        ld_vec(h, Ph + o);
+        ld_vec(T, PT + o);
+#pragma unroll
+        for (int i = 0; i < V; ++i) pg_[i] += (c1.z + c1.w) * (h[i] * (T[i] + tr) * rv1);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < V; ++i) {
+    s_e[c][tx * V + i] = pe_[i];
+    s_f[c][tx * V + i] = pf_[i];
+    if (kTracers) s_g[c][tx * V + i] = pg_[i];
+  }
+  __syncthreads();
+  if (!active) return;
+  float Fe[V], Ff[V], pre_e[V], pre_f[V];
+#pragma unroll
+  for (int i = 0; i < V; ++i) {
+    Fe[i] = Ff[i] = pre_e[i] = pre_f[i] = 0.f;
+    for (int cc = 0; cc < C; ++cc) {
+      if (cc == c) {
+        pre_e[i] = Fe[i];
+        pre_f[i] = Ff[i];
+      }
+      Fe[i] += s_e[cc][tx * V + i];
+      Ff[i] += s_f[cc][tx * V + i];
+    }
   }
 
   // Moist: geopotential of the virtual-temperature difference, G @ td with
   // G[k][h] = R alpha_k (h = k), R (alpha_h + alpha_{h-1}) (h > k): a suffix
   // sum evaluated bottom-up (get_geopotential_weights_sigma, :306-338).
-  if (a.hum >= 0) {
-    float suffix = 0.f;
-    const float* Ph = Pq + a.hum * tstride;
+  if (hum >= 0) {
+    float suffix[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      suffix[i] = 0.f;
+      for (int cc = C - 1; cc > c; --cc) suffix[i] += s_g[cc][tx * V + i];
+    }
     float* Ogh = out(a.o_gh);
-    for (int k = K - 1; k >= 0; --k) {
-      const size_t o = (size_t)k * IJ;
-      const float td = Ph[o] * (PT[o] + tref[k]) * (a.Rv_over_R - 1.f);
-      Ogh[o] = a.R * (alpha[k] * td + suffix);
-      if (k > 0) suffix += (alpha[k] + alpha[k - 1]) * td;
+    for (int k = k1 - 1; k >= k0; --k) {
+      const unsigned o = (unsigned)k * IJ;
+      const float4 c1 = s_lev[4 * k + 1];
+      const float tr = s_lev[4 * k].w;
+      float h[V], T[V], g[V];
+      ld_vec(h, Ph + o);
+      ld_vec(T, PT + o);
+#pragma unroll
+      for (int i = 0; i < V; ++i) {
+        const float td = h[i] * (T[i] + tr) * rv1;
+        g[i] = a.R * (c1.z * td + suffix[i]);
+        suffix[i] += (c1.z + c1.w) * td;
+      }
+      st_vec(Ogh + o, g);
     }
   }
 
@@ -317,155 +433,224 @@ __global__ void __launch_bounds__(128) pe_nodal_kernel(NodalArgs a) {
   float* OvT = out(a.o_vT);
   float* OTn = out(a.o_Tn);
   float* Otr = out(a.o_tr);
-  // Pass 2: everything else, streaming over levels top-down with a window
-  // of (k-1, k, k+1) for the vertically advected fields.
-  float u_p = 0.f, v_p = 0.f, T_p = 0.f;
-  float u_c = Pu[0], v_c = Pv[0], T_c = PT[0];
-  float q_p[kMaxTracers], q_c[kMaxTracers], q_n[kMaxTracers];
-#pragma unroll
-  for (int t = 0; t < kMaxTracers; ++t) {
-    q_p[t] = 0.f;
-    q_c[t] = (t < a.nT) ? Pq[t * tstride] : 0.f;
-    q_n[t] = 0.f;
-  }
-  float fe = 0.f, ff = 0.f, fe_prev = 0.f, ff_prev = 0.f;
-  float sd_up_f = 0.f, sd_up_e = 0.f;  // sigma-dot at k - 1/2
-  float lnps_n = 0.f, sin2 = 0.f, cos2 = 0.f;
+  // Per-column Held-Suarez factors: T_eq = max(T_min, (sigma/p0)^kappa
+  // ps^kappa (A0 - B0 log(sigma/p0))) and k_T = k_a + (k_s - k_a) cutoff cos^4.
+  float hs_e[V], hs_A0[V], hs_B0[V], hs_dk[V];
   if (a.hs) {
-    lnps_n = a.nod[((size_t)a.p_lnps + mb) * IJ + col];
-    sin2 = a.lat[2 * a.J + j];
-    cos2 = a.lat[3 * a.J + j];
-  }
-  float laplnps = 0.f;
-  if (a.hum >= 0) laplnps = a.nod[((size_t)a.p_laplnps + mb) * IJ + col];
-
-  for (int k = 0; k < K; ++k) {
-    const size_t o = (size_t)k * IJ;
-    const bool has_next = k + 1 < K;
-    float u_n = 0.f, v_n = 0.f, T_n = 0.f;
-    if (has_next) {
-      u_n = Pu[o + IJ];
-      v_n = Pv[o + IJ];
-      T_n = PT[o + IJ];
-    }
+    float lnps_n[V], sin2[V], cos2[V];
+    ld_vec(lnps_n, a.nod + ((size_t)a.p_lnps + mb) * IJ + col);
+    ld_vec(sin2, a.lat + 2 * a.J + j);
+    ld_vec(cos2, a.lat + 3 * a.J + j);
 #pragma unroll
-    for (int t = 0; t < kMaxTracers; ++t)
-      if (t < a.nT) q_n[t] = has_next ? Pq[t * tstride + o + IJ] : 0.f;
-    const float zeta = Pz[o];
-    const float div = Pd[o];
-    const float ugl = (u_c * gx + v_c * gy) * sec2;
-    fe += ugl * dsig[k];
-    ff += (div + ugl) * dsig[k];
-    float sd_dn_f = 0.f, sd_dn_e = 0.f;  // sigma-dot at k + 1/2
-    if (has_next) {
-      sd_dn_f = sumsig[k] * Ff - ff;
-      sd_dn_e = sumsig[k] * Fe - fe;
+    for (int i = 0; i < V; ++i) {
+      hs_e[i] = expf(a.kappa * lnps_n[i]);
+      hs_A0[i] = a.hs_maxT - a.hs_dTy * sin2[i] - a.hs_dThz * lnps_n[i] * cos2[i];
+      hs_B0[i] = a.hs_dThz * cos2[i];
+      hs_dk[i] = (a.hs_ks - a.hs_ka) * (cos2[i] * cos2[i]);
     }
-    const float ci_dn = has_next ? c2ci[k] : 0.f;
-    const float ci_up = (k > 0) ? c2ci[k - 1] : 0.f;
-    // centered_vertical_advection(w, x)[k] = -0.5 (w_{k+1/2} dx_{k+1/2} +
-    // w_{k-1/2} dx_{k-1/2}) (sigma_coordinates.py:344-405).
-    auto vadv = [&](float xp, float xc, float xn, float wdn, float wup) {
-      float pd = has_next ? wdn * ((xn - xc) * ci_dn) : 0.f;
-      float pu = (k > 0) ? wup * ((xc - xp) * ci_up) : 0.f;
-      return -0.5f * (pd + pu);
-    };
-    float q_h = 0.f;
-    if (a.hum >= 0) {
+  }
+  float laplnps[V];
+  if (hum >= 0) ld_vec(laplnps, a.nod + ((size_t)a.p_laplnps + mb) * IJ + col);
+
+  // Pass 2: everything else, streaming over the chunk's levels top-down with
+  // a window of (k-1, k, k+1) for the vertically advected fields.  The level
+  // coefficients hold zero for the half levels outside the column, and the
+  // window reads level K-1 again in place of a level K, so the boundary terms
+  // vanish without branches.
+  const unsigned o0 = (unsigned)k0 * IJ;
+  const unsigned om = k0 > 0 ? o0 - IJ : o0;
+  float u_p[V], v_p[V], T_p[V], u_c[V], v_c[V], T_c[V];
+  ld_vec(u_p, Pu + om);
+  ld_vec(v_p, Pv + om);
+  ld_vec(T_p, PT + om);
+  ld_vec(u_c, Pu + o0);
+  ld_vec(v_c, Pv + o0);
+  ld_vec(T_c, PT + o0);
+  float q_p[kTracers ? kMaxTracers : 1][V], q_c[kTracers ? kMaxTracers : 1][V];
+  if (kTracers) {
+#pragma unroll
+    for (int t = 0; t < kMaxTracers; ++t) {
+      if (t < nT) {
+        ld_vec(q_p[t], Pq + t * tstride + om);
+        ld_vec(q_c[t], Pq + t * tstride + o0);
+      }
+    }
+  }
+  // Prefix sums through level k (fe, ff) and k - 1 (fe_prev, ff_prev).
+  float loc_e[V], loc_f[V], fe_prev[V], ff_prev[V], sd_up_f[V], sd_up_e[V];
+  {
+    const float ssu = k0 > 0 ? s_lev[4 * (k0 - 1)].z : 0.f;
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      loc_e[i] = loc_f[i] = 0.f;
+      fe_prev[i] = pre_e[i];
+      ff_prev[i] = pre_f[i];
+      // sigma-dot at k0 - 1/2 (0 at the top)
+      sd_up_f[i] = k0 > 0 ? ssu * Ff[i] - pre_f[i] : 0.f;
+      sd_up_e[i] = k0 > 0 ? ssu * Fe[i] - pre_e[i] : 0.f;
+    }
+  }
+
+  for (int k = k0; k < k1; ++k) {
+    const unsigned o = (unsigned)k * IJ;
+    const unsigned on = (k + 1 < K) ? o + IJ : o;
+    const float4 c0 = s_lev[4 * k], c1 = s_lev[4 * k + 1];
+    const float4 c2 = s_lev[4 * k + 2], c3 = s_lev[4 * k + 3];
+    const float ds = c0.x, inv_ds = c0.y, ss = c0.z, tr = c0.w;
+    const float ci_dn = c1.x, ci_up = c1.y, al = c1.z, al_up = c1.w;
+    float u_n[V], v_n[V], T_n[V], zeta[V], div[V];
+    ld_vec(u_n, Pu + on);
+    ld_vec(v_n, Pv + on);
+    ld_vec(T_n, PT + on);
+    ld_vec(zeta, Pz + o);
+    ld_vec(div, Pd + o);
+    float q_n[kTracers ? kMaxTracers : 1][V];
+    if (kTracers) {
 #pragma unroll
       for (int t = 0; t < kMaxTracers; ++t)
-        if (t == a.hum) q_h = q_c[t];
+        if (t < nT) ld_vec(q_n[t], Pq + t * tstride + on);
     }
-    // curl_and_div_tendencies (:1001-1059)
-    const float adj = (a.hum >= 0) ? 1.f + (a.Rv_over_R - 1.f) * q_h : 1.f;
-    const float rt = a.R * T_c * adj;
-    float sdu = 0.f, sdv = 0.f;
-    if (a.vadv) {
-      sdu = -vadv(u_p, u_c, u_n, sd_dn_f, sd_up_f);
-      sdv = -vadv(v_p, v_c, v_n, sd_dn_f, sd_up_f);
+    float gqx[V], gqy[V];
+    if (hum >= 0) {
+      ld_vec(gqx, a.nod + pl(a.p_gqx, mb, K, 0) * IJ + col + o);
+      ld_vec(gqy, a.nod + pl(a.p_gqy, mb, K, 0) * IJ + col + o);
     }
-    const float tv = zeta + fcor;
-    float Au = -v_c * tv * sec2 + (sdu + rt * gx) * sec2;
-    float Av = u_c * tv * sec2 + (sdv + rt * gy) * sec2;
-    if (a.hs) {
-      // Rayleigh drag folded in: curl/div of -(-kv u / cos^2).
-      const float kv = a.lev[a.lo.kv + k];
-      Au += kv * u_c * sec2;
-      Av += kv * v_c * sec2;
-    }
-    OAu[o] = Au;
-    OAv[o] = Av;
-    OKE[o] = (u_c * u_c + v_c * v_c) * sec2 * 0.5f;
-    OuT[o] = u_c * T_c * sec2;
-    OvT[o] = v_c * T_c * sec2;
-    // Temperature: horizontal nodal term, vertical advection, adiabatic.
-    float Tn = T_c * div;
-    if (a.vadv) Tn += vadv(T_p, T_c, T_n, sd_dn_f, sd_up_f);
-    if (a.tref_varies) {
-      const float* trd = a.lev + a.lo.trefdiff;
-      float pd = has_next ? sd_dn_e * trd[k] : 0.f;
-      float pu = (k > 0) ? sd_up_e * trd[k - 1] : 0.f;
-      Tn += -0.5f * (pd + pu);
-    }
-    const float inv_ds = 1.f / dsig[k];
-    const float ge = (alpha[k] * fe + (k > 0 ? alpha[k - 1] * fe_prev : 0.f)) * inv_ds;
-    const float gf = (alpha[k] * ff + (k > 0 ? alpha[k - 1] * ff_prev : 0.f)) * inv_ds;
-    const float mean_part = tref[k] * (ugl - ge);
-    float var_part;
-    if (a.hum < 0) {
-      var_part = T_c * (ugl - gf);
-    } else {
-      const float den = 1.f + (a.Cpv_over_Cp - 1.f) * q_h;
-      const float tv_var = T_c * ((1.f + (a.Rv_over_R - 1.f) * q_h) / den);
-      const float tv_ref = tref[k] * (((a.Rv_over_R - a.Cpv_over_Cp) * q_h) / den);
-      var_part = (tv_var + tv_ref) * (ugl - gf);
-    }
-    Tn += a.kappa * (mean_part + var_part);
-    OTn[o] = Tn;
-    // Tracers: u q, v q (times sec^2) and q div + vertical advection.
+    float rAu[V], rAv[V], rKE[V], ruT[V], rvT[V], rTn[V], rhs[V], rvh[V], rdh[V];
+    float sdn_f[V], sdn_e[V];
 #pragma unroll
-    for (int t = 0; t < kMaxTracers; ++t) {
-      if (t >= a.nT) break;
-      float* ob = Otr + 3 * t * tstride;
-      ob[o] = u_c * q_c[t] * sec2;
-      ob[tstride + o] = v_c * q_c[t] * sec2;
-      float qn = q_c[t] * div;
-      if (a.vadv) qn += vadv(q_p[t], q_c[t], q_n[t], sd_dn_f, sd_up_f);
-      ob[2 * tstride + o] = qn;
+    for (int i = 0; i < V; ++i) {
+      const float ugl = (u_c[i] * gx[i] + v_c[i] * gy[i]) * sec2[i];
+      loc_e[i] += ugl * ds;
+      loc_f[i] += (div[i] + ugl) * ds;
+      const float fe = pre_e[i] + loc_e[i];
+      const float ff = pre_f[i] + loc_f[i];
+      const float sd_dn_f = ss * Ff[i] - ff;  // sigma-dot at k + 1/2
+      const float sd_dn_e = ss * Fe[i] - fe;
+      sdn_f[i] = sd_dn_f;
+      sdn_e[i] = sd_dn_e;
+      // centered_vertical_advection(w, x)[k] = -0.5 (w_{k+1/2} dx_{k+1/2} +
+      // w_{k-1/2} dx_{k-1/2}) (sigma_coordinates.py:344-405).
+      auto vadv = [&](float xp, float xc, float xn) {
+        return -0.5f * (sd_dn_f * ((xn - xc) * ci_dn) + sd_up_f[i] * ((xc - xp) * ci_up));
+      };
+      float q_h = 0.f;
+      if (kTracers && hum >= 0) {
+#pragma unroll
+        for (int t = 0; t < kMaxTracers; ++t)
+          if (t == hum) q_h = q_c[t][i];
+      }
+      // curl_and_div_tendencies (:1001-1059)
+      const float adj = (hum >= 0) ? 1.f + rv1 * q_h : 1.f;
+      const float rt = a.R * T_c[i] * adj;
+      float sdu = 0.f, sdv = 0.f;
+      if (a.vadv) {
+        sdu = -vadv(u_p[i], u_c[i], u_n[i]);
+        sdv = -vadv(v_p[i], v_c[i], v_n[i]);
+      }
+      const float tv = zeta[i] + fcor[i];
+      float Au = -v_c[i] * tv * sec2[i] + (sdu + rt * gx[i]) * sec2[i];
+      float Av = u_c[i] * tv * sec2[i] + (sdv + rt * gy[i]) * sec2[i];
+      if (a.hs) {
+        // Rayleigh drag folded in: curl/div of -(-kv u / cos^2).
+        Au += c2.x * u_c[i] * sec2[i];
+        Av += c2.x * v_c[i] * sec2[i];
+      }
+      rAu[i] = Au;
+      rAv[i] = Av;
+      rKE[i] = (u_c[i] * u_c[i] + v_c[i] * v_c[i]) * sec2[i] * 0.5f;
+      ruT[i] = u_c[i] * T_c[i] * sec2[i];
+      rvT[i] = v_c[i] * T_c[i] * sec2[i];
+      // Temperature: horizontal nodal term, vertical advection, adiabatic.
+      float Tn = T_c[i] * div[i];
+      if (a.vadv) Tn += vadv(T_p[i], T_c[i], T_n[i]);
+      if (a.tref_varies) Tn += -0.5f * (sd_dn_e * c3.x + sd_up_e[i] * c3.y);
+      const float ge = (al * fe + al_up * fe_prev[i]) * inv_ds;
+      const float gf = (al * ff + al_up * ff_prev[i]) * inv_ds;
+      const float mean_part = tr * (ugl - ge);
+      float var_part;
+      if (hum < 0) {
+        var_part = T_c[i] * (ugl - gf);
+      } else {
+        const float den = 1.f + (a.Cpv_over_Cp - 1.f) * q_h;
+        const float tv_var = T_c[i] * ((1.f + rv1 * q_h) / den);
+        const float tv_ref = tr * (((a.Rv_over_R - a.Cpv_over_Cp) * q_h) / den);
+        var_part = (tv_var + tv_ref) * (ugl - gf);
+      }
+      rTn[i] = Tn + a.kappa * (mean_part + var_part);
+      if (hum >= 0) {
+        const float coef = tr * a.Rv_minus_R;
+        rvh[i] = coef * sec2[i] * (gx[i] * gqy[i] - gy[i] * gqx[i]);
+        rdh[i] = coef * sec2[i] * (gqx[i] * gx[i] + gqy[i] * gy[i]) +
+                 q_h * laplnps[i] * tr * a.Rv_minus_R;
+      }
+      if (a.hs) {
+        // held_suarez.py:105-120, :138-151, with log(p / p0) = log(sigma / p0)
+        // + ln ps, so (p / p0)^kappa = (sigma / p0)^kappa ps^kappa.
+        const float kt = a.hs_ka + hs_dk[i] * c2.y;
+        float teq = c2.z * hs_e[i] * (hs_A0[i] - hs_B0[i] * c2.w);
+        teq = fmaxf(a.hs_minT, teq);
+        rhs[i] = -kt * (tr + T_c[i] - teq);
+      }
+      fe_prev[i] = fe;
+      ff_prev[i] = ff;
     }
-    if (a.hum >= 0) {
-      const float gqx = a.nod[pl(a.p_gqx, mb, K, k) * IJ + col];
-      const float gqy = a.nod[pl(a.p_gqy, mb, K, k) * IJ + col];
-      const float coef = tref[k] * a.Rv_minus_R;
-      a.fwd[pl(a.o_vh, mb, K, k) * IJ + col] = coef * sec2 * (gx * gqy - gy * gqx);
-      a.fwd[pl(a.o_dh, mb, K, k) * IJ + col] =
-          coef * sec2 * (gqx * gx + gqy * gy) + q_h * laplnps * tref[k] * a.Rv_minus_R;
+    st_vec(OAu + o, rAu);
+    st_vec(OAv + o, rAv);
+    st_vec(OKE + o, rKE);
+    st_vec(OuT + o, ruT);
+    st_vec(OvT + o, rvT);
+    st_vec(OTn + o, rTn);
+    if (hum >= 0) {
+      st_vec(a.fwd + pl(a.o_vh, mb, K, 0) * IJ + col + o, rvh);
+      st_vec(a.fwd + pl(a.o_dh, mb, K, 0) * IJ + col + o, rdh);
     }
-    if (a.hs) {
-      // held_suarez.py:105-120, :138-151, with log(p / p0) = log(sigma / p0)
-      // + ln ps and (p / p0)^kappa = exp(kappa log(p / p0)).
-      const float sig = a.lev[a.lo.sigma + k];
-      const float cutoff = fmaxf(0.f, (sig - a.hs_sigma_b) / (1.f - a.hs_sigma_b));
-      const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (cutoff * cos2 * cos2);
-      const float lp = a.lev[a.lo.logsp0 + k] + lnps_n;
-      float teq = expf(a.kappa * lp) * (a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * lp * cos2);
-      teq = fmaxf(a.hs_minT, teq);
-      a.fwd[pl(a.o_hsT, mb, K, k) * IJ + col] = -kt * (tref[k] + T_c - teq);
+    if (a.hs) st_vec(a.fwd + pl(a.o_hsT, mb, K, 0) * IJ + col + o, rhs);
+    // Tracers: u q, v q (times sec^2) and q div + vertical advection.
+    if (kTracers) {
+#pragma unroll
+      for (int t = 0; t < kMaxTracers; ++t) {
+        if (t >= nT) break;
+        float* ob = Otr + 3 * t * tstride;
+        float fu[V], fv[V], fq[V];
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+          fu[i] = u_c[i] * q_c[t][i] * sec2[i];
+          fv[i] = v_c[i] * q_c[t][i] * sec2[i];
+          float qn = q_c[t][i] * div[i];
+          if (a.vadv)
+            qn += -0.5f * (sdn_f[i] * ((q_n[t][i] - q_c[t][i]) * ci_dn) +
+                           sd_up_f[i] * ((q_c[t][i] - q_p[t][i]) * ci_up));
+          fq[i] = qn;
+        }
+        st_vec(ob + o, fu);
+        st_vec(ob + tstride + o, fv);
+        st_vec(ob + 2 * tstride + o, fq);
+      }
     }
     // Advance the window.
-    fe_prev = fe;
-    ff_prev = ff;
-    sd_up_f = sd_dn_f;
-    sd_up_e = sd_dn_e;
-    u_p = u_c; v_p = v_c; T_p = T_c;
-    u_c = u_n; v_c = v_n; T_c = T_n;
 #pragma unroll
-    for (int t = 0; t < kMaxTracers; ++t) {
-      q_p[t] = q_c[t];
-      q_c[t] = q_n[t];
+    for (int i = 0; i < V; ++i) {
+      sd_up_f[i] = sdn_f[i];
+      sd_up_e[i] = sdn_e[i];
+      u_p[i] = u_c[i]; v_p[i] = v_c[i]; T_p[i] = T_c[i];
+      u_c[i] = u_n[i]; v_c[i] = v_n[i]; T_c[i] = T_n[i];
+    }
+    if (kTracers) {
+#pragma unroll
+      for (int t = 0; t < kMaxTracers; ++t)
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+          q_p[t][i] = q_c[t][i];
+          q_c[t][i] = q_n[t][i];
+        }
     }
   }
-  a.fwd[((size_t)a.o_lnps + mb) * IJ + col] = -Fe;
+  if (c == 0) {
+    float l[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) l[i] = -Fe[i];
+    st_vec(a.fwd + ((size_t)a.o_lnps + mb) * IJ + col, l);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1657,6 +1842,55 @@ static int pe_nodal_inputs(dino_pe* pe, const float* state, cudaStream_t st) {
   return DINO_OK;
 }
 
+// Level chunks per column for pe_nodal_kernel: the fewest (1, 2 or 4) that
+// give about two waves of 16 warps per SM, keeping four or more levels a chunk.
+static int nodal_chunks(const dino_pe* pe, int V) {
+  const int64_t warps = (int64_t)ceil_div((int)(pe->IJ / V), kNodalCols) * pe->mem;
+  int C = 1;
+  while (2 * C <= kNodalMaxChunks && warps * C < 16LL * pe->sms && pe->K >= 8 * C) C *= 2;
+  return C;
+}
+
+// Adjacent columns per thread for pe_nodal_kernel: two for dry states where
+// the latitude count is even (122 registers; four need 188 and run slower),
+// one with tracers (whose windows two columns would double).
+static int nodal_vec(const dino_pe* pe) {
+  return (pe->nT == 0 && pe->J % 2 == 0) ? 2 : 1;
+}
+
+static size_t nodal_smem(int K) { return (size_t)K * kLevPack * sizeof(float); }
+
+// Opts every pe_nodal_kernel form into the level table's shared memory.
+static int nodal_prepare(int K) {
+  const size_t smem = nodal_smem(K);
+  if (smem <= 48 * 1024) return DINO_OK;
+  const int n = (int)smem;
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_nodal_kernel<false, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, n));
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_nodal_kernel<false, 2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, n));
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_nodal_kernel<true, 1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, n));
+  return DINO_OK;
+}
+
+static NodalArgs make_nodal_args(dino_pe* pe);
+
+static int launch_nodal(dino_pe* pe, cudaStream_t st) {
+  const NodalArgs a = make_nodal_args(pe);
+  const int V = nodal_vec(pe);
+  const dim3 grid(ceil_div((int)(pe->IJ / V), kNodalCols), pe->mem);
+  const dim3 block(kNodalCols, nodal_chunks(pe, V));
+  const size_t smem = nodal_smem(pe->K);
+  if (pe->nT > 0)
+    pe_nodal_kernel<true, 1><<<grid, block, smem, st>>>(a);
+  else if (V == 2)
+    pe_nodal_kernel<false, 2><<<grid, block, smem, st>>>(a);
+  else
+    pe_nodal_kernel<false, 1><<<grid, block, smem, st>>>(a);
+  return check_launch("pe_nodal");
+}
+
 static NodalArgs make_nodal_args(dino_pe* pe) {
   const int K = pe->K, mem = pe->mem;
   const int mK = mem * K;
@@ -1699,6 +1933,7 @@ static NodalArgs make_nodal_args(dino_pe* pe) {
     a.o_lnps = pe->o_lnps;
     a.lev = pe->d_lev;
     a.lo = lev_offsets(K);
+    a.levpack = pe->d_levpack;
     a.lat = pe->d_lat;
     a.R = (float)pe->R;
     a.kappa = (float)pe->kappa;
@@ -1725,10 +1960,7 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
   DINO_TRY(pe_nodal_inputs(pe, state, st));
   // 3. fused nodal column kernel
   {
-    NodalArgs a = make_nodal_args(pe);
-    dim3 grid(ceil_div((int)pe->IJ, 128), mem);
-    pe_nodal_kernel<<<grid, 128, 0, st>>>(a);
-    DINO_TRY(check_launch("pe_nodal"));
+    DINO_TRY(launch_nodal(pe, st));
   }
   // 4. forward SHT
   DINO_TRY(sht_forward_to(p, pe->d_fwd_in, pe->d_fwd_out, pe->n_fwd, pe->d_work,
@@ -2043,6 +2275,7 @@ static void pe_free(dino_pe* pe) {
   for (auto& e : pe->mat_cache) cudaFree(e.d);
   for (auto& e : pe->filter_cache) cudaFree(e.d_filter);
   cudaFree(pe->d_lev);
+  cudaFree(pe->d_levpack);
   cudaFree(pe->d_lat);
   cudaFree(pe->d_orog);
   cudaFree(pe->d_aux);
@@ -2103,6 +2336,36 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
     }
   }
   DINO_TRY(upload_vec(&pe->d_lev, lev));
+  // The same constants packed per level for pe_nodal_kernel (kLevPack).
+  std::vector<float> pack((size_t)K * kLevPack, 0.f);
+  for (int k = 0; k < K; ++k) {
+    float* q = pack.data() + (size_t)k * kLevPack;
+    const double cut = std::max(0.0, (pe->sigma[k] - pe->hs_sigma_b) / (1.0 - pe->hs_sigma_b));
+    q[0] = lev[lo.dsig + k];
+    q[1] = (float)(1.0 / pe->dsig[k]);
+    q[2] = lev[lo.sumsig + k];
+    q[3] = lev[lo.tref + k];
+    q[4] = lev[lo.c2ci + k];
+    q[5] = k > 0 ? lev[lo.c2ci + k - 1] : 0.f;
+    q[6] = lev[lo.alpha + k];
+    q[7] = k > 0 ? lev[lo.alpha + k - 1] : 0.f;
+    q[8] = lev[lo.kv + k];
+    q[9] = (float)cut;
+    if (pe->hs_p0 > 0) {
+      const double lsp = std::log(pe->sigma[k] / pe->hs_p0);
+      q[10] = (float)std::exp(pe->kappa * lsp);
+      q[11] = (float)lsp;
+    }
+    q[12] = lev[lo.trefdiff + k];
+    q[13] = k > 0 ? lev[lo.trefdiff + k - 1] : 0.f;
+  }
+  DINO_TRY(upload_vec(&pe->d_levpack, pack));
+  DINO_TRY(nodal_prepare(K));
+  {
+    int dev = 0;
+    DINO_CHECK_CUDA(cudaGetDevice(&dev));
+    DINO_CHECK_CUDA(cudaDeviceGetAttribute(&pe->sms, cudaDevAttrMultiProcessorCount, dev));
+  }
   // Latitude constants: sec^2, Coriolis 2 Omega sin, sin^2, cos^2.
   std::vector<float> lat(4 * J);
   for (int j = 0; j < J; ++j) {
@@ -2208,6 +2471,8 @@ int dino_pe_create(dino_plan* plan, const dino_pe_desc* d, dino_pe** out) {
                DINO_ERR_ARG, "dino_pe_create: missing vertical arrays");
   DINO_REQUIRE(!(d->held_suarez && d->n_tracers > 0), DINO_ERR_UNSUPPORTED,
                "Held-Suarez forcing composes with tracer-free states only");
+  DINO_REQUIRE((int64_t)d->layers * plan->I * plan->J < ((int64_t)1 << 31),
+               DINO_ERR_UNSUPPORTED, "layers x nodal points must be below 2^31");
   dino_pe* pe = new dino_pe();
   pe->plan = plan;
   pe->K = d->layers;

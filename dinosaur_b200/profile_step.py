@@ -25,6 +25,8 @@ def main():
   ap.add_argument('--layers', type=int, default=24)
   ap.add_argument('--members', type=int, default=1)
   ap.add_argument('--held-suarez', action='store_true')
+  ap.add_argument('--moist', action='store_true',
+                  help='specific humidity and two passive tracers')
   ap.add_argument('--precision', default='fp32', choices=['fp32', 'bf16x3'])
   ap.add_argument('--steps', type=int, default=3)
   ap.add_argument('--dt-minutes', type=float, default=15.0)
@@ -36,8 +38,9 @@ def main():
   ps = units.SimUnits()
   tref = np.full(args.layers, 285.0) if args.held_suarez else np.linspace(
       220.0, 288.0, args.layers)
-  eq = pe.PrimitiveEquationsSigma(tref, np.zeros(g.modal_shape, np.float32),
-                                  coords, ps)
+  eq = pe.PrimitiveEquationsSigma(
+      tref, np.zeros(g.modal_shape, np.float32), coords, ps,
+      humidity_key='specific_humidity' if args.moist else None)
   if args.held_suarez:
     eq = ti.compose_equations(
         [eq, held_suarez.HeldSuarezForcingSigma(coords, ps, tref)])
@@ -51,7 +54,15 @@ def main():
   t = lambda shp: torch.as_tensor(
       (1e-4 * rng.standard_normal(shp) * scale).astype(np.float32), device='cuda')
   shape = lead + (args.layers,) + g.modal_shape
-  state = pe.State(t(shape), t(shape), t(shape), t(lead + (1,) + g.modal_shape))
+  tracers = {}
+  if args.moist:
+    const = np.zeros(shape, np.float32)
+    const[..., 0, 0] = 2.0 * np.sqrt(np.pi)  # the constant field 1
+    dev = lambda a: torch.as_tensor(a, device='cuda')
+    tracers = {'specific_humidity': dev(5e-3 * const) + 1e-2 * t(shape),
+               'tracer_a': dev(const) + t(shape), 'tracer_b': dev(const) + t(shape)}
+  state = pe.State(t(shape), t(shape), t(shape), t(lead + (1,) + g.modal_shape),
+                   tracers=tracers)
   eng = eq.engine(state)
   buf = eng.pack(state)
   eng.step_(buf, dt, step.filter_scaling, 1, graph=False)
@@ -62,7 +73,7 @@ def main():
   e1.record()
   torch.cuda.synchronize()
   print(f'{args.grid} K={args.layers} members={args.members} '
-        f'hs={args.held_suarez} {args.precision}: '
+        f'hs={args.held_suarez} moist={args.moist} {args.precision}: '
         f'{e0.elapsed_time(e1) / args.steps * 1e3:.1f} us/step, '
         f'finite={bool(torch.isfinite(buf).all())}')
 
