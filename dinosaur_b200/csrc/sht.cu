@@ -399,34 +399,50 @@ __device__ __forceinline__ void dft_reg(float2* v) {
 
 // One radix-R Stockham pass over N points for kFftJS columns.  load(n, c)
 // returns element n of column c; store(n, c, v) writes output element n.
-template <int N, int R, int kSign, class Load, class Store>
+// Every thread issues all of its loads before its first store; kSync puts a
+// barrier between the two, so that the pass may run in place on one shared
+// buffer.
+template <int N, int R, int kSign, bool kSync, class Load, class Store>
 __device__ __forceinline__ void stockham_pass(int Ns, const float2* twn,
                                               Load load, Store store) {
   constexpr int Q = N / R;
+  constexpr int kTotal = Q * kFftJS;
+  constexpr int kItems = (kTotal + kFftThreads - 1) / kFftThreads;
   const int stride = N / (Ns * R);
-  for (int item = threadIdx.x; item < Q * kFftJS; item += kFftThreads) {
-    const int c = item % kFftJS, j = item / kFftJS;
-    const int k = j % Ns;
-    float2 v[R];
+  float2 v[kItems][R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = load(j + r * Q, c);
-    if (k) {
+  for (int it = 0; it < kItems; ++it) {
+    const int item = threadIdx.x + it * kFftThreads;
+    if (item < kTotal) {
+      const int c = item % kFftJS, j = item / kFftJS;
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = twn[r * k * stride];
-        if (kSign < 0) w = cconj(w);
-        v[r] = cmul(v[r], w);
-      }
+      for (int r = 0; r < R; ++r) v[it][r] = load(j + r * Q, c);
     }
-    dft_reg<R, kSign>(v);
-    const int base = (j / Ns) * Ns * R + k;
+  }
+  if (kSync) __syncthreads();
 #pragma unroll
-    for (int r = 0; r < R; ++r) store(base + r * Ns, c, v[r]);
+  for (int it = 0; it < kItems; ++it) {
+    const int item = threadIdx.x + it * kFftThreads;
+    if (item < kTotal) {
+      const int c = item % kFftJS, j = item / kFftJS;
+      const int k = j % Ns;
+      if (k) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 w = twn[r * k * stride];
+          if (kSign < 0) w = cconj(w);
+          v[it][r] = cmul(v[it][r], w);
+        }
+      }
+      dft_reg<R, kSign>(v[it]);
+      const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) store(base + r * Ns, c, v[it][r]);
+    }
   }
 }
 
-// Radix schedule (at most three passes) for each supported N; the kernels
-// use one N x kFftJS shared buffer per pass.
+// Radix schedule (at most three passes) for each supported N.
 template <int N> struct FftRadix;
 template <> struct FftRadix<8> { static constexpr int r1 = 8, r2 = 1, r3 = 1; };
 template <> struct FftRadix<16> { static constexpr int r1 = 16, r2 = 1, r3 = 1; };
@@ -436,36 +452,34 @@ template <> struct FftRadix<128> { static constexpr int r1 = 16, r2 = 8, r3 = 1;
 template <> struct FftRadix<256> { static constexpr int r1 = 16, r2 = 16, r3 = 1; };
 template <> struct FftRadix<512> { static constexpr int r1 = 8, r2 = 8, r3 = 8; };
 
+// Shared memory of both kernels: one N x kFftJS complex buffer and the two
+// N-entry twiddle tables.
 template <int N>
-constexpr int fft_buffers() {
-  return 1 + (FftRadix<N>::r2 > 1) + (FftRadix<N>::r3 > 1);
+constexpr size_t fft_smem_bytes() {
+  return sizeof(float2) * ((size_t)N * kFftJS + 2 * N);
 }
 
-// Runs all passes: first pass reads via `first`, last pass writes via `last`,
-// intermediate passes ping-pong between the shared buffers a and b.
-template <int N, int kSign, class First, class Last>
-__device__ __forceinline__ void fft_passes(float2* a, float2* b,
-                                           const float2* twn, First first,
+// Runs all passes on the one shared buffer S: the first pass reads via
+// `first` (in place when kFirstInS), the last writes via `last`; the passes
+// between run in place.
+template <int N, int kSign, bool kFirstInS, class First, class Last>
+__device__ __forceinline__ void fft_passes(float2* S, const float2* twn, First first,
                                            Last last) {
   using Rd = FftRadix<N>;
-  auto smem_load = [](float2* buf) {
-    return [buf](int n, int c) { return buf[n * kFftJS + c]; };
-  };
-  auto smem_store = [](float2* buf) {
-    return [buf](int n, int c, float2 v) { buf[n * kFftJS + c] = v; };
-  };
+  auto s_load = [S](int n, int c) { return S[n * kFftJS + c]; };
+  auto s_store = [S](int n, int c, float2 v) { S[n * kFftJS + c] = v; };
   if constexpr (Rd::r2 == 1) {
-    stockham_pass<N, Rd::r1, kSign>(1, twn, first, last);
+    stockham_pass<N, Rd::r1, kSign, kFirstInS>(1, twn, first, last);
   } else if constexpr (Rd::r3 == 1) {
-    stockham_pass<N, Rd::r1, kSign>(1, twn, first, smem_store(a));
+    stockham_pass<N, Rd::r1, kSign, kFirstInS>(1, twn, first, s_store);
     __syncthreads();
-    stockham_pass<N, Rd::r2, kSign>(Rd::r1, twn, smem_load(a), last);
+    stockham_pass<N, Rd::r2, kSign, false>(Rd::r1, twn, s_load, last);
   } else {
-    stockham_pass<N, Rd::r1, kSign>(1, twn, first, smem_store(a));
+    stockham_pass<N, Rd::r1, kSign, kFirstInS>(1, twn, first, s_store);
     __syncthreads();
-    stockham_pass<N, Rd::r2, kSign>(Rd::r1, twn, smem_load(a), smem_store(b));
+    stockham_pass<N, Rd::r2, kSign, true>(Rd::r1, twn, s_load, s_store);
     __syncthreads();
-    stockham_pass<N, Rd::r3, kSign>(Rd::r1 * Rd::r2, twn, smem_load(b), last);
+    stockham_pass<N, Rd::r3, kSign, false>(Rd::r1 * Rd::r2, twn, s_load, last);
   }
 }
 
@@ -501,8 +515,10 @@ __device__ __forceinline__ void stage_tile(const float* __restrict__ src, int ro
 
 // Fourier coefficients F[b][row][j] -> nodal[b][i][j] (optionally scaled by
 // wq[j], which gives the adjoint of the weighted forward transform).
-// Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]) is formed from
-// global loads, then z = IDFT_N(Z) and x[2n] = Re z[n], x[2n+1] = Im z[n].
+// Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]), then
+// z = IDFT_N(Z) and x[2n] = Re z[n], x[2n+1] = Im z[n].  The coefficient tile
+// (at most 2N - 1 rows of kFftJS floats) is staged in the shared buffer, Z is
+// formed in registers and written back over it, and the passes run in place.
 template <int N>
 __global__ void __launch_bounds__(kFftThreads)
 rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
@@ -510,11 +526,8 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
                     const float2* __restrict__ tw_i,
                     const float* __restrict__ wq) {
   extern __shared__ float2 sm[];
-  constexpr int kBufs = fft_buffers<N>();
-  float2* Zs = sm;
-  float2* A = Zs + N * kFftJS;
-  float2* Bf = A + N * kFftJS;
-  float2* twn = Zs + kBufs * N * kFftJS;
+  float2* S = sm;
+  float2* twn = S + N * kFftJS;
   float2* twi = twn + N;
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
@@ -524,45 +537,51 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
     twn[t] = tw_n[t];
     twi[t] = tw_i[t];
   }
-  __syncthreads();
   const float* Fb = F + (size_t)b * M * J + j0;
+  const int rows = min(M, 2 * min(lw, N) - 1);  // rows X() reads; <= 2N - 1
+  const float* src = reinterpret_cast<const float*>(S);
+  stage_tile<2 * N>(Fb, rows, J, ncol, reinterpret_cast<float*>(S));
+  __syncthreads();
   const float inv_sqrt_2pi = 0.3989422804014327f;
   const float half_inv_sqrt_pi = 0.28209479177387814f;
-  // With two or more buffers, the coefficient tile (M <= 2N - 1 rows) is
-  // first staged in A, which the passes overwrite only after Zs is formed.
-  constexpr bool kStaged = kBufs > 1;
-  const float* src = Fb;
-  int sJ = J;
-  if constexpr (kStaged) {
-    const int rows = min(M, 2 * min(lw, N) - 1);  // rows X() reads; <= 2N - 1
-    stage_tile<2 * N>(Fb, rows, J, ncol, reinterpret_cast<float*>(A));
-    __syncthreads();
-    src = reinterpret_cast<const float*>(A);
-    sJ = kFftJS;
-  }
   auto X = [&](int k, int c) -> float2 {
     if (c >= ncol || k >= lw || k >= N) return make_float2(0.f, 0.f);
     if (k == 0) return make_float2(src[c] * inv_sqrt_2pi, 0.f);
-    return make_float2(src[(size_t)(2 * k - 1) * sJ + c] * half_inv_sqrt_pi,
-                       -src[(size_t)(2 * k) * sJ + c] * half_inv_sqrt_pi);
+    return make_float2(src[(2 * k - 1) * kFftJS + c] * half_inv_sqrt_pi,
+                       -src[(2 * k) * kFftJS + c] * half_inv_sqrt_pi);
   };
   // Pairs (k, N - k), k = 0..N/2; k = 0 pairs with the (zero) Nyquist term.
-  for (int item = tid; item < (N / 2 + 1) * kFftJS; item += kFftThreads) {
-    const int k = item / kFftJS, c = item % kFftJS;
-    const float2 xk = X(k, c);
-    const float2 xn = (k == 0) ? make_float2(0.f, 0.f) : X(N - k, c);
-    const float2 xnc = cconj(xn), xkc = cconj(xk);
-    Zs[k * kFftJS + c] =
-        cadd(cadd(xk, xnc), cmul_i<1>(cmul(twi[k], csub(xk, xnc))));
-    if (k > 0 && k < N / 2 + (N & 1)) {
-      const int kn = N - k;
-      Zs[kn * kFftJS + c] =
-          cadd(cadd(xn, xkc), cmul_i<1>(cmul(twi[kn], csub(xn, xkc))));
+  constexpr int kTotal = (N / 2 + 1) * kFftJS;
+  constexpr int kItems = (kTotal + kFftThreads - 1) / kFftThreads;
+  float2 xk[kItems], xn[kItems];
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    const int item = tid + it * kFftThreads;
+    if (item < kTotal) {
+      const int k = item / kFftJS, c = item % kFftJS;
+      xk[it] = X(k, c);
+      xn[it] = (k == 0) ? make_float2(0.f, 0.f) : X(N - k, c);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kItems; ++it) {
+    const int item = tid + it * kFftThreads;
+    if (item < kTotal) {
+      const int k = item / kFftJS, c = item % kFftJS;
+      const float2 xnc = cconj(xn[it]), xkc = cconj(xk[it]);
+      S[k * kFftJS + c] =
+          cadd(cadd(xk[it], xnc), cmul_i<1>(cmul(twi[k], csub(xk[it], xnc))));
+      if (k > 0 && k < N / 2 + (N & 1)) {
+        const int kn = N - k;
+        S[kn * kFftJS + c] =
+            cadd(cadd(xn[it], xkc), cmul_i<1>(cmul(twi[kn], csub(xn[it], xkc))));
+      }
     }
   }
   __syncthreads();
   float* ob = out + (size_t)b * (2 * N) * J + j0;
-  auto first = [Zs](int n, int c) { return Zs[n * kFftJS + c]; };
+  auto first = [S](int n, int c) { return S[n * kFftJS + c]; };
   auto last = [ob, ncol, J, wq, j0](int n, int c, float2 v) {
     if (c < ncol) {
       const float s = wq ? wq[j0 + c] : 1.f;
@@ -570,7 +589,7 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
       ob[(size_t)(2 * n + 1) * J + c] = v.y * s;
     }
   };
-  fft_passes<N, 1>(A, Bf, twn, first, last);
+  fft_passes<N, 1, true>(S, twn, first, last);
 }
 
 // nodal[b][i][j] -> F[b][row][j] (times wq[j] when given: the forward SHT's
@@ -582,11 +601,8 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
                     const float2* __restrict__ tw_i,
                     const float* __restrict__ wq) {
   extern __shared__ float2 sm[];
-  constexpr int kBufs = fft_buffers<N>();
-  float2* Zs = sm;
-  float2* A = Zs + N * kFftJS;
-  float2* Bf = A + N * kFftJS;
-  float2* twn = Zs + kBufs * N * kFftJS;
+  float2* S = sm;
+  float2* twn = S + N * kFftJS;
   float2* twi = twn + N;
   const int tid = threadIdx.x;
   const int b = blockIdx.y;
@@ -598,14 +614,14 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
   }
   __syncthreads();
   const float* xb = x + (size_t)b * (2 * N) * J + j0;
-  // The first pass reads the nodal tile straight from global memory, which
-  // overlaps the loads with its butterflies.
+  // The first pass reads the nodal tile straight from global memory, all of
+  // a thread's loads in flight together.
   auto first = [xb, ncol, J](int n, int c) {
     if (c >= ncol) return make_float2(0.f, 0.f);
     return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
   };
-  auto last = [Zs](int n, int c, float2 v) { Zs[n * kFftJS + c] = v; };
-  fft_passes<N, -1>(A, Bf, twn, first, last);
+  auto last = [S](int n, int c, float2 v) { S[n * kFftJS + c] = v; };
+  fft_passes<N, -1, false>(S, twn, first, last);
   __syncthreads();
   float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
@@ -613,8 +629,8 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
   for (int idx = tid; idx < lw * kFftJS; idx += kFftThreads) {
     int k = idx / kFftJS, c = idx % kFftJS;
     if (c >= ncol) continue;
-    float2 zk = Zs[(k % N) * kFftJS + c];
-    float2 zc = cconj(Zs[((N - k) % N) * kFftJS + c]);
+    float2 zk = S[(k % N) * kFftJS + c];
+    float2 zc = cconj(S[((N - k) % N) * kFftJS + c]);
     float2 s = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
     float2 d = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
     // X[k] = s + e^{-2 pi i k / I} * (-i d)
@@ -667,7 +683,7 @@ static int configure_rfft() {
   // Kernel attributes are set once per process, outside any stream capture.
   static bool configured = false;
   if (configured) return DINO_OK;
-  const int smem = (int)(sizeof(float2) * (fft_buffers<N>() * (size_t)N * kFftJS + 2 * N));
+  const int smem = (int)fft_smem_bytes<N>();
   DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_inverse_kernel<N>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_forward_kernel<N>,
@@ -679,7 +695,7 @@ static int configure_rfft() {
 template <int N>
 static int launch_rfft(dino_plan* p, const float* in, float* out, int nf,
                        bool inverse, const float* wq, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * (fft_buffers<N>() * (size_t)N * kFftJS + 2 * N);
+  const size_t smem = fft_smem_bytes<N>();
   if (!p) return configure_rfft<N>();
   DINO_TRY(configure_rfft<N>());
   dim3 grid(ceil_div(p->J, kFftJS), nf);
