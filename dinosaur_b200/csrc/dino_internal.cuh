@@ -174,12 +174,12 @@ int sht_inverse_adjoint_to(dino_plan* p, const float* nodal_ct, float* modal_ct,
                            int nfields, float* work, int work_fields, cudaStream_t st);
 int sht_forward_adjoint_to(dino_plan* p, const float* modal_ct, float* nodal_ct,
                            int nfields, float* work, int work_fields, cudaStream_t st);
-// slot: -1 uses the whole tensor-core operand slabs; 0 / 1 one half each, so
-// that two chunks can run at once on different streams.
+// Fields per chunk of a chunked transform of nf fields (sht.cu).
+int l2_chunk(dino_plan* p, int nf, int work_fields);
 int legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
-                     int nfields, cudaStream_t st, int slot = -1);
+                     int nfields, cudaStream_t st);
 int legendre_forward(dino_plan* p, const float* fourier, float* out_modal,
-                     int nfields, cudaStream_t st, int slot = -1);
+                     int nfields, cudaStream_t st);
 int fourier_inverse(dino_plan* p, const float* fourier, float* nodal,
                     int nfields, bool weighted_adjoint, cudaStream_t st);
 int fourier_forward(dino_plan* p, const float* nodal, float* fourier,
@@ -197,11 +197,9 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 int tc_tables_build(dino_plan* p);
 void tc_tables_free(dino_plan* p);
 int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out_fourier,
-                        int nfields, cudaStream_t st, int slot);
+                        int nfields, cudaStream_t st);
 int tc_legendre_forward(dino_plan* p, const float* fourier, float* out_modal,
-                        int nfields, cudaStream_t st, int slot);
-// Fields one operand-slab half holds (any count for the FP32 path).
-int tc_slot_fields(dino_plan* p);
+                        int nfields, cudaStream_t st);
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 

@@ -11,10 +11,13 @@
 //   forward:  D[r, l'] = sum_j  G_p[r, j]  P_p[l', j]     (K = j,  N = l')
 // with r = (field, cos/sin) rows, p the parity of l - m (the N/S fold),
 // l = m + 2 l' + p, and G_0 / G_1 the symmetric / antisymmetric latitude
-// folds.  All operands are K-major bf16 in HBM, loaded by TMA (no multicast)
-// into 128-byte-swizzled shared memory tiles; one thread issues
+// folds.  The tables P_p are K-major split bf16 in HBM, loaded by TMA (no
+// multicast) into 128-byte-swizzled shared memory tiles; the A operand is
+// produced in the same layout by six warps of the CTA straight from the FP32
+// modal coefficients (inverse) or Fourier coefficients (forward): one read of
+// the source gives both parities, folded and split.  One thread issues
 // tcgen05.mma (M = 128, N = latitudes or l', K = 16 per instruction) into two
-// TMEM accumulators (one per parity); four warps read them back with
+// TMEM accumulators (one per parity); all eight warps read them back with
 // tcgen05.ld and write the unfolded FP32 result.  Only the K steps and N
 // columns that the triangular (m, l) range needs are issued.
 
@@ -38,11 +41,8 @@ struct TcTables {
   int Np = 0;   // inverse N (latitudes), multiple of 16
   int Kj = 0;   // forward K extent (latitudes), multiple of 64
   int Nf = 0;   // forward N (l'), multiple of 16
-  int cap = 0;  // fields per launch
-  int Rp = 0;   // rows per (m, parity) slab of the A operands
   bf16 *Bih = nullptr, *Bil = nullptr, *Bfh = nullptr, *Bfl = nullptr;
-  bf16 *Aih = nullptr, *Ail = nullptr, *Afh = nullptr, *Afl = nullptr;
-  CUtensorMap tAih, tAil, tBih, tBil, tAfh, tAfl, tBfh, tBfl;
+  CUtensorMap tBih, tBil, tBfh, tBfl;
   int* d_err = nullptr;
   int stages_inv = 0, stages_fwd = 0;
   size_t smem_inv = 0, smem_fwd = 0;
@@ -99,122 +99,12 @@ __global__ void tc_table_kernel(int lw, int L, int Jh, const double* __restrict_
   }
 }
 
-__device__ __forceinline__ void split_bf16(float v, bf16& hi, bf16& lo) {
-  hi = __float2bfloat16_rn(v);
-  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-}
-
-__device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
-  if (m == 0) {
-    b = r;
-    row = 0;
-  } else {
-    b = r >> 1;
-    row = 2 * m - 1 + (r & 1);
-  }
-}
-
-// Eight consecutive split values as one 16-byte store of each half.
-__device__ __forceinline__ void store_split8(const float (&v)[8], bf16* hi, bf16* lo) {
-  __align__(16) bf16 h[8];
-  __align__(16) bf16 l[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) split_bf16(v[i], h[i], l[i]);
-  *reinterpret_cast<uint4*>(hi) = *reinterpret_cast<const uint4*>(h);
-  *reinterpret_cast<uint4*>(lo) = *reinterpret_cast<const uint4*>(l);
-}
-
-// Modal rows -> A[m][p][r][kk] = x[b][row][m + 2 kk + p], zero-padded to the
-// next multiple of 64 in kk.  A thread converts 8 consecutive kk of both
-// parities (16 consecutive l, read as one contiguous run) and writes them as
-// 16-byte stores.
-__global__ void tc_split_inverse_kernel(Segs in, int nf, int M, int L, int Rp,
-                                        int Kp, int roff, bf16* __restrict__ Ah,
-                                        bf16* __restrict__ Al) {
-  const int m = blockIdx.y;
-  const int rows = (m == 0) ? nf : 2 * nf;
-  const int Lm = L - m;
-  const int gw = round_up((Lm + 1) >> 1, 64) / 8;  // 8-kk groups per row
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (size_t)rows * gw) return;
-  const int g = idx % gw;
-  const int r = idx / gw;
-  int b, row;
-  tc_row_map(m, r, b, row);
-  const float* xr = seg_field(in, b, (size_t)M * L) + (size_t)row * L + m;
-  const int k0 = 16 * g;
-  float ev[8], od[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int ke = k0 + 2 * i, ko = ke + 1;
-    ev[i] = (ke < Lm) ? xr[ke] : 0.f;
-    od[i] = (ko < Lm) ? xr[ko] : 0.f;
-  }
-  const size_t o0 = ((size_t)(m * 2) * Rp + roff + r) * Kp + 8 * g;
-  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + roff + r) * Kp + 8 * g;
-  store_split8(ev, Ah + o0, Al + o0);
-  store_split8(od, Ah + o1, Al + o1);
-}
-
-// Weighted Fourier coefficients G[b][row][j] -> symmetric (p = 0) and
-// antisymmetric (p = 1) latitude folds, split into A[m][p][r][j].  A thread
-// folds 8 consecutive latitudes against their mirrors and writes 16-byte
-// stores.
-__global__ void tc_fold_forward_kernel(const float* __restrict__ G, int nf, int M,
-                                       int J, int Jh, int Rp, int Kj, int roff,
-                                       bf16* __restrict__ Ah, bf16* __restrict__ Al) {
-  const int m = blockIdx.y;
-  const int rows = (m == 0) ? nf : 2 * nf;
-  const int gw = Kj / 8;
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (size_t)rows * gw) return;
-  const int g = idx % gw;
-  const int r = idx / gw;
-  int b, row;
-  tc_row_map(m, r, b, row);
-  const float* gr = G + ((size_t)b * M + row) * J;
-  const int j0 = 8 * g;
-  float sv[8], dv[8];
-  if (j0 + 8 <= Jh && (J & 3) == 0) {
-    // Aligned fast path: j0..j0+7 and J-8-j0..J-1-j0 are float4 pairs.
-    const float4 a0 = *reinterpret_cast<const float4*>(gr + j0);
-    const float4 a1 = *reinterpret_cast<const float4*>(gr + j0 + 4);
-    const float4 b0 = *reinterpret_cast<const float4*>(gr + J - 8 - j0);
-    const float4 b1 = *reinterpret_cast<const float4*>(gr + J - 4 - j0);
-    const float d[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-    const float e[8] = {b1.w, b1.z, b1.y, b1.x, b0.w, b0.z, b0.y, b0.x};
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      sv[i] = d[i] + e[i];
-      dv[i] = d[i] - e[i];
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int j = j0 + i;
-      float s = 0.f, d = 0.f;
-      if (j < Jh) {
-        const float g1 = gr[j];
-        const int jm = J - 1 - j;
-        const float g2 = (jm != j) ? gr[jm] : 0.f;
-        s = g1 + g2;
-        d = g1 - g2;
-      }
-      sv[i] = s;
-      dv[i] = d;
-    }
-  }
-  const size_t o0 = ((size_t)(m * 2) * Rp + roff + r) * Kj + j0;
-  const size_t o1 = ((size_t)(m * 2 + 1) * Rp + roff + r) * Kj + j0;
-  store_split8(sv, Ah + o0, Al + o0);
-  store_split8(dv, Ah + o1, Al + o1);
-}
-
 // ---------------------------------------------------------------------------
 // tcgen05 / TMA / mbarrier primitives (inline PTX)
 // ---------------------------------------------------------------------------
 
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 256;
+constexpr int kTcProducers = 192;  // warps 2-7
 constexpr int kMaxStages = 4;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 
@@ -241,11 +131,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// True once the phase with the given parity has completed; the hardware may
+// suspend the thread for a while before answering false (try_wait), so a
+// waiting warp does not spin on the issue slots.
 __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}\n"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
@@ -328,28 +225,219 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void split_bf16(float v, bf16& hi, bf16& lo) {
+  hi = __float2bfloat16_rn(v);
+  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+__device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
+  if (m == 0) {
+    b = r;
+    row = 0;
+  } else {
+    b = r >> 1;
+    row = 2 * m - 1 + (r & 1);
+  }
+}
+
+// Byte offset of 16-byte chunk c (K entries 8c .. 8c+7) of row r in a
+// 128-row x 64-entry bf16 K-major tile with the 128-byte swizzle: the layout
+// that TMA writes for CU_TENSOR_MAP_SWIZZLE_128B and the UMMA descriptor
+// (umma_desc_sw128) reads.
+__device__ __forceinline__ uint32_t sw128_off(int r, int c) {
+  return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(bf16 a, bf16 b) {
+  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// Splits eight values v[s0], v[s0 + st], ... into hi / lo bf16 and writes
+// them as one 16-byte chunk of each tile (shared memory).
+template <int N>
+__device__ __forceinline__ void put_split8(const float (&v)[N], int s0, int st,
+                                           uint8_t* hi, uint8_t* lo, uint32_t off) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    bf16 h0, l0, h1, l1;
+    split_bf16(v[s0 + (2 * i) * st], h0, l0);
+    split_bf16(v[s0 + (2 * i + 1) * st], h1, l1);
+    h[i] = pack_bf16x2(h0, h1);
+    l[i] = pack_bf16x2(l0, l1);
+  }
+  *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
 // ---------------------------------------------------------------------------
 // The contraction kernel
 // ---------------------------------------------------------------------------
 
 struct TcArgs {
   int nf, M, L, J, Jh;
-  int Rp;        // A slab rows
-  int roff;      // first A slab row of this launch (operand-slab half)
   int Nrows;     // rows of one (m, parity) B table (Np or Nf)
   int Nsub;      // B tile rows = N columns of this CTA (blockIdx.z-th range)
   int stages;
   int tmem_cols; // allocated TMEM columns (power of two)
+  int vec;       // inverse: rows of the modal input start 16-byte aligned
+  Segs in;       // inverse: modal coefficients [nf][M][L]
+  const float* G;  // forward: weighted Fourier coefficients [nf][M][J]
   float* out;    // inverse: Fourier [nf][M][J]; forward: modal [nf][M][L]
   int* err;
 };
 
+// Pipeline order of the (K block, parity) stages: block k's parity 0, then
+// its parity 1 while k < kb1 (kb1 = K blocks of parity 1 <= those of parity 0).
+__device__ __forceinline__ void tc_seq(int i, int kb1, int& k, int& p) {
+  if (i < 2 * kb1) {
+    k = i >> 1;
+    p = i & 1;
+  } else {
+    k = i - kb1;
+    p = 0;
+  }
+}
+
+// A operand of K block k for this CTA's 128 rows, both parities from one
+// read of the FP32 source, written split into the stage tiles t0 (parity 0)
+// and t1 (parity 1, null when absent): hi at t, lo at t + 16 KB.
+//   inverse: A_p[r][kk] = x[b][row][m + 2 (64 k + kk) + p]  (0 past l = L - 1)
+//   forward: A_p[r][jj] = G[j] + (-1)^p G[J - 1 - j], j = 64 k + jj  (0 past Jh)
+// A task is one (row, 16-byte chunk); each thread loads kTcUnroll tasks before
+// converting any, so that enough bytes are in flight to cover the latency.
+// S = m mod 4 places the 16 inverse entries inside five aligned float4.
+constexpr int kTcTasks = 128 * 8;
+constexpr int kTcUnroll = 3;
+
+template <int S>
+__device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int tile, int rows,
+                                                   int k, uint8_t* t0, uint8_t* t1, int pt) {
+  constexpr uint32_t kTile = 128u * 128u;
+  for (int q0 = pt; q0 < kTcTasks; q0 += kTcUnroll * kTcProducers) {
+    float w[kTcUnroll][20];
+#pragma unroll
+    for (int u = 0; u < kTcUnroll; ++u) {
+      const int q = q0 + u * kTcProducers;
+#pragma unroll
+      for (int e = 0; e < 20; ++e) w[u][e] = 0.f;
+      if (q >= kTcTasks) continue;
+      const int r = q >> 3, c = q & 7;
+      const int rr = tile * 128 + r;
+      if (rr >= rows) continue;
+      int b, row;
+      tc_row_map(m, rr, b, row);
+      const int l0 = 128 * k + 16 * c;  // relative to l = m
+      const int lim = (a.L - m) - l0;   // valid entries from l0
+      const float* src = seg_field(a.in, b, (size_t)a.M * a.L) + (size_t)row * a.L + m + l0;
+      if (a.vec && lim >= 20) {
+        const float4* w4 = reinterpret_cast<const float4*>(src - S);
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const float4 t = __ldg(w4 + i);
+          w[u][4 * i] = t.x;
+          w[u][4 * i + 1] = t.y;
+          w[u][4 * i + 2] = t.z;
+          w[u][4 * i + 3] = t.w;
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) w[u][e + S] = (e < lim) ? __ldg(src + e) : 0.f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kTcUnroll; ++u) {
+      const int q = q0 + u * kTcProducers;
+      if (q >= kTcTasks) continue;
+      const uint32_t off = sw128_off(q >> 3, q & 7);
+      // Entries S .. S+15: even l - m are parity 0, odd ones parity 1.
+      put_split8(w[u], S, 2, t0, t0 + kTile, off);
+      if (t1) put_split8(w[u], S + 1, 2, t1, t1 + kTile, off);
+    }
+  }
+}
+
+__device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int tile, int rows,
+                                                   int k, uint8_t* t0, uint8_t* t1, int pt) {
+  constexpr uint32_t kTile = 128u * 128u;
+  const bool vec = (a.J & 3) == 0;
+  for (int q0 = pt; q0 < kTcTasks; q0 += kTcUnroll * kTcProducers) {
+    float d[kTcUnroll][8], e[kTcUnroll][8];  // G[j0 + t], G[J - 1 - j0 - t]
+#pragma unroll
+    for (int u = 0; u < kTcUnroll; ++u) {
+      const int q = q0 + u * kTcProducers;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) d[u][t] = e[u][t] = 0.f;
+      if (q >= kTcTasks) continue;
+      const int r = q >> 3, c = q & 7;
+      const int rr = tile * 128 + r;
+      if (rr >= rows) continue;
+      int b, row;
+      tc_row_map(m, rr, b, row);
+      const float* gr = a.G + ((size_t)b * a.M + row) * a.J;
+      const int j0 = 64 * k + 8 * c;
+      if (vec && j0 + 8 <= a.Jh) {
+        // j0 .. j0+7 and J-8-j0 .. J-1-j0 are float4 pairs.
+        const float4 a0 = __ldg(reinterpret_cast<const float4*>(gr + j0));
+        const float4 a1 = __ldg(reinterpret_cast<const float4*>(gr + j0 + 4));
+        const float4 b0 = __ldg(reinterpret_cast<const float4*>(gr + a.J - 8 - j0));
+        const float4 b1 = __ldg(reinterpret_cast<const float4*>(gr + a.J - 4 - j0));
+        d[u][0] = a0.x; d[u][1] = a0.y; d[u][2] = a0.z; d[u][3] = a0.w;
+        d[u][4] = a1.x; d[u][5] = a1.y; d[u][6] = a1.z; d[u][7] = a1.w;
+        e[u][0] = b1.w; e[u][1] = b1.z; e[u][2] = b1.y; e[u][3] = b1.x;
+        e[u][4] = b0.w; e[u][5] = b0.z; e[u][6] = b0.y; e[u][7] = b0.x;
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const int j = j0 + t;
+          if (j < a.Jh) {
+            const int jm = a.J - 1 - j;
+            d[u][t] = __ldg(gr + j);
+            e[u][t] = (jm != j) ? __ldg(gr + jm) : 0.f;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kTcUnroll; ++u) {
+      const int q = q0 + u * kTcProducers;
+      if (q >= kTcTasks) continue;
+      const uint32_t off = sw128_off(q >> 3, q & 7);
+      float sv[8], dv[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        sv[t] = d[u][t] + e[u][t];
+        dv[t] = d[u][t] - e[u][t];
+      }
+      put_split8(sv, 0, 1, t0, t0 + kTile, off);
+      if (t1) put_split8(dv, 0, 1, t1, t1 + kTile, off);
+    }
+  }
+}
+
+template <bool kForward>
+__device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int rows, int k,
+                                           uint8_t* t0, uint8_t* t1, int pt) {
+  if (kForward) {
+    tc_produce_forward(a, m, tile, rows, k, t0, t1, pt);
+  } else {
+    switch (m & 3) {
+      case 0: tc_produce_inverse<0>(a, m, tile, rows, k, t0, t1, pt); break;
+      case 1: tc_produce_inverse<1>(a, m, tile, rows, k, t0, t1, pt); break;
+      case 2: tc_produce_inverse<2>(a, m, tile, rows, k, t0, t1, pt); break;
+      default: tc_produce_inverse<3>(a, m, tile, rows, k, t0, t1, pt); break;
+    }
+  }
+}
+
+// Warp roles: warp 0 lane 0 loads the B tables by TMA, warp 1 allocates TMEM
+// and its lane 0 issues the MMAs, warps 2-7 produce the A tiles; all eight
+// warps drain TMEM in the epilogue (warp w reads lane quarter w mod 4 and
+// every other 16-column chunk).
 template <bool kForward>
 __global__ void __launch_bounds__(kTcThreads, 2)
-legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
-                   const __grid_constant__ CUtensorMap tAl,
-                   const __grid_constant__ CUtensorMap tBh,
-                   const __grid_constant__ CUtensorMap tBl, TcArgs a) {
+legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
+                   const __grid_constant__ CUtensorMap tBl, const __grid_constant__ TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kMaxStages];
   __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
@@ -394,7 +482,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.stages; ++s) {
-      mbar_init(&full_bar[s], 1);
+      // One arrive with the B bytes (TMA) and one per producer thread.
+      mbar_init(&full_bar[s], 1 + kTcProducers);
       mbar_init(&empty_bar[s], 1);
     }
     mbar_init(&done_bar, 1);
@@ -415,19 +504,16 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
   const int acc_cols = a.Nsub;  // parity p accumulates at column p * Nsub
 
   if (threadIdx.x == 0) {
-    // TMA producer.
+    // B producer (TMA).
     for (int i = 0; i < nblocks; ++i) {
       const int s = i % a.stages;
       const int use = i / a.stages;
       if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, a.err, 1)) break;
-      const int p = (i < kblk[0]) ? 0 : 1;
-      const int k = (p == 0) ? i : i - kblk[0];
+      int k, p;
+      tc_seq(i, kblk[1], k, p);
       uint8_t* st = base + (size_t)s * stage_bytes;
-      mbar_expect_tx(&full_bar[s], stage_bytes);
-      const int ya = (m * 2 + p) * a.Rp + a.roff + tile * 128;
+      mbar_expect_tx(&full_bar[s], 2 * tile_b);
       const int yb = (m * 2 + p) * a.Nrows + lo;
-      tma_load_2d(st, &tAh, &full_bar[s], k * 64, ya);
-      tma_load_2d(st + tile_a, &tAl, &full_bar[s], k * 64, ya);
       tma_load_2d(st + 2 * tile_a, &tBh, &full_bar[s], k * 64, yb);
       tma_load_2d(st + 2 * tile_a + tile_b, &tBl, &full_bar[s], k * 64, yb);
     }
@@ -438,11 +524,11 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
       const int use = i / a.stages;
       if (!mbar_wait(&full_bar[s], use & 1, a.err, 2)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int p = (i < kblk[0]) ? 0 : 1;
-      const int k = (p == 0) ? i : i - kblk[0];
-      const int steps = min(4, ksteps[p] - k * 4);
+      int k, p;
+      tc_seq(i, kblk[1], k, p);
+      const int steps = min(4, (p ? ksteps[1] : ksteps[0]) - k * 4);
       const uint32_t d = tmem + (uint32_t)(p * acc_cols);
-      const uint32_t idesc = umma_idesc_bf16(ncols[p]);
+      const uint32_t idesc = umma_idesc_bf16(p ? ncols[1] : ncols[0]);
       uint8_t* st = base + (size_t)s * stage_bytes;
       const uint64_t dah = umma_desc_sw128(st);
       const uint64_t dal = umma_desc_sw128(st + tile_a);
@@ -459,6 +545,24 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
     }
     // Arrives once every MMA issued above has completed.
     umma_commit(&done_bar);
+  } else if (warp >= 2) {
+    // A producers: block k's parities go to consecutive stages.
+    const int pt = threadIdx.x - 64;
+    for (int k = 0; k < kblk[0]; ++k) {
+      const bool two = k < kblk[1];
+      const int i0 = two ? 2 * k : k + kblk[1];
+      const int s0 = i0 % a.stages, u0 = i0 / a.stages;
+      const int s1 = (i0 + 1) % a.stages, u1 = (i0 + 1) / a.stages;
+      if (u0 > 0 && !mbar_wait(&empty_bar[s0], (u0 - 1) & 1, a.err, 4)) break;
+      if (two && u1 > 0 && !mbar_wait(&empty_bar[s1], (u1 - 1) & 1, a.err, 4)) break;
+      uint8_t* t0 = base + (size_t)s0 * stage_bytes;
+      uint8_t* t1 = two ? base + (size_t)s1 * stage_bytes : nullptr;
+      tc_produce<kForward>(a, m, tile, rows, k, t0, t1, pt);
+      // Make the generic-proxy stores visible to the tensor cores.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&full_bar[s0]);
+      if (two) mbar_arrive(&full_bar[s1]);
+    }
   }
   __syncwarp();
   bool ok = mbar_wait(&done_bar, 0, a.err, 3);
@@ -466,17 +570,18 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
   if (ok) {
-    // Epilogue.  Each warp owns TMEM lanes (rows) 32w .. 32w+31; a thread
-    // reads its row's accumulator columns, the warp stages a 32-row block in
-    // shared memory (the drained pipeline buffers) and writes it back with
-    // row-contiguous, coalesced stores.
+    // Epilogue.  Warp w reads TMEM lanes (rows) 32 (w mod 4) .. +31, stages a
+    // 32-row block in shared memory (the drained pipeline buffers) and writes
+    // it back with row-contiguous, coalesced stores; the two warps of a lane
+    // quarter take alternate 16-column chunks.
     constexpr int kStride = 36;  // floats per staged row (16-byte multiple)
+    const int quarter = warp & 3, half = warp >> 2;
     float* stage = reinterpret_cast<float*>(base) + warp * 32 * kStride;
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-    const int row0 = tile * 128 + warp * 32;  // first row of this warp
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+    const int row0 = tile * 128 + quarter * 32;  // first row of this warp
     if (!kForward) {
       const bool vec = (a.J & 3) == 0;
-      for (int c = 0; c < a.Nsub / 16; ++c) {
+      for (int c = half; c < a.Nsub / 16; c += 2) {
         float e[16], od[16];
         tmem_ld16(lane_base + c * 16, e);
         if (n_par[1] > 0) {
@@ -497,7 +602,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
         const int jm = a.J - jb - 16;
         // 4 threads per row, 8 rows per pass, 4 passes; two half-blocks.
         for (int pass = 0; pass < 8; ++pass) {
-          const int half = pass >> 2;                 // 0: direct, 1: mirror
+          const int hb = pass >> 2;                    // 0: direct, 1: mirror
           const int r = (pass & 3) * 8 + (lane >> 2);  // staged row
           const int q = lane & 3;                      // float4 within 16
           const int rr = row0 + r;
@@ -505,9 +610,9 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
             int b, row;
             tc_row_map(m, rr, b, row);
             float* o = a.out + ((size_t)b * a.M + row) * a.J;
-            const float* src = stage + r * kStride + half * 16 + q * 4;
-            const int j = (half ? jm : jb) + q * 4;
-            if (vec && jb + 16 <= a.Jh && (half == 0 || jm >= a.Jh)) {
+            const float* src = stage + r * kStride + hb * 16 + q * 4;
+            const int j = (hb ? jm : jb) + q * 4;
+            if (vec && jb + 16 <= a.Jh && (hb == 0 || jm >= a.Jh)) {
               *reinterpret_cast<float4*>(o + j) =
                   *reinterpret_cast<const float4*>(src);
             } else {
@@ -516,7 +621,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
                 const int jj = j + e2;
                 // direct half covers j < Jh; mirrored half covers j >= J - Jh
                 // except the self-mirrored middle row of an odd J.
-                if (half == 0) {
+                if (hb == 0) {
                   if (jj < a.Jh) o[jj] = src[e2];
                 } else {
                   const int jsrc = a.J - 1 - jj;  // its direct index
@@ -529,8 +634,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
         __syncwarp();
       }
     } else {
-      // Structural zeros l < m (first N range only), one row at a time.
-      for (int r = 0; r < 32 && lo == 0; ++r) {
+      // Structural zeros l < m (first N range only), alternate rows.
+      for (int r = half; r < 32 && lo == 0; r += 2) {
         const int rr = row0 + r;
         if (rr >= rows) break;
         int b, row;
@@ -539,7 +644,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tAh,
         for (int l = lane; l < m; l += 32) o[l] = 0.f;
       }
       const int nchunks = (max(cnt[0], cnt[1]) + 15) / 16;
-      for (int c = 0; c < nchunks; ++c) {
+      for (int c = half; c < nchunks; c += 2) {
         float e[16], od[16];
         tmem_ld16(lane_base + c * 16, e);
         if (cnt[1] > 0) {
@@ -652,9 +757,34 @@ static void tc_candidates(int nfull, std::vector<TcShape>* out) {
   }
 }
 
+// Modal rows start 16-byte aligned in every segment (the inverse producer's
+// float4 path).
+static int tc_vec_input(const dino_plan* p, const Segs& in) {
+  if (p->L % 4 != 0) return 0;
+  for (int i = 0; i < in.n; ++i)
+    if (((uintptr_t)in.ptr[i] & 15) != 0) return 0;
+  return 1;
+}
+
+static TcArgs tc_args(const dino_plan* p, const TcTables* t, bool forward, int nf) {
+  TcArgs a{};
+  a.nf = nf;
+  a.M = p->M;
+  a.L = p->L;
+  a.J = p->J;
+  a.Jh = p->Jh;
+  a.Nrows = forward ? t->Nf : t->Np;
+  a.Nsub = forward ? t->Nsub_fwd : t->Nsub_inv;
+  a.stages = forward ? t->stages_fwd : t->stages_inv;
+  a.tmem_cols = tmem_cols_for(2 * a.Nsub);
+  a.err = t->d_err;
+  return a;
+}
+
 template <bool kForward>
-static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf, float* out,
-                         cudaEvent_t e0, cudaEvent_t e1, float* us) {
+static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
+                         const float* src, float* out, cudaEvent_t e0, cudaEvent_t e1,
+                         float* us) {
   const size_t lw2 = (size_t)p->lw * 2;
   CUtensorMap bh, bl;
   if (!kForward) {
@@ -664,26 +794,22 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf, fl
     DINO_TRY(make_map(&bh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
     DINO_TRY(make_map(&bl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
   }
-  TcArgs a{};
-  a.nf = nf;
-  a.M = p->M;
-  a.L = p->L;
-  a.J = p->J;
-  a.Jh = p->Jh;
-  a.Rp = t->Rp;
-  a.Nrows = kForward ? t->Nf : t->Np;
+  TcArgs a = tc_args(p, t, kForward, nf);
   a.Nsub = c.Nsub;
   a.stages = c.stages;
   a.tmem_cols = tmem_cols_for(2 * c.Nsub);
   a.out = out;
-  a.err = t->d_err;
+  if (kForward) {
+    a.G = src;
+  } else {
+    a.in = one_seg(src, nf);
+    a.vec = tc_vec_input(p, a.in);
+  }
   dim3 grid(ceil_div(2 * nf, 128), p->lw, c.nsplit);
-  const CUtensorMap& ah = kForward ? t->tAfh : t->tAih;
-  const CUtensorMap& al = kForward ? t->tAfl : t->tAil;
   constexpr int kReps = 3;
   for (int r = 0; r <= kReps; ++r) {
     if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
-    legendre_tc_kernel<kForward><<<grid, kTcThreads, c.smem, 0>>>(ah, al, bh, bl, a);
+    legendre_tc_kernel<kForward><<<grid, kTcThreads, c.smem, 0>>>(bh, bl, a);
     DINO_TRY(check_launch("legendre_tc (autotune)"));
   }
   DINO_CHECK_CUDA(cudaEventRecord(e1, 0));
@@ -695,15 +821,18 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf, fl
 }
 
 // Times every candidate shape of both directions on this plan's tables with
-// an L2-sized batch (the chunk the transforms launch) and keeps the fastest.
+// the chunk that the transforms launch for large batches, and keeps the
+// fastest.
 static int tc_autotune(dino_plan* p, TcTables* t) {
-  const size_t per_field = (size_t)p->M * p->J * sizeof(float);
-  int nf = (int)((48ull << 20) / (per_field ? per_field : 1));
-  nf = nf < 1 ? 1 : nf;
-  nf = nf > t->cap ? t->cap : nf;
+  // The chunk that a large batch is transformed in.
+  const int nf = l2_chunk(p, 1 << 20, p->max_fields);
   t->tuned_fields = nf;
-  float* fwd_out = nullptr;
-  DINO_CHECK_CUDA(cudaMalloc(&fwd_out, sizeof(float) * (size_t)nf * p->M * p->L));
+  // Zero inputs: modal [nf][M][L] here, Fourier [nf][M][J] in the workspace.
+  float* modal = nullptr;
+  const size_t modal_bytes = sizeof(float) * (size_t)nf * p->M * p->L;
+  DINO_CHECK_CUDA(cudaMalloc(&modal, modal_bytes));
+  DINO_CHECK_CUDA(cudaMemset(modal, 0, modal_bytes));
+  DINO_CHECK_CUDA(cudaMemset(p->d_work, 0, sizeof(float) * (size_t)nf * p->M * p->J));
   cudaEvent_t e0, e1;
   DINO_CHECK_CUDA(cudaEventCreate(&e0));
   DINO_CHECK_CUDA(cudaEventCreate(&e1));
@@ -714,8 +843,9 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
     TcShape pick = cands.front();
     for (const TcShape& c : cands) {
       float us = 0.f;
-      const int rc = forward ? tc_time_shape<true>(p, t, c, nf, fwd_out, e0, e1, &us)
-                             : tc_time_shape<false>(p, t, c, nf, p->d_work, e0, e1, &us);
+      const int rc = forward
+                         ? tc_time_shape<true>(p, t, c, nf, p->d_work, modal, e0, e1, &us)
+                         : tc_time_shape<false>(p, t, c, nf, modal, p->d_work, e0, e1, &us);
       if (rc != DINO_OK) return rc;
       if (us < best) {
         best = us;
@@ -748,7 +878,7 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
   if (rc == DINO_OK) rc = tune(true);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(fwd_out);
+  cudaFree(modal);
   if (rc != DINO_OK) return rc;
   return tc_status(p);
 }
@@ -778,45 +908,22 @@ int tc_tables_build(dino_plan* p) {
   t->Np = round_up(p->Jh, 16);
   t->Kj = round_up(p->Jh, 64);
   t->Nf = round_up(half_l, 16);
-  // Fields per launch: A operands at most ~256 MiB each direction.
-  const size_t per_field = (size_t)p->lw * 2 * 2 * (t->Kp + t->Kj) * 2 * sizeof(bf16);
-  int cap = (int)((512ull << 20) / (per_field ? per_field : 1));
-  if (cap > p->max_fields) cap = p->max_fields;
-  if (cap < 1) cap = 1;
-  t->cap = cap;
-  t->Rp = round_up(2 * cap, 128);
   const size_t lw2 = (size_t)p->lw * 2;
   const size_t nBi = lw2 * t->Np * t->Kp, nBf = lw2 * t->Nf * t->Kj;
-  const size_t nAi = lw2 * t->Rp * t->Kp, nAf = lw2 * t->Rp * t->Kj;
   DINO_CHECK_CUDA(cudaMalloc(&t->Bih, nBi * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMalloc(&t->Bil, nBi * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMalloc(&t->Bfh, nBf * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMalloc(&t->Bfl, nBf * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Aih, nAi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Ail, nAi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Afh, nAf * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Afl, nAf * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMemset(t->Bih, 0, nBi * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMemset(t->Bil, 0, nBi * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMemset(t->Bfh, 0, nBf * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMemset(t->Bfl, 0, nBf * sizeof(bf16)));
-  // The A slabs are rewritten by every call; zero them once so that rows
-  // past a short batch hold finite values.
-  DINO_CHECK_CUDA(cudaMemset(t->Aih, 0, nAi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Ail, 0, nAi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Afh, 0, nAf * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Afl, 0, nAf * sizeof(bf16)));
   DINO_CHECK_CUDA(cudaMalloc(&t->d_err, sizeof(int)));
   DINO_CHECK_CUDA(cudaMemset(t->d_err, 0, sizeof(int)));
   dim3 grid(ceil_div(p->Jh, 128), p->lw);
   tc_table_kernel<<<grid, 128>>>(p->lw, p->L, p->Jh, p->d_x64, t->Kp, t->Np, t->Kj, t->Nf,
                                  t->Bih, t->Bil, t->Bfh, t->Bfl);
   DINO_TRY(check_launch("tc_table"));
-  const long long rowsA = (long long)lw2 * t->Rp;
-  DINO_TRY(make_map(&t->tAih, t->Aih, t->Kp, rowsA, 128));
-  DINO_TRY(make_map(&t->tAil, t->Ail, t->Kp, rowsA, 128));
-  DINO_TRY(make_map(&t->tAfh, t->Afh, t->Kj, rowsA, 128));
-  DINO_TRY(make_map(&t->tAfl, t->Afl, t->Kj, rowsA, 128));
   DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kTcSmemLimit));
@@ -834,10 +941,6 @@ void tc_tables_free(dino_plan* p) {
   cudaFree(t->Bil);
   cudaFree(t->Bfh);
   cudaFree(t->Bfl);
-  cudaFree(t->Aih);
-  cudaFree(t->Ail);
-  cudaFree(t->Afh);
-  cudaFree(t->Afl);
   cudaFree(t->d_err);
   delete t;
   p->tc = nullptr;
@@ -849,86 +952,31 @@ static int tmem_cols_for(int cols) {
   return c;
 }
 
-// Rows of one operand-slab half (a multiple of the 128-row MMA tile).
-static int tc_slot_rows(const TcTables* t) { return (t->Rp / 2) / 128 * 128; }
-
-int tc_slot_fields(dino_plan* p) {
-  return p->tc ? tc_slot_rows(p->tc) / 2 : (1 << 30);
-}
-
 int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
-                        cudaStream_t st, int slot) {
+                        cudaStream_t st) {
   TcTables* t = p->tc;
   DINO_REQUIRE(t, DINO_ERR_ARG, "plan has no tensor-core tables");
-  const size_t ms = (size_t)p->M * p->L, fs = (size_t)p->M * p->J;
-  const int cap = slot < 0 ? t->cap : tc_slot_rows(t) / 2;
-  const int roff = slot > 0 ? tc_slot_rows(t) : 0;
-  DINO_REQUIRE(cap >= 1, DINO_ERR_UNSUPPORTED, "operand slab too small for two slots");
-  for (int f0 = 0; f0 < nf; f0 += cap) {
-    const int n = nf - f0 < cap ? nf - f0 : cap;
-    Segs sub = seg_offset(in, f0, n, ms);
-    const int max_rows = 2 * n;
-    dim3 g1((unsigned)(((size_t)max_rows * (t->Kp / 8) + 255) / 256), p->lw);
-    tc_split_inverse_kernel<<<g1, 256, 0, st>>>(sub, n, p->M, p->L, t->Rp, t->Kp, roff,
-                                                t->Aih, t->Ail);
-    DINO_TRY(check_launch("tc_split_inverse"));
-    TcArgs a{};
-    a.nf = n;
-    a.M = p->M;
-    a.L = p->L;
-    a.J = p->J;
-    a.Jh = p->Jh;
-    a.Rp = t->Rp;
-    a.roff = roff;
-    a.Nrows = t->Np;
-    a.Nsub = t->Nsub_inv;
-    a.stages = t->stages_inv;
-    a.tmem_cols = tmem_cols_for(2 * t->Nsub_inv);
-    a.out = out + f0 * fs;
-    a.err = t->d_err;
-    dim3 g2(ceil_div(max_rows, 128), p->lw, t->nsplit_inv);
-    legendre_tc_kernel<false><<<g2, kTcThreads, t->smem_inv, st>>>(t->tAih, t->tAil, t->tBih,
-                                                                   t->tBil, a);
-    DINO_TRY(check_launch("legendre_tc_inverse"));
-  }
-  return DINO_OK;
+  if (nf == 0) return DINO_OK;
+  TcArgs a = tc_args(p, t, false, nf);
+  a.in = in;
+  a.vec = tc_vec_input(p, in);
+  a.out = out;
+  dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_inv);
+  legendre_tc_kernel<false><<<grid, kTcThreads, t->smem_inv, st>>>(t->tBih, t->tBil, a);
+  return check_launch("legendre_tc_inverse");
 }
 
 int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
-                        cudaStream_t st, int slot) {
+                        cudaStream_t st) {
   TcTables* t = p->tc;
   DINO_REQUIRE(t, DINO_ERR_ARG, "plan has no tensor-core tables");
-  const size_t ms = (size_t)p->M * p->L, fs = (size_t)p->M * p->J;
-  const int cap = slot < 0 ? t->cap : tc_slot_rows(t) / 2;
-  const int roff = slot > 0 ? tc_slot_rows(t) : 0;
-  DINO_REQUIRE(cap >= 1, DINO_ERR_UNSUPPORTED, "operand slab too small for two slots");
-  for (int f0 = 0; f0 < nf; f0 += cap) {
-    const int n = nf - f0 < cap ? nf - f0 : cap;
-    const int max_rows = 2 * n;
-    dim3 g1((unsigned)(((size_t)max_rows * (t->Kj / 8) + 255) / 256), p->lw);
-    tc_fold_forward_kernel<<<g1, 256, 0, st>>>(G + f0 * fs, n, p->M, p->J, p->Jh, t->Rp, t->Kj,
-                                               roff, t->Afh, t->Afl);
-    DINO_TRY(check_launch("tc_fold_forward"));
-    TcArgs a{};
-    a.nf = n;
-    a.M = p->M;
-    a.L = p->L;
-    a.J = p->J;
-    a.Jh = p->Jh;
-    a.Rp = t->Rp;
-    a.roff = roff;
-    a.Nrows = t->Nf;
-    a.Nsub = t->Nsub_fwd;
-    a.stages = t->stages_fwd;
-    a.tmem_cols = tmem_cols_for(2 * t->Nsub_fwd);
-    a.out = out + f0 * ms;
-    a.err = t->d_err;
-    dim3 g2(ceil_div(max_rows, 128), p->lw, t->nsplit_fwd);
-    legendre_tc_kernel<true><<<g2, kTcThreads, t->smem_fwd, st>>>(t->tAfh, t->tAfl, t->tBfh,
-                                                                  t->tBfl, a);
-    DINO_TRY(check_launch("legendre_tc_forward"));
-  }
-  return DINO_OK;
+  if (nf == 0) return DINO_OK;
+  TcArgs a = tc_args(p, t, true, nf);
+  a.G = G;
+  a.out = out;
+  dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_fwd);
+  legendre_tc_kernel<true><<<grid, kTcThreads, t->smem_fwd, st>>>(t->tBfh, t->tBfl, a);
+  return check_launch("legendre_tc_forward");
 }
 
 int tc_status(dino_plan* p) {

@@ -15,6 +15,8 @@
 
 #include <cmath>
 
+#include <algorithm>
+
 #include "dino_internal.cuh"
 
 namespace dino {
@@ -306,9 +308,9 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 }
 
 int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
-                     cudaStream_t st, int slot) {
+                     cudaStream_t st) {
   if (p->precision == DINO_PREC_BF16X3)
-    return tc_legendre_inverse(p, in, out, nf, st, slot);
+    return tc_legendre_inverse(p, in, out, nf, st);
   dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
       in, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
@@ -316,9 +318,9 @@ int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
 }
 
 int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
-                     cudaStream_t st, int slot) {
+                     cudaStream_t st) {
   if (p->precision == DINO_PREC_BF16X3)
-    return tc_legendre_forward(p, G, out, nf, st, slot);
+    return tc_legendre_forward(p, G, out, nf, st);
   dim3 grid(ceil_div(p->L, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_forward_simt<<<grid, kLegThreads, 0, st>>>(
       G, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
@@ -761,21 +763,27 @@ int fourier_forward(dino_plan* p, const float* nodal, float* F, int nf,
 
 // Fields per launch such that the intermediate Fourier coefficients of one
 // chunk (fields x M x J floats) stay resident in L2 between the Legendre and
-// FFT kernels; chunks are balanced.
-static int l2_chunk(dino_plan* p, int nf, int work_fields) {
+// FFT kernels; chunks are balanced, and on the tensor-core path whole
+// 128-row MMA tiles (64 fields) where the cap allows.
+int l2_chunk(dino_plan* p, int nf, int work_fields) {
   const size_t per_field = (size_t)p->M * p->J * sizeof(float);
   int cap = (int)((48ull << 20) / (per_field ? per_field : 1));
   if (cap < 1) cap = 1;
   if (cap > work_fields) cap = work_fields;
+  if (p->precision == DINO_PREC_BF16X3 && cap >= 64) {
+    cap = cap / 64 * 64;
+    const int chunks = (nf + cap - 1) / cap;
+    const int even = (nf + chunks - 1) / chunks;
+    return std::min(cap, (even + 63) / 64 * 64);
+  }
   const int chunks = (nf + cap - 1) / cap;
   return (nf + chunks - 1) / chunks;
 }
 
 // Chunks alternate between the caller's stream and the plan's side stream
-// when two of them fit in the workspace (and in the tensor-core operand
-// slabs): each stream has its own half, both chunks' intermediates stay in
-// L2, and one chunk's kernels fill the SMs the other leaves idle in its
-// waves' tails.  The side stream forks from and joins back into the
+// when two of them fit in the workspace: each stream has its own half, both
+// chunks' intermediates stay in L2, and one chunk's kernels fill the SMs the
+// other leaves idle in its waves' tails.  The side stream forks from and joins back into the
 // caller's stream with events, so the pattern also records into CUDA graphs.
 struct ChunkRun {
   dino_plan* p;
@@ -787,8 +795,7 @@ struct ChunkRun {
   ChunkRun(dino_plan* p_, cudaStream_t st_, float* work_, int chunk, int nf,
            int work_fields)
       : p(p_), st(st_), work(work_), work_stride((size_t)chunk * p_->M * p_->J) {
-    dual = p->side && nf > chunk && 2 * chunk <= work_fields &&
-           chunk <= tc_slot_fields(p);
+    dual = p->side && nf > chunk && 2 * chunk <= work_fields;
   }
   int begin() {
     if (!dual) return DINO_OK;
@@ -816,7 +823,7 @@ int sht_inverse_segs(dino_plan* p, const Segs& in, float* out, int nf,
   for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
     Segs sub = seg_offset(in, f0, n, ms);
-    DINO_TRY(legendre_inverse(p, sub, run.buf(c), n, run.stream(c), run.slot(c)));
+    DINO_TRY(legendre_inverse(p, sub, run.buf(c), n, run.stream(c)));
     DINO_TRY(fourier_inverse(p, run.buf(c), out + f0 * ns, n, false, run.stream(c)));
   }
   return run.end();
@@ -831,7 +838,7 @@ int sht_forward_to(dino_plan* p, const float* nodal, float* out, int nf,
   for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
     DINO_TRY(fourier_forward(p, nodal + f0 * ns, run.buf(c), n, true, run.stream(c)));
-    DINO_TRY(legendre_forward(p, run.buf(c), out + f0 * ms, n, run.stream(c), run.slot(c)));
+    DINO_TRY(legendre_forward(p, run.buf(c), out + f0 * ms, n, run.stream(c)));
   }
   return run.end();
 }
@@ -849,8 +856,7 @@ int sht_inverse_adjoint_to(dino_plan* p, const float* nodal_ct, float* modal_ct,
   for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
     DINO_TRY(fourier_forward(p, nodal_ct + f0 * ns, run.buf(c), n, false, run.stream(c)));
-    DINO_TRY(legendre_forward(p, run.buf(c), modal_ct + f0 * ms, n, run.stream(c),
-                              run.slot(c)));
+    DINO_TRY(legendre_forward(p, run.buf(c), modal_ct + f0 * ms, n, run.stream(c)));
   }
   return run.end();
 }
@@ -864,7 +870,7 @@ int sht_forward_adjoint_to(dino_plan* p, const float* modal_ct, float* nodal_ct,
   for (int c = 0, f0 = 0; f0 < nf; ++c, f0 += chunk) {
     int n = nf - f0 < chunk ? nf - f0 : chunk;
     DINO_TRY(legendre_inverse(p, one_seg(modal_ct + f0 * ms, n), run.buf(c), n,
-                              run.stream(c), run.slot(c)));
+                              run.stream(c)));
     DINO_TRY(fourier_inverse(p, run.buf(c), nodal_ct + f0 * ns, n, true, run.stream(c)));
   }
   return run.end();
