@@ -211,8 +211,9 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
+// Issues a 16-column TMEM load (32 lanes x 32 bits); the values are valid
+// after tmem_wait16 / tmem_tie16 on the same registers.
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
       "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
@@ -220,15 +221,43 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
         "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
         "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void split_bf16(float v, bf16& hi, bf16& lo) {
-  hi = __float2bfloat16_rn(v);
-  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+// Waits for this thread's TMEM loads; the register operands order every
+// later use of r after the wait.
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
 }
+
+// Orders the uses of a second load's registers after a preceding tmem_wait16
+// (volatile asm statements keep their order).
+__device__ __forceinline__ void tmem_tie16(uint32_t (&r)[16]) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]));
+}
+
+// Both parities' 16 columns at c0 (parity 1 only when `odd`), one wait.
+__device__ __forceinline__ void tmem_ld_pair(uint32_t c0, uint32_t c1, bool odd,
+                                             float (&e)[16], float (&o)[16]) {
+  uint32_t re[16], ro[16];
+  tmem_ld16_issue(c0, re);
+  if (odd) tmem_ld16_issue(c1, ro);
+  tmem_wait16(re);
+  if (odd) tmem_tie16(ro);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    e[i] = __uint_as_float(re[i]);
+    o[i] = odd ? __uint_as_float(ro[i]) : 0.f;
+  }
+}
+
 
 __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
   if (m == 0) {
@@ -248,8 +277,14 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int c) {
   return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
 }
 
-__device__ __forceinline__ uint32_t pack_bf16x2(bf16 a, bf16 b) {
-  return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+// hi = bf16x2(x0, x1) and lo = bf16x2 of the remainders x - hi, each rounded
+// to nearest: one packed conversion per pair for each half.
+__device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+  hi = reinterpret_cast<const uint32_t&>(h);
+  lo = reinterpret_cast<const uint32_t&>(l);
 }
 
 // Splits eight values v[s0], v[s0 + st], ... into hi / lo bf16 and writes
@@ -259,13 +294,8 @@ __device__ __forceinline__ void put_split8(const float (&v)[N], int s0, int st,
                                            uint8_t* hi, uint8_t* lo, uint32_t off) {
   uint32_t h[4], l[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    bf16 h0, l0, h1, l1;
-    split_bf16(v[s0 + (2 * i) * st], h0, l0);
-    split_bf16(v[s0 + (2 * i + 1) * st], h1, l1);
-    h[i] = pack_bf16x2(h0, h1);
-    l[i] = pack_bf16x2(l0, l1);
-  }
+  for (int i = 0; i < 4; ++i)
+    split_pair(v[s0 + (2 * i) * st], v[s0 + (2 * i + 1) * st], h[i], l[i]);
   *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
   *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
@@ -583,13 +613,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       const bool vec = (a.J & 3) == 0;
       for (int c = half; c < a.Nsub / 16; c += 2) {
         float e[16], od[16];
-        tmem_ld16(lane_base + c * 16, e);
-        if (n_par[1] > 0) {
-          tmem_ld16(lane_base + acc_cols + c * 16, od);
-        } else {
-#pragma unroll
-          for (int t = 0; t < 16; ++t) od[t] = 0.f;
-        }
+        tmem_ld_pair(lane_base + c * 16, lane_base + acc_cols + c * 16, n_par[1] > 0, e, od);
         // stage[r][t] = E + O at j = 16c + t; stage[r][16 + t] = E - O at
         // j = J - 16(c+1) + t (the mirrored block, ascending).
 #pragma unroll
@@ -646,13 +670,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       const int nchunks = (max(cnt[0], cnt[1]) + 15) / 16;
       for (int c = half; c < nchunks; c += 2) {
         float e[16], od[16];
-        tmem_ld16(lane_base + c * 16, e);
-        if (cnt[1] > 0) {
-          tmem_ld16(lane_base + acc_cols + c * 16, od);
-        } else {
-#pragma unroll
-          for (int t = 0; t < 16; ++t) od[t] = 0.f;
-        }
+        tmem_ld_pair(lane_base + c * 16, lane_base + acc_cols + c * 16, cnt[1] > 0, e, od);
         // Interleave parities: l = m + 32c + 2t + p.
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
