@@ -493,19 +493,20 @@ template <int kMaxRows>
 __device__ __forceinline__ void stage_tile(const float* __restrict__ src, int rows,
                                            int J, int ncol, float* dst) {
   if ((J & 3) == 0 && ncol == kFftJS) {
-    constexpr int kChunks = (kMaxRows * 4 + kFftThreads - 1) / kFftThreads;
+    constexpr int kQ = kFftJS / 4;  // float4 per row
+    constexpr int kChunks = (kMaxRows * kQ + kFftThreads - 1) / kFftThreads;
     float4 v[kChunks];
 #pragma unroll
     for (int i = 0; i < kChunks; ++i) {
       const int t = threadIdx.x + i * kFftThreads;
-      const int r = t >> 2, q = t & 3;
+      const int r = t / kQ, q = t % kQ;
       v[i] = (r < rows) ? *reinterpret_cast<const float4*>(src + (size_t)r * J + 4 * q)
                         : make_float4(0.f, 0.f, 0.f, 0.f);
     }
 #pragma unroll
     for (int i = 0; i < kChunks; ++i) {
       const int t = threadIdx.x + i * kFftThreads;
-      if ((t >> 2) < rows) reinterpret_cast<float4*>(dst)[t] = v[i];
+      if (t / kQ < rows) reinterpret_cast<float4*>(dst)[t] = v[i];
     }
   } else {
     for (int t = threadIdx.x; t < rows * kFftJS; t += kFftThreads) {
