@@ -152,6 +152,36 @@ def test_moist_explicit_terms_with_tracers_match_oracle():
   assert_state(got, ref, 2e-5)
 
 
+@pytest.mark.parametrize('moist', [False, True])
+def test_explicit_terms_24_levels_match_oracle(moist):
+  # With 24 levels the nodal column kernel splits every column into four
+  # level chunks whose column totals and sigma-dot prefix sums are exchanged
+  # through shared memory (two columns per thread dry, one with tracers).
+  # The FP32 error of the vorticity tendency is spread evenly over the levels
+  # (measured 0.5-2.6e-5 relative to its maximum, no peak at the chunk
+  # boundaries 6, 12, 18), hence 5e-5 here against 2e-5 at 6 levels.
+  kw = dict(tracers=_tracers, humidity='specific_humidity') if moist else {}
+  og, oeq, st, g, eq = make(layers=24, **kw)
+  got = eq.explicit_terms(to_state(st))
+  ref = oeq.explicit_terms(st)
+  assert_state(got, ref, 5e-5)
+
+
+def test_level_chunks_agree_across_batch_sizes():
+  # T42 / 24 levels: one member runs four level chunks per column, a batch of
+  # sixteen two (the chunk count follows the available parallelism); the
+  # chunked prefix sums may differ from each other only by FP32 rounding.
+  og, oeq, st, g, eq = make('T42', layers=24)
+  s1 = to_state(st)
+  batch = pe.State(*[torch.stack([getattr(s1, k)] * 16) for k in KEYS])
+  ob = eq.explicit_terms(batch)
+  o1 = eq.explicit_terms(s1)
+  for k in KEYS:
+    a, b = getattr(ob, k)[5].double(), getattr(o1, k).double()
+    err = float((a - b).abs().max() / b.abs().max())
+    assert err < 1e-6, (k, err)
+
+
 def test_dry_tracer_advection_matches_oracle():
   og, oeq, st, g, eq = make(tracers=_tracers)
   got = eq.explicit_terms(to_state(st))
