@@ -855,32 +855,43 @@ struct NodalAdjArgs {
   float* xbar;        // cotangents of the nodal inputs (nodal-buffer layout)
 };
 
-// Five CTAs per SM (96 registers, no spills).
+// Five CTAs per SM (96 registers, no spills).  The per-level coefficients
+// come from the packed table in shared memory (kLevPack, as in
+// pe_nodal_kernel); plane offsets are 32-bit (the nodal and forward-input
+// buffers hold fewer than 2^32 floats, checked on the host).
 __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A) {
+  extern __shared__ float4 s_lev[];  // [K][kLevPack / 4]
   const NodalArgs& a = A.f;
-  const size_t IJ = (size_t)a.I * a.J;
-  const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int K = a.K;
+  for (int i = threadIdx.x; i < K * (kLevPack / 4); i += blockDim.x)
+    s_lev[i] = reinterpret_cast<const float4*>(a.levpack)[i];
+  __syncthreads();
+  const unsigned IJ = (unsigned)a.I * (unsigned)a.J;
+  const unsigned col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= IJ) return;
   const int mb = blockIdx.y;
-  const int K = a.K;
-  const int j = col % a.J;
+  const int j = (int)(col % (unsigned)a.J);
   const float sec2 = a.lat[j];
   const float fcor = a.lat[a.J + j];
-  const float* dsig = a.lev + a.lo.dsig;
-  const float* c2ci = a.lev + a.lo.c2ci;
-  const float* alpha = a.lev + a.lo.alpha;
-  const float* tref = a.lev + a.lo.tref;
-  const float* sumsig = a.lev + a.lo.sumsig;
-  const float* trd = a.lev + a.lo.trefdiff;
+  // Per-level coefficients (see kLevPack).
+  auto dsig = [&](int k) { return s_lev[4 * k].x; };
+  auto invds = [&](int k) { return s_lev[4 * k].y; };
+  auto sumsig = [&](int k) { return s_lev[4 * k].z; };
+  auto tref = [&](int k) { return s_lev[4 * k].w; };
+  auto c2ci = [&](int k) { return s_lev[4 * k + 1].x; };
+  auto alpha = [&](int k) { return s_lev[4 * k + 1].z; };
+  auto alpha_up = [&](int k) { return s_lev[4 * k + 1].w; };
+  auto trd = [&](int k) { return s_lev[4 * k + 3].x; };
   const float* nod = a.nod;
   const float* fb = A.fbar;
   float* xb = A.xbar;
-#define NOD(p, k) nod[pl(p, mb, K, k) * IJ + col]
-#define FB(p, k) fb[pl(p, mb, K, k) * IJ + col]
-#define XB(p, k) xb[pl(p, mb, K, k) * IJ + col]
+  const unsigned mK = (unsigned)mb * (unsigned)K;
+#define NOD(p, k) nod[((unsigned)(p) + mK + (unsigned)(k)) * IJ + col]
+#define FB(p, k) fb[((unsigned)(p) + mK + (unsigned)(k)) * IJ + col]
+#define XB(p, k) xb[((unsigned)(p) + mK + (unsigned)(k)) * IJ + col]
   const bool moist = a.hum >= 0;
-  const float gx = nod[((size_t)a.p_gx + mb) * IJ + col];
-  const float gy = nod[((size_t)a.p_gy + mb) * IJ + col];
+  const float gx = nod[((unsigned)a.p_gx + mb) * IJ + col];
+  const float gy = nod[((unsigned)a.p_gy + mb) * IJ + col];
   const float ra = a.Rv_over_R - 1.f;
   const float rb = a.Cpv_over_Cp - 1.f;
   const float rc = a.Rv_over_R - a.Cpv_over_Cp;
@@ -891,23 +902,25 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
   for (int k = 0; k < K; ++k) {
     const float u = NOD(a.p_u, k), v = NOD(a.p_v, k), d = NOD(a.p_div, k);
     const float ugl = (u * gx + v * gy) * sec2;
-    Fe += ugl * dsig[k];
-    Ff += (d + ugl) * dsig[k];
-    Su += u * dsig[k];
-    Sv += v * dsig[k];
+    const float ds = dsig(k);
+    Fe += ugl * ds;
+    Ff += (d + ugl) * ds;
+    Su += u * ds;
+    Sv += v * ds;
     if (moist) Gh += FB(a.o_gh, k);
   }
   float laplnps = 0.f;
-  if (moist) laplnps = nod[((size_t)a.p_laplnps + mb) * IJ + col];
-  float lnps_n = 0.f, sin2 = 0.f, cos2 = 0.f;
+  if (moist) laplnps = nod[((unsigned)a.p_laplnps + mb) * IJ + col];
+  float lnps_n = 0.f, sin2 = 0.f, cos2 = 0.f, hs_e = 0.f;
   if (a.hs) {
-    lnps_n = nod[((size_t)a.p_lnps + mb) * IJ + col];
+    lnps_n = nod[((unsigned)a.p_lnps + mb) * IJ + col];
     sin2 = a.lat[2 * a.J + j];
     cos2 = a.lat[3 * a.J + j];
+    hs_e = expf(kap * lnps_n);  // ps^kappa; (p / p0)^kappa = (sigma / p0)^kappa ps^kappa
   }
 
   float gxb = 0.f, gyb = 0.f, laplnpsb = 0.f, lnpsb = 0.f;
-  float Feb = -fb[((size_t)a.o_lnps + mb) * IJ + col], Ffb = 0.f;
+  float Feb = -fb[((unsigned)a.o_lnps + mb) * IJ + col], Ffb = 0.f;
   // Window: values of level k+1.
   float u_n = 0.f, v_n = 0.f, T_n = 0.f;
   float Vu_n = 0.f, Vv_n = 0.f, VT_n = 0.f, Tnb_n = 0.f;
@@ -932,9 +945,10 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     }
     const float ugl = (u * gx + v * gy) * sec2;
     const float fe_k = fe, ff_k = ff;
-    const float fe_km = fe_k - ugl * dsig[k];
-    const float ff_km = ff_k - (d + ugl) * dsig[k];
-    const float inv_ds = 1.f / dsig[k];
+    const float fe_km = fe_k - ugl * dsig(k);
+    const float ff_km = ff_k - (d + ugl) * dsig(k);
+    const float inv_ds = invds(k);
+    const float trk = tref(k);
 
     const float Aub = FB(a.o_Au, k), Avb = FB(a.o_Av, k), KEb = FB(a.o_KE, k);
     const float uTb = FB(a.o_uT, k), vTb = FB(a.o_vT, k), Tnb = FB(a.o_Tn, k);
@@ -945,7 +959,7 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     float ub = tv * sec2 * Avb + u * sec2 * KEb + T * sec2 * uTb;
     float vb = -tv * sec2 * Aub + v * sec2 * KEb + T * sec2 * vTb;
     if (a.hs) {
-      const float kv = a.lev[a.lo.kv + k];
+      const float kv = s_lev[4 * k + 2].x;
       ub += kv * sec2 * Aub;
       vb += kv * sec2 * Avb;
     }
@@ -956,9 +970,9 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     gyb += rt * sec2 * Avb;
     float db = T * Tnb;
     // Adiabatic term kappa (Tref (ugl - ge) + P (ugl - gf)).
-    const float gf = (alpha[k] * ff_k + (k > 0 ? alpha[k - 1] * ff_km : 0.f)) * inv_ds;
-    float uglb = kap * tref[k] * Tnb;
-    const float geb = -kap * tref[k] * Tnb;
+    const float gf = (alpha(k) * ff_k + alpha_up(k) * ff_km) * inv_ds;
+    float uglb = kap * trk * Tnb;
+    const float geb = -kap * trk * Tnb;
     float gfb;
     if (!moist) {
       Tb += kap * (ugl - gf) * Tnb;
@@ -966,9 +980,9 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
       gfb = -kap * T * Tnb;
     } else {
       const float den = 1.f + rb * q_h;
-      const float P = (T * (1.f + ra * q_h) + tref[k] * rc * q_h) / den;
+      const float P = (T * (1.f + ra * q_h) + trk * rc * q_h) / den;
       Tb += kap * (ugl - gf) * Tnb * (1.f + ra * q_h) / den;
-      qhb += kap * (ugl - gf) * Tnb * (T * (ra - rb) + tref[k] * rc) / (den * den);
+      qhb += kap * (ugl - gf) * Tnb * (T * (ra - rb) + trk * rc) / (den * den);
       uglb += kap * P * Tnb;
       gfb = -kap * P * Tnb;
     }
@@ -992,7 +1006,7 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     if (moist) {
       const float gqx = NOD(a.p_gqx, k), gqy = NOD(a.p_gqy, k);
       const float vhb = FB(a.o_vh, k), dhb = FB(a.o_dh, k), ghb = FB(a.o_gh, k);
-      const float coef = tref[k] * a.Rv_minus_R;
+      const float coef = trk * a.Rv_minus_R;
       gxb += coef * sec2 * (gqy * vhb + gqx * dhb);
       gyb += coef * sec2 * (-gqx * vhb + gqy * dhb);
       XB(a.p_gqx, k) = coef * sec2 * (-gy * vhb + gx * dhb);
@@ -1002,9 +1016,9 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
       // Geopotential of the virtual-temperature difference.
       SGh += ghb;
       const float above = Gh - SGh;  // sum of the cotangents of levels < k
-      const float tdb = a.R * alpha[k] * ghb +
-                        (k > 0 ? a.R * (alpha[k] + alpha[k - 1]) * above : 0.f);
-      qhb += (T + tref[k]) * ra * tdb;
+      const float tdb = a.R * alpha(k) * ghb +
+                        (k > 0 ? a.R * (alpha(k) + alpha_up(k)) * above : 0.f);
+      qhb += (T + trk) * ra * tdb;
       Tb += q_h * ra * tdb;
 #pragma unroll
       for (int t = 0; t < kMaxTracers; ++t)
@@ -1012,11 +1026,10 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     }
     if (a.hs) {
       const float hsTb = FB(a.o_hsT, k);
-      const float sig = a.lev[a.lo.sigma + k];
-      const float cutoff = fmaxf(0.f, (sig - a.hs_sigma_b) / (1.f - a.hs_sigma_b));
-      const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (cutoff * cos2 * cos2);
-      const float lp = a.lev[a.lo.logsp0 + k] + lnps_n;  // log(p / p0)
-      const float pk = expf(kap * lp);
+      const float4 c2 = s_lev[4 * k + 2];  // kv, cutoff, (sigma/p0)^kappa, log(sigma/p0)
+      const float kt = a.hs_ka + (a.hs_ks - a.hs_ka) * (c2.y * cos2 * cos2);
+      const float lp = c2.w + lnps_n;  // log(p / p0)
+      const float pk = c2.z * hs_e;
       const float B = a.hs_maxT - a.hs_dTy * sin2 - a.hs_dThz * lp * cos2;
       Tb += -kt * hsTb;
       if (pk * B > a.hs_minT) lnpsb += kt * hsTb * pk * (kap * B - a.hs_dThz * cos2);
@@ -1024,13 +1037,14 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     const float Vu = a.vadv ? -sec2 * Aub : 0.f;
     const float Vv = a.vadv ? -sec2 * Avb : 0.f;
     const float VT = a.vadv ? Tnb : 0.f;
-    float fe_b = alpha[k] * inv_ds * geb + carry_fe;
-    float ff_b = alpha[k] * inv_ds * gfb + carry_ff;
+    float fe_b = alpha(k) * inv_ds * geb + carry_fe;
+    float ff_b = alpha(k) * inv_ds * gfb + carry_ff;
     if (has_next) {
       // Half level k+1/2.
-      const float c = c2ci[k];
+      const float c = c2ci(k);
+      const float ssk = sumsig(k);
       if (a.vadv) {
-        const float wf = sumsig[k] * Ff - ff_k;
+        const float wf = ssk * Ff - ff_k;
         float wfb = 0.f;
         auto half = [&](float xc, float xn, float Vc, float Vn, float& xbc, float& xbn) {
           const float vs = Vc + Vn;
@@ -1046,12 +1060,12 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
         for (int t = 0; t < kMaxTracers; ++t)
           if (t < a.nT) half(q[t], q_n[t], Vq[t], Vq_n[t], qb[t], qb_n[t]);
         ff_b -= wfb;
-        Ffb += sumsig[k] * wfb;
+        Ffb += ssk * wfb;
       }
       if (a.tref_varies) {
-        const float web = -0.5f * trd[k] * (Tnb + Tnb_n);
+        const float web = -0.5f * trd(k) * (Tnb + Tnb_n);
         fe_b -= web;
-        Feb += sumsig[k] * web;
+        Feb += ssk * web;
       }
       // Level k+1 has all its contributions.
       XB(a.p_u, k + 1) = ub_n;
@@ -1063,16 +1077,16 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
     }
     Se += fe_b;
     Sf += ff_b;
-    uglb += dsig[k] * (Se + Sf);
-    db += dsig[k] * Sf;
+    uglb += dsig(k) * (Se + Sf);
+    db += dsig(k) * Sf;
     ub += gx * sec2 * uglb;
     vb += gy * sec2 * uglb;
     gxb += u * sec2 * uglb;
     gyb += v * sec2 * uglb;
     XB(a.p_vort, k) = zb;
     XB(a.p_div, k) = db;
-    carry_fe = k > 0 ? alpha[k - 1] * inv_ds * geb : 0.f;
-    carry_ff = k > 0 ? alpha[k - 1] * inv_ds * gfb : 0.f;
+    carry_fe = alpha_up(k) * inv_ds * geb;
+    carry_ff = alpha_up(k) * inv_ds * gfb;
     u_n = u; v_n = v; T_n = T;
     Vu_n = Vu; Vv_n = Vv; VT_n = VT; Tnb_n = Tnb;
     ub_n = ub; vb_n = vb; Tb_n = Tb;
@@ -1095,16 +1109,17 @@ __global__ void __launch_bounds__(128, 5) pe_nodal_adjoint_kernel(NodalAdjArgs A
   // Pass 2: cotangents of the column totals.
   const float Ftb = Feb + Ffb;
   for (int k = 0; k < K; ++k) {
-    XB(a.p_u, k) += gx * sec2 * dsig[k] * Ftb;
-    XB(a.p_v, k) += gy * sec2 * dsig[k] * Ftb;
-    XB(a.p_div, k) += dsig[k] * Ffb;
+    const float ds = dsig(k);
+    XB(a.p_u, k) += gx * sec2 * ds * Ftb;
+    XB(a.p_v, k) += gy * sec2 * ds * Ftb;
+    XB(a.p_div, k) += ds * Ffb;
   }
   gxb += sec2 * Ftb * Su;
   gyb += sec2 * Ftb * Sv;
-  xb[((size_t)a.p_gx + mb) * IJ + col] = gxb;
-  xb[((size_t)a.p_gy + mb) * IJ + col] = gyb;
-  if (moist) xb[((size_t)a.p_laplnps + mb) * IJ + col] = laplnpsb;
-  if (a.hs) xb[((size_t)a.p_lnps + mb) * IJ + col] = lnpsb;
+  xb[((unsigned)a.p_gx + mb) * IJ + col] = gxb;
+  xb[((unsigned)a.p_gy + mb) * IJ + col] = gyb;
+  if (moist) xb[((unsigned)a.p_laplnps + mb) * IJ + col] = laplnpsb;
+  if (a.hs) xb[((unsigned)a.p_lnps + mb) * IJ + col] = lnpsb;
 #undef NOD
 #undef FB
 #undef XB
@@ -1871,6 +1886,8 @@ static int nodal_prepare(int K) {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, n));
   DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_nodal_kernel<true, 1>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, n));
+  DINO_CHECK_CUDA(cudaFuncSetAttribute(pe_nodal_adjoint_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, n));
   return DINO_OK;
 }
 
@@ -2118,7 +2135,7 @@ static int pe_explicit_vjp_impl(dino_pe* pe, const float* state, const float* tb
     a.fbar = pe->d_fwd_in;
     a.xbar = pe->d_xbar_n;
     dim3 grid(ceil_div((int)pe->IJ, 128), mem);
-    pe_nodal_adjoint_kernel<<<grid, 128, 0, st>>>(a);
+    pe_nodal_adjoint_kernel<<<grid, 128, nodal_smem(K), st>>>(a);
     DINO_TRY(check_launch("pe_nodal_adjoint"));
   }
   DINO_TRY(sht_inverse_adjoint_to(p, pe->d_xbar_n, pe->d_xbar_m, pe->n_inv,
@@ -2426,6 +2443,9 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
     pe->n_fwd = q;
   }
   const size_t ML = pe->ML, IJ = pe->IJ;
+  // The nodal kernels address these buffers with 32-bit offsets.
+  DINO_REQUIRE((uint64_t)pe->n_inv * IJ < (1ull << 32) && (uint64_t)pe->n_fwd * IJ < (1ull << 32),
+               DINO_ERR_UNSUPPORTED, "nodal buffers must hold fewer than 2^32 values");
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_aux, sizeof(float) * pe->n_aux * ML));
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_nodal, sizeof(float) * pe->n_inv * IJ));
   DINO_CHECK_CUDA(cudaMalloc(&pe->d_fwd_in, sizeof(float) * pe->n_fwd * IJ));
