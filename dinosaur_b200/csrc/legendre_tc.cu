@@ -174,6 +174,32 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm,
       : "memory");
 }
 
+// TMA tensor store of a shared-memory box (bulk async-group completion).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* tm, const void* src, int x,
+                                             int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+          reinterpret_cast<uint64_t>(tm)),
+      "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Waits until at most N of this thread's committed bulk groups still read
+// their shared-memory source.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Waits until this thread's bulk groups have completed.
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
 // 1024 bytes apart (SBO), leading offset unused for swizzled K-major.
 __device__ __forceinline__ uint64_t umma_desc_sw128(const void* p) {
@@ -311,6 +337,7 @@ struct TcArgs {
   int stages;
   int tmem_cols; // allocated TMEM columns (power of two)
   int vec;       // inverse: rows of the modal input start 16-byte aligned
+  int tma_out;   // inverse: full 16-latitude blocks leave by TMA tensor stores
   Segs in;       // inverse: modal coefficients [nf][M][L]
   const float* G;  // forward: weighted Fourier coefficients [nf][M][J]
   float* out;    // inverse: Fourier [nf][M][J]; forward: modal [nf][M][L]
@@ -467,7 +494,9 @@ __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int
 template <bool kForward>
 __global__ void __launch_bounds__(kTcThreads, 2)
 legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
-                   const __grid_constant__ CUtensorMap tBl, const __grid_constant__ TcArgs a) {
+                   const __grid_constant__ CUtensorMap tBl,
+                   const __grid_constant__ CUtensorMap tO2,
+                   const __grid_constant__ CUtensorMap tO1, const __grid_constant__ TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kMaxStages];
   __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
@@ -606,14 +635,58 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
     // quarter take alternate 16-column chunks.
     constexpr int kStride = 36;  // floats per staged row (16-byte multiple)
     const int quarter = warp & 3, half = warp >> 2;
-    float* stage = reinterpret_cast<float*>(base) + warp * 32 * kStride;
+    // Each warp owns 8 KB of the drained pipeline buffers: two TMA-store
+    // buffers (a direct and a mirrored 32 x 16 block each, the box layout of
+    // tO2 / tO1), which the row-store path reuses as its staging area.
+    float* wbuf = reinterpret_cast<float*>(base) + warp * 2048;
+    float* stage = wbuf;
     const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
     const int row0 = tile * 128 + quarter * 32;  // first row of this warp
     if (!kForward) {
       const bool vec = (a.J & 3) == 0;
+      int nb = 0;  // TMA-stored chunks of this warp (buffer nb & 1)
       for (int c = half; c < a.Nsub / 16; c += 2) {
         float e[16], od[16];
         tmem_ld_pair(lane_base + c * 16, lane_base + acc_cols + c * 16, n_par[1] > 0, e, od);
+        const int jb = lo + 16 * c;
+        const int jm = a.J - jb - 16;
+        if (a.tma_out && jb + 16 <= a.Jh && jm >= a.Jh) {
+          // Direct block j = jb .. jb+15 and mirrored block j = jm .. jm+15,
+          // both ascending, 16 floats per staged row.
+          float* sd = wbuf + (nb & 1) * 1024;
+          float* sm = sd + 512;
+          if (lane == 0) bulk_wait_read<1>();  // this buffer's store two chunks ago
+          __syncwarp();
+          float4* d4 = reinterpret_cast<float4*>(sd + lane * 16);
+          float4* m4 = reinterpret_cast<float4*>(sm + lane * 16);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            d4[i] = make_float4(e[4 * i] + od[4 * i], e[4 * i + 1] + od[4 * i + 1],
+                                e[4 * i + 2] + od[4 * i + 2], e[4 * i + 3] + od[4 * i + 3]);
+            m4[i] = make_float4(e[15 - 4 * i] - od[15 - 4 * i], e[14 - 4 * i] - od[14 - 4 * i],
+                                e[13 - 4 * i] - od[13 - 4 * i], e[12 - 4 * i] - od[12 - 4 * i]);
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            // Rows (field, cos / sin of m) are the box's (z, y); fields past
+            // nf fall outside the tensor and are not written.
+            if (m == 0) {
+              tma_store_3d(&tO1, sd, jb, 0, row0);
+              tma_store_3d(&tO1, sm, jm, 0, row0);
+            } else {
+              tma_store_3d(&tO2, sd, jb, 2 * m - 1, row0 >> 1);
+              tma_store_3d(&tO2, sm, jm, 2 * m - 1, row0 >> 1);
+            }
+            bulk_commit();
+          }
+          ++nb;
+          continue;
+        }
+        // Row-store path: the staging area is this warp's TMA buffers, so
+        // their stores must have read them.
+        if (lane == 0 && nb > 0) bulk_wait_read<0>();
+        __syncwarp();
         // stage[r][t] = E + O at j = 16c + t; stage[r][16 + t] = E - O at
         // j = J - 16(c+1) + t (the mirrored block, ascending).
 #pragma unroll
@@ -622,8 +695,6 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
           stage[lane * kStride + 16 + (15 - t)] = e[t] - od[t];
         }
         __syncwarp();
-        const int jb = lo + 16 * c;
-        const int jm = a.J - jb - 16;
         // 4 threads per row, 8 rows per pass, 4 passes; two half-blocks.
         for (int pass = 0; pass < 8; ++pass) {
           const int hb = pass >> 2;                    // 0: direct, 1: mirror
@@ -657,6 +728,9 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
         }
         __syncwarp();
       }
+      // The stores have completed before the CTA (and its shared memory) ends.
+      if (lane == 0 && nb > 0) bulk_wait_all();
+      __syncwarp();
     } else {
       // Structural zeros l < m (first N range only), alternate rows.
       for (int r = half; r < 32 && lo == 0; r += 2) {
@@ -742,6 +816,31 @@ static int make_map(CUtensorMap* tm, const bf16* ptr, int inner, long long rows,
   return DINO_OK;
 }
 
+// FP32 output tensor [nf][M][J] for the inverse epilogue's TMA stores: box
+// 16 latitudes x box_y rows x box_z fields.  Returns false (row stores are
+// used instead) when the layout does not allow tensor stores.
+static bool make_out_map(CUtensorMap* tm, const float* out, int J, int M, int nf, int box_y,
+                         int box_z) {
+  auto fn = encode_fn();
+  if (!fn || (J & 3) != 0 || ((uintptr_t)out & 15) != 0 || nf < 1) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)J, (cuuint64_t)M, (cuuint64_t)nf};
+  cuuint64_t strides[2] = {(cuuint64_t)J * sizeof(float), (cuuint64_t)M * J * sizeof(float)};
+  cuuint32_t box[3] = {16u, (cuuint32_t)box_y, (cuuint32_t)box_z};
+  cuuint32_t elem[3] = {1u, 1u, 1u};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)out, dims, strides, box, elem,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Both output maps of an inverse launch; sets a.tma_out.
+static void tc_out_maps(const dino_plan* p, TcArgs* a, float* out, int nf, CUtensorMap* o2,
+                        CUtensorMap* o1) {
+  memset(o2, 0, sizeof(*o2));
+  memset(o1, 0, sizeof(*o1));
+  a->tma_out = make_out_map(o2, out, p->J, p->M, nf, 2, 16) &&
+               make_out_map(o1, out, p->J, p->M, nf, 1, 32);
+}
+
 // ---------------------------------------------------------------------------
 // Autotuning of the tensor-core launch shape
 // ---------------------------------------------------------------------------
@@ -817,17 +916,21 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
   a.stages = c.stages;
   a.tmem_cols = tmem_cols_for(2 * c.Nsub);
   a.out = out;
+  CUtensorMap o2, o1;
+  memset(&o2, 0, sizeof(o2));
+  memset(&o1, 0, sizeof(o1));
   if (kForward) {
     a.G = src;
   } else {
     a.in = one_seg(src, nf);
     a.vec = tc_vec_input(p, a.in);
+    tc_out_maps(p, &a, out, nf, &o2, &o1);
   }
   dim3 grid(ceil_div(2 * nf, 128), p->lw, c.nsplit);
   constexpr int kReps = 3;
   for (int r = 0; r <= kReps; ++r) {
     if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
-    legendre_tc_kernel<kForward><<<grid, kTcThreads, c.smem, 0>>>(bh, bl, a);
+    legendre_tc_kernel<kForward><<<grid, kTcThreads, c.smem, 0>>>(bh, bl, o2, o1, a);
     DINO_TRY(check_launch("legendre_tc (autotune)"));
   }
   DINO_CHECK_CUDA(cudaEventRecord(e1, 0));
@@ -979,8 +1082,11 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
   a.in = in;
   a.vec = tc_vec_input(p, in);
   a.out = out;
+  CUtensorMap o2, o1;
+  tc_out_maps(p, &a, out, nf, &o2, &o1);
   dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_inv);
-  legendre_tc_kernel<false><<<grid, kTcThreads, t->smem_inv, st>>>(t->tBih, t->tBil, a);
+  legendre_tc_kernel<false><<<grid, kTcThreads, t->smem_inv, st>>>(t->tBih, t->tBil, o2, o1,
+                                                                   a);
   return check_launch("legendre_tc_inverse");
 }
 
@@ -992,8 +1098,11 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
   TcArgs a = tc_args(p, t, true, nf);
   a.G = G;
   a.out = out;
+  CUtensorMap unused;  // the forward epilogue uses row stores
+  memset(&unused, 0, sizeof(unused));
   dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_fwd);
-  legendre_tc_kernel<true><<<grid, kTcThreads, t->smem_fwd, st>>>(t->tBfh, t->tBfl, a);
+  legendre_tc_kernel<true><<<grid, kTcThreads, t->smem_fwd, st>>>(t->tBfh, t->tBfl, unused,
+                                                                  unused, a);
   return check_launch("legendre_tc_forward");
 }
 
