@@ -34,6 +34,21 @@ GRID = dict(name='TL255', max_wavenumber=255, gaussian_nodes=128)
 FIELDS = 128
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# each transform phase over the 128 TL255 fields, from one ncu capture
+# (profiles/sht_phase_tl255_b128_dram_traffic.md).
+PHASE_TRAFFIC = {
+    ('bf16x3', 'legendre_inverse'): 94114048 + 32891136,
+    ('bf16x3', 'fourier_inverse'): 67014912 + 23471360,
+    ('bf16x3', 'fourier_forward'): 67135744 + 25449472,
+    ('bf16x3', 'legendre_forward'): 121940736 + 36291840,
+    ('fp32', 'legendre_inverse'): 58467584 + 19169536,
+    ('fp32', 'fourier_inverse'): 67018752 + 23803136,
+    ('fp32', 'fourier_forward'): 67136000 + 25746688,
+    ('fp32', 'legendre_forward'): 84814592 + 29821696,
+}
+
+
 def workload_dims():
   lw = GRID['max_wavenumber'] + 1
   L = GRID['max_wavenumber'] + 2
@@ -319,6 +334,28 @@ def run_ours(args):
     nodal = plan.inverse(x)
     return plan.forward(nodal)
 
+  lw, L, I, J, M, _ = workload_dims()
+  phases = {'legendre_inverse': 0, 'fourier_inverse': 1, 'fourier_forward': 2,
+            'legendre_forward': 3}
+  if args.profile_phase:
+    # One phase over all fields, the last launch inside an NVTX range named
+    # "phase" (for an ncu capture with --nvtx --nvtx-include "phase/").
+    shapes = [(fields, M, L), (fields, M, J), (fields, I, J), (fields, M, J)]
+    code = phases[args.profile_phase]
+    src = x if code == 0 else torch.randn(shapes[code], device='cuda')
+    dst = torch.empty(shapes[(code + 1) % 4], device='cuda')
+    for i in range(args.warmup + 1):
+      if i == args.warmup:
+        torch.cuda.nvtx.range_push('phase')
+      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
+                                           fields, sh.stream_handle()))
+      if i == args.warmup:
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    if rank == 0:
+      print(json.dumps({'profile_phase': args.profile_phase}), flush=True)
+    return
+
   for _ in range(args.warmup):
     y = step()
   torch.cuda.synchronize()
@@ -395,7 +432,6 @@ def run_ours(args):
                   torch.linalg.vector_norm(y))
 
   # Per-phase kernel timing (live CUDA events on the launching stream).
-  lw, L, I, J, M, _ = workload_dims()
   buf_f = torch.empty((fields, M, J), device='cuda')
   buf_n = torch.empty((fields, I, J), device='cuda')
   buf_m = torch.empty((fields, M, L), device='cuda')
@@ -429,7 +465,9 @@ def run_ours(args):
   per_field = M * J * 4
   cap = max(1, (48 << 20) // per_field)
   chunks = -(-fields // min(cap, plan.max_fields))
-  launches_per_step = chunks * (4 if args.precision == 'fp32' else 6)
+  # Per chunk: inverse Legendre, inverse FFT, forward FFT, forward Legendre
+  # (the split-BF16 operand split and fold run inside the Legendre kernels).
+  launches_per_step = chunks * 4
 
   extra = {}
   if not args.no_extra and world == 1:
@@ -479,7 +517,9 @@ def run_ours(args):
         'roofline': {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved,
                      'peak': hbm_peak, 'unit': 'GB/s',
                      'frac': achieved / hbm_peak, 'peak_source': peak_src,
-                     'traffic': None, 'phase_ms': phase_ms},
+                     'traffic': PHASE_TRAFFIC.get((args.precision, dominant)),
+                     'traffic_unit': 'bytes per launch (ncu, one capture)',
+                     'phase_ms': phase_ms},
         'clocks': clocks,
         'gpu_launches': launches_per_step * args.steps,
         'round_trip_rel_l2': rt_err,
@@ -698,6 +738,10 @@ def main():
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--profile', action='store_true',
                   help='only the device-resident timed loop (for ncu captures)')
+  ap.add_argument('--profile-phase', default=None,
+                  choices=['legendre_inverse', 'fourier_inverse', 'fourier_forward',
+                           'legendre_forward'],
+                  help='only one transform phase over all fields (for ncu captures)')
   args = ap.parse_args()
   if args.warmup < 3:
     args.warmup = 3
