@@ -53,6 +53,27 @@ def test_tc_transforms_match_fp64_oracle(name):
   assert np.all(modal.cpu().numpy()[:, ~og.mask] == 0)
 
 
+@pytest.mark.parametrize('n,spacing', [(24, 'gauss'), (24, 'equiangular_with_poles'),
+                                       (62, 'gauss')])
+def test_tc_transforms_on_ragged_latitude_blocks(n, spacing):
+  # J = 37 (odd: a self-mirrored middle latitude, 19 latitude pairs) and
+  # J = 94 (47 pairs, J not a multiple of 4): partial 16-latitude blocks take
+  # the row-store epilogue and the operands the scalar (non-float4) paths.
+  impl = lambda **kw: sh.CudaSphericalHarmonics(precision='bf16x3', **kw)
+  g = sh.Grid.with_wavenumbers(n, latitude_spacing=spacing, spherical_harmonics_impl=impl)
+  og = osht.Grid.with_wavenumbers(n, latitude_spacing=spacing)
+  x = ost.sht_modal_input(og, 3, seed=9)
+  nodal = g.to_nodal(torch.as_tensor(x, device='cuda'))
+  _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
+  ref = og.to_nodal(x.astype(np.float64))
+  assert l2(nodal, ref) < 1e-5 and maxrel(nodal, ref) < 5e-5
+  z = np.random.default_rng(10).standard_normal((3,) + og.nodal_shape)
+  modal = g.to_modal(torch.as_tensor(z, device='cuda', dtype=torch.float32))
+  _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
+  refm = og.to_modal(z.astype(np.float32).astype(np.float64))
+  assert l2(modal, refm) < 1e-5 and maxrel(modal, refm) < 5e-5
+
+
 def test_tc_matches_fp32_plan_on_large_batch():
   g = tc_grid('TL255')
   f = sh.Grid.TL255()
