@@ -149,22 +149,6 @@ __device__ __forceinline__ float dlat_at(const float* x, const float* s,
   return v;
 }
 
-// Transposed cos_lat_d_dlat (tab 0) / sec_lat_d_dlat_cos2 (tab 2) at (row, l)
-// of a plane y whose entries at l >= lclip count as zero:
-//   (D^T y)[l] = ta[l] y[l-1] + tb[l] y[l+1].
-__device__ __forceinline__ float dlat_t_at(const float* y, int row, int l, int L,
-                                           int lclip, int lw, const float* deriv,
-                                           int tab) {
-  const int m = (row + 1) >> 1;
-  const float* ta = deriv + (size_t)tab * lw * L + (size_t)m * L;
-  const float* tb = ta + (size_t)lw * L;
-  const float* yr = y + (size_t)row * L;
-  float v = 0.f;
-  if (l >= 1 && l - 1 < lclip) v += ta[l] * yr[l - 1];
-  if (l + 1 < lclip) v += tb[l] * yr[l + 1];
-  return v;
-}
-
 // sht.cu
 int sht_inverse_segs(dino_plan* p, const Segs& in, float* out_nodal, int nfields,
                      float* work, int work_fields, cudaStream_t st);

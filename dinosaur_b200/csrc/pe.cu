@@ -65,8 +65,7 @@ struct dino_pe {
   // Host copies (FP64).
   std::vector<double> dsig, c2c, alpha, tref, sumsig, sigma, G, H;
   // Device constants.
-  float* d_lev = nullptr;   // per-level constants (see LevOff)
-  float* d_levpack = nullptr;  // the same, packed per level (kLevPack)
+  float* d_levpack = nullptr;  // per-level constants, packed per level (kLevPack)
   int sms = 148;               // multiprocessors of the device
   float* d_lat = nullptr;   // per-latitude constants: sec2, f, sin2, cos2
   float* d_orog = nullptr;  // modal orography [M][L]
@@ -104,7 +103,8 @@ struct dino_pe {
 
 namespace dino {
 
-// Offsets into d_lev (floats); every array has K entries (c2ci and trefdiff
+// Offsets into the host-side per-level arrays (floats) from which the packed
+// table (kLevPack) is built; every array has K entries (c2ci and trefdiff
 // hold 0 at K - 1).
 struct LevOff {
   int dsig, c2ci, alpha, tref, sumsig, sigma, kv, trefdiff, logsp0;
@@ -253,9 +253,7 @@ struct NodalArgs {
       p_laplnps, p_lnps;
   int o_Au, o_Av, o_KE, o_uT, o_vT, o_Tn, o_tr, o_vh, o_gh, o_dh, o_hsT,
       o_lnps;
-  const float* lev;
-  LevOff lo;
-  const float* levpack;  // [K][kLevPack] (pe_nodal_kernel)
+  const float* levpack;  // [K][kLevPack] per-level coefficients
   const float* lat;  // [4][J]: sec2, coriolis, sin^2, cos^2
   float R, kappa, Rv_over_R, Cpv_over_Cp, Rv_minus_R;
   float hs_p0, hs_ka, hs_ks, hs_sigma_b, hs_minT, hs_maxT, hs_dTy, hs_dThz;
@@ -1948,8 +1946,6 @@ static NodalArgs make_nodal_args(dino_pe* pe) {
     a.o_dh = pe->o_dh;
     a.o_hsT = pe->o_hsT;
     a.o_lnps = pe->o_lnps;
-    a.lev = pe->d_lev;
-    a.lo = lev_offsets(K);
     a.levpack = pe->d_levpack;
     a.lat = pe->d_lat;
     a.R = (float)pe->R;
@@ -2291,7 +2287,6 @@ static void pe_free(dino_pe* pe) {
   if (pe->graph.graph) cudaGraphDestroy(pe->graph.graph);
   for (auto& e : pe->mat_cache) cudaFree(e.d);
   for (auto& e : pe->filter_cache) cudaFree(e.d_filter);
-  cudaFree(pe->d_lev);
   cudaFree(pe->d_levpack);
   cudaFree(pe->d_lat);
   cudaFree(pe->d_orog);
@@ -2352,7 +2347,6 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
       lev[lo.trefdiff + k] = (float)((pe->tref[k + 1] - pe->tref[k]) * pe->c2c[k]);
     }
   }
-  DINO_TRY(upload_vec(&pe->d_lev, lev));
   // The same constants packed per level for pe_nodal_kernel (kLevPack).
   std::vector<float> pack((size_t)K * kLevPack, 0.f);
   for (int k = 0; k < K; ++k) {
