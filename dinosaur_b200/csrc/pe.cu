@@ -1494,15 +1494,18 @@ struct ApplyArgs {
   int R, nin, RP, Cp;
 };
 
-constexpr int kApplyCols = 64;
-constexpr int kApplyMaxTR = 13;
+constexpr int kApplyCols = 128;
+constexpr int kApplyMaxTR = 9;
 
-// A CTA takes one l, 64 columns and 16*TR rows of A_l: it stages A_l^T and
-// the operand rows in shared memory and each thread accumulates a TR x 4
-// register tile (broadcast A reads, float4 operand reads and stores).
+// A CTA takes one l, 128 columns and 16*TR rows of A_l: it stages A_l^T and
+// the operand rows in shared memory and each thread accumulates a TR x 8
+// register tile, columns 4 cg .. 4 cg + 3 and 64 + 4 cg .. 64 + 4 cg + 3
+// (two conflict-free float4 operand reads per k, broadcast A reads, float4
+// stores).
 template <int TR>
 __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
   constexpr int RPT = 16 * TR;
+  constexpr int Q4 = kApplyCols / 4;  // float4 per operand row
   extern __shared__ __align__(16) float smem[];
   const int nin = a.nin;
   float* At = smem;                    // [nin][RPT]
@@ -1520,43 +1523,52 @@ __global__ void __launch_bounds__(256) pe_apply_kernel(ApplyArgs a) {
           reinterpret_cast<const float4*>(Ag + (size_t)k * a.RP)[q];
     }
     const float* Yg = a.ylm + (size_t)l * nin * a.Cp + c0;
-    constexpr int QC = kApplyCols / 4;
-    for (int e = tid; e < nin * QC; e += 256) {
-      const int k = e / QC, q = e - k * QC;
+    for (int e = tid; e < nin * Q4; e += 256) {
+      const int k = e / Q4, q = e - k * Q4;
       reinterpret_cast<float4*>(Ys)[e] =
           reinterpret_cast<const float4*>(Yg + (size_t)k * a.Cp)[q];
     }
   }
   __syncthreads();
   const int cg = tid & 15, rg = tid >> 4;
-  float acc[TR][4];
+  float acc[TR][8];
 #pragma unroll
-  for (int i = 0; i < TR; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+  for (int i = 0; i < TR; ++i)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[i][c] = 0.f;
   const float* ar = At + rg * TR;
   const float4* yr = reinterpret_cast<const float4*>(Ys) + cg;
 #pragma unroll 2
   for (int k = 0; k < nin; ++k) {
-    const float4 y = yr[k * (kApplyCols / 4)];
+    const float4 y0 = yr[k * Q4];
+    const float4 y1 = yr[k * Q4 + 16];
 #pragma unroll
     for (int i = 0; i < TR; ++i) {
       const float av = ar[k * RPT + i];
-      acc[i][0] = fmaf(av, y.x, acc[i][0]);
-      acc[i][1] = fmaf(av, y.y, acc[i][1]);
-      acc[i][2] = fmaf(av, y.z, acc[i][2]);
-      acc[i][3] = fmaf(av, y.w, acc[i][3]);
+      acc[i][0] = fmaf(av, y0.x, acc[i][0]);
+      acc[i][1] = fmaf(av, y0.y, acc[i][1]);
+      acc[i][2] = fmaf(av, y0.z, acc[i][2]);
+      acc[i][3] = fmaf(av, y0.w, acc[i][3]);
+      acc[i][4] = fmaf(av, y1.x, acc[i][4]);
+      acc[i][5] = fmaf(av, y1.y, acc[i][5]);
+      acc[i][6] = fmaf(av, y1.z, acc[i][6]);
+      acc[i][7] = fmaf(av, y1.w, acc[i][7]);
     }
   }
   float* og = a.olm + (size_t)l * a.R * a.Cp + c0 + cg * 4;
 #pragma unroll
   for (int i = 0; i < TR; ++i) {
     const int r = r0 + rg * TR + i;
-    if (r < a.R)
-      *reinterpret_cast<float4*>(og + (size_t)r * a.Cp) =
-          make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+    if (r < a.R) {
+      float* o = og + (size_t)r * a.Cp;
+      *reinterpret_cast<float4*>(o) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+      *reinterpret_cast<float4*>(o + 64) =
+          make_float4(acc[i][4], acc[i][5], acc[i][6], acc[i][7]);
+    }
   }
 }
 
-// Rows per thread for an operator of R rows (one row tile while R <= 208).
+// Rows per thread for an operator of R rows (one row tile while R <= 144).
 static int apply_tr(int R) {
   int tr = (R + 15) / 16;
   return tr > kApplyMaxTR ? kApplyMaxTR : tr;
@@ -1588,10 +1600,6 @@ static int prepare_apply() {
   DINO_TRY(apply_attr<7>());
   DINO_TRY(apply_attr<8>());
   DINO_TRY(apply_attr<9>());
-  DINO_TRY(apply_attr<10>());
-  DINO_TRY(apply_attr<11>());
-  DINO_TRY(apply_attr<12>());
-  DINO_TRY(apply_attr<13>());
   done = true;
   return DINO_OK;
 }
@@ -1647,11 +1655,7 @@ static int launch_apply(dino_pe* pe, const MatEntry* m, const float* src,
     case 6: apply_launch<6>(grid, smem, st, a); break;
     case 7: apply_launch<7>(grid, smem, st, a); break;
     case 8: apply_launch<8>(grid, smem, st, a); break;
-    case 9: apply_launch<9>(grid, smem, st, a); break;
-    case 10: apply_launch<10>(grid, smem, st, a); break;
-    case 11: apply_launch<11>(grid, smem, st, a); break;
-    case 12: apply_launch<12>(grid, smem, st, a); break;
-    default: apply_launch<13>(grid, smem, st, a); break;
+    default: apply_launch<9>(grid, smem, st, a); break;
   }
   DINO_TRY(check_launch("pe_apply"));
   g.lm = pe->d_lm_out;
