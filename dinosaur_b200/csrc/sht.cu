@@ -172,7 +172,13 @@ legendre_inverse_simt(Segs in, float* __restrict__ out, int B, int M, int L,
 }
 
 // out_modal[b][row][l] = sum_j p[m,j,l] G[b][row][j] (forward contraction);
-// writes zeros for l < m.
+// writes zeros for l < m.  A CTA covers 128 rows and TN values of l (64 for
+// long l ranges, 32 for short ones, which keeps more CTAs per SM): thread
+// (tx, ty) accumulates rows 8 ty .. 8 ty + 7 at l - m = k0 + tx + 8 t,
+// t < TN / 8, all of one parity, so it reads only the symmetric (even) or
+// antisymmetric (odd) latitude fold.  Folds and table chunks are fetched with
+// float4 loads where the rows allow.
+template <int TN>
 __global__ void __launch_bounds__(kLegThreads)
 legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
                       int B, int M, int L, int J, int Jh,
@@ -183,7 +189,10 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
   const int r0 = blockIdx.y * kLegTB;
   if (r0 >= rows) return;
   const int Lm = L - m;
-  const int k0 = blockIdx.x * kLegTN;  // l - m offset of this tile
+  constexpr int TT = TN / 8;           // l values per thread
+  constexpr int PV = TN / 8;           // table values fetched per thread and chunk
+  constexpr int PT = kLegKC / PV;      // threads per table row
+  const int k0 = blockIdx.x * TN;  // l - m offset of this tile
   const int tid = threadIdx.x;
   const int tx = tid & 7;
   const int ty = tid >> 3;
@@ -205,7 +214,7 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
 
   __shared__ __align__(16) float Ss[kLegKC][kLegTB + 4];
   __shared__ __align__(16) float Ds[kLegKC][kLegTB + 4];
-  __shared__ float Ps[kLegKC][kLegTN + 1];
+  __shared__ float Ps[kLegKC][TN + 1];
 
   const int lq = tid & 3;
   const float* grow[4];
@@ -219,37 +228,65 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
       grow[i] = G + ((size_t)b * M + row) * J;
     }
   }
-  // P chunk 32 (l) x 16 (j): thread loads l = tid / 4, j = 4 (tid % 4) .. +3.
-  const int pl_ = tid >> 2, pjq = (tid & 3) * 4;
-  float sv[4][4], dv[4][4], pvr[4];
+  // Row starts are 16-byte aligned when J % 4 == 0 (then so are j and the
+  // mirrored J - 4 - j for j a multiple of 4).
+  const bool vec = (J & 3) == 0;
+  // P chunk TN (l) x 16 (j): thread loads l = tid / PT, j = PV (tid % PT) ..
+  const int pl_ = tid / PT, pjq = (tid % PT) * PV;
+  float sv[4][4], dv[4][4], pvr[PV];
   auto fetch = [&](int jc) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i) {
+      const int j = jc + lq * 4;
+      float g1[4] = {0.f, 0.f, 0.f, 0.f}, g2[4] = {0.f, 0.f, 0.f, 0.f};
+      if (grow[i]) {
+        if (vec && j + 4 <= Jh) {
+          const float4 d = *reinterpret_cast<const float4*>(grow[i] + j);
+          const float4 e = *reinterpret_cast<const float4*>(grow[i] + J - 4 - j);
+          g1[0] = d.x; g1[1] = d.y; g1[2] = d.z; g1[3] = d.w;
+          g2[0] = e.w; g2[1] = e.z; g2[2] = e.y; g2[3] = e.x;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            if (j + e < Jh) {
+              g1[e] = grow[i][j + e];
+              const int jm = J - 1 - (j + e);
+              g2[e] = (jm != j + e) ? grow[i][jm] : 0.f;
+            }
+          }
+        }
+      }
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const int j = jc + lq * 4 + e;
-        float g1 = 0.f, g2 = 0.f;
-        if (grow[i] && j < Jh) {
-          g1 = grow[i][j];
-          const int jm = J - 1 - j;
-          g2 = (jm != j) ? grow[i][jm] : 0.f;
-        }
-        sv[i][e] = g1 + g2;
-        dv[i][e] = g1 - g2;
+        sv[i][e] = g1[e] + g2[e];
+        dv[i][e] = g1[e] - g2[e];
       }
+    }
     const int k = k0 + pl_;
+    const int j = jc + pjq;
+    const float* pr = P + (size_t)k * Jh + j;
+    if ((Jh & 3) == 0 && k < Lm && j + PV <= Jh) {
+      // Table rows start 16-byte aligned (the per-m offsets are multiples of
+      // Jh).
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int j = jc + pjq + e;
-      pvr[e] = (k < Lm && j < Jh) ? P[(size_t)k * Jh + j] : 0.f;
+      for (int q = 0; q < PV / 4; ++q) {
+        const float4 v = *reinterpret_cast<const float4*>(pr + 4 * q);
+        pvr[4 * q] = v.x;
+        pvr[4 * q + 1] = v.y;
+        pvr[4 * q + 2] = v.z;
+        pvr[4 * q + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < PV; ++e) pvr[e] = (k < Lm && j + e < Jh) ? pr[e] : 0.f;
     }
   };
 
-  float acc[8][4];
+  float acc[8][TT];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int t = 0; t < 4; ++t) acc[i][t] = 0.f;
+    for (int t = 0; t < TT; ++t) acc[i][t] = 0.f;
 
   fetch(0);
   for (int jc = 0; jc < Jh; jc += kLegKC) {
@@ -262,24 +299,22 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
         Ds[lq * 4 + e][(tid >> 2) + 32 * i] = dv[i][e];
       }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) Ps[pjq + e][pl_] = pvr[e];
+    for (int e = 0; e < PV; ++e) Ps[pjq + e][pl_] = pvr[e];
     __syncthreads();
     if (jc + kLegKC < Jh) fetch(jc + kLegKC);
-    // Output l - m = k0 + tx + 8 t: its parity is that of tx, so a thread
-    // reads only the symmetric (even) or antisymmetric (odd) fold.
     const float* fold = (tx & 1) ? &Ds[0][0] : &Ss[0][0];
 #pragma unroll
     for (int jj = 0; jj < kLegKC; ++jj) {
       float4 fa = *reinterpret_cast<const float4*>(fold + jj * (kLegTB + 4) + ty * 8);
       float4 fb = *reinterpret_cast<const float4*>(fold + jj * (kLegTB + 4) + ty * 8 + 4);
       float f8[8] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w};
-      float pw[4];
+      float pw[TT];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) pw[t] = Ps[jj][tx + 8 * t];
+      for (int t = 0; t < TT; ++t) pw[t] = Ps[jj][tx + 8 * t];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int t = 0; t < 4; ++t) acc[i][t] = fmaf(f8[i], pw[t], acc[i][t]);
+        for (int t = 0; t < TT; ++t) acc[i][t] = fmaf(f8[i], pw[t], acc[i][t]);
     }
   }
 
@@ -291,7 +326,7 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
     row_map(m, r, b, row);
     float* o = out + ((size_t)b * M + row) * L + m;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
+    for (int t = 0; t < TT; ++t) {
       int k = k0 + tx + 8 * t;
       if (k < Lm) o[k] = acc[i][t];
     }
@@ -321,9 +356,15 @@ int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
                      cudaStream_t st) {
   if (p->precision == DINO_PREC_BF16X3)
     return tc_legendre_forward(p, G, out, nf, st);
-  dim3 grid(ceil_div(p->L, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
-  legendre_forward_simt<<<grid, kLegThreads, 0, st>>>(
-      G, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
+  if (p->L > 64) {
+    dim3 grid(ceil_div(p->L, 64), ceil_div(2 * nf, kLegTB), p->lw);
+    legendre_forward_simt<64><<<grid, kLegThreads, 0, st>>>(
+        G, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
+  } else {
+    dim3 grid(ceil_div(p->L, 32), ceil_div(2 * nf, kLegTB), p->lw);
+    legendre_forward_simt<32><<<grid, kLegThreads, 0, st>>>(
+        G, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
+  }
   return check_launch("legendre_forward_simt");
 }
 
