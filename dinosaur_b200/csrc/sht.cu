@@ -409,8 +409,47 @@ __device__ __forceinline__ float2 root16(int k) {
   }
 }
 
+// exp(kSign 2 pi i k / 16) for any k >= 0.
+template <int kSign>
+__device__ __forceinline__ float2 w16(int k) {
+  float2 w = root16(k & 7);
+  if (k & 8) w = make_float2(-w.x, -w.y);
+  return kSign < 0 ? cconj(w) : w;
+}
+
+// Multiplies by exp(kSign 2 pi i k / 16) for a compile-time k: multiples of
+// 4 are sign swaps (no multiply), the others one complex multiply.
+template <int K, int kSign>
+__device__ __forceinline__ float2 twiddle16(float2 a) {
+  constexpr int k = K & 15;
+  if constexpr (k == 0) {
+    return a;
+  } else if constexpr (k == 4) {
+    return cmul_i<kSign>(a);
+  } else if constexpr (k == 8) {
+    return make_float2(-a.x, -a.y);
+  } else if constexpr (k == 12) {
+    return cmul_i<-kSign>(a);
+  } else {
+    return cmul(a, w16<kSign>(k));
+  }
+}
+
+// DFT of length 4: X_k = sum_q v_q exp(kSign 2 pi i q k / 4).
+template <int kSign>
+__device__ __forceinline__ void dft4(float2& a, float2& b, float2& c, float2& d) {
+  const float2 s0 = cadd(a, c), d0 = csub(a, c);
+  const float2 s1 = cadd(b, d), d1 = cmul_i<kSign>(csub(b, d));
+  a = cadd(s0, s1);
+  c = csub(s0, s1);
+  b = cadd(d0, d1);
+  d = csub(d0, d1);
+}
+
 // In-register DFT of length R (power of two <= 16), natural order in and
-// out: v_s <- sum_q v_q exp(kSign 2 pi i q s / R).
+// out: v_s <- sum_q v_q exp(kSign 2 pi i q s / R).  Lengths 4 and 16 use
+// DFT-4 butterflies (16 = 4 x 4 with the twiddles of multiples of 4 as sign
+// swaps); 2 and 8 split once more by two.
 template <int R, int kSign>
 __device__ __forceinline__ void dft_reg(float2* v) {
   if constexpr (R == 1) {
@@ -419,7 +458,41 @@ __device__ __forceinline__ void dft_reg(float2* v) {
     float2 a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    dft4<kSign>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 16) {
+    // q = 4 q1 + q2, s = s1 + 4 s2: DFT-4 over q1 for each q2, twiddle
+    // W16^(q2 s1), DFT-4 over q2 for each s1.
+    float2 y[16];
+#pragma unroll
+    for (int q2 = 0; q2 < 4; ++q2) {
+      float2 a = v[q2], b = v[4 + q2], c = v[8 + q2], d = v[12 + q2];
+      dft4<kSign>(a, b, c, d);
+      y[4 * q2] = a;      // s1 = 0
+      y[4 * q2 + 1] = b;  // s1 = 1
+      y[4 * q2 + 2] = c;  // s1 = 2
+      y[4 * q2 + 3] = d;  // s1 = 3
+    }
+    y[5] = twiddle16<1, kSign>(y[5]);
+    y[6] = twiddle16<2, kSign>(y[6]);
+    y[7] = twiddle16<3, kSign>(y[7]);
+    y[9] = twiddle16<2, kSign>(y[9]);
+    y[10] = twiddle16<4, kSign>(y[10]);
+    y[11] = twiddle16<6, kSign>(y[11]);
+    y[13] = twiddle16<3, kSign>(y[13]);
+    y[14] = twiddle16<6, kSign>(y[14]);
+    y[15] = twiddle16<9, kSign>(y[15]);
+#pragma unroll
+    for (int s1 = 0; s1 < 4; ++s1) {
+      float2 a = y[s1], b = y[4 + s1], c = y[8 + s1], d = y[12 + s1];
+      dft4<kSign>(a, b, c, d);
+      v[s1] = a;
+      v[s1 + 4] = b;
+      v[s1 + 8] = c;
+      v[s1 + 12] = d;
+    }
   } else {
+    // R = 8: even / odd halves, then W8^k = W16^(2k) on the odd half.
     constexpr int H = R / 2;
     float2 e[H], o[H];
 #pragma unroll
@@ -429,14 +502,18 @@ __device__ __forceinline__ void dft_reg(float2* v) {
     }
     dft_reg<H, kSign>(e);
     dft_reg<H, kSign>(o);
-#pragma unroll
-    for (int k = 0; k < H; ++k) {
-      float2 w = root16(k * (16 / R));
-      if (kSign < 0) w = cconj(w);
-      float2 t = (k == 0) ? o[k] : cmul(o[k], w);
-      v[k] = cadd(e[k], t);
-      v[k + H] = csub(e[k], t);
-    }
+    const float2 t0 = o[0];
+    const float2 t1 = twiddle16<2, kSign>(o[1]);
+    const float2 t2 = twiddle16<4, kSign>(o[2]);
+    const float2 t3 = twiddle16<6, kSign>(o[3]);
+    v[0] = cadd(e[0], t0);
+    v[4] = csub(e[0], t0);
+    v[1] = cadd(e[1], t1);
+    v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2);
+    v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3);
+    v[7] = csub(e[3], t3);
   }
 }
 
