@@ -291,7 +291,8 @@ def phase_bytes(phase, fields, precision):
   lw, L, I, J, M, n_tri = workload_dims()
   Jh = J // 2
   table_elems = Jh * sum(L - m for m in range(lw))
-  table_bytes = table_elems * (4 if precision == 'fp32' else 4)  # fp32 or bf16 hi+lo
+  # fp32 table, bf16 hi + lo (4 bytes per entry) or tf32 hi + lo (8 bytes)
+  table_bytes = table_elems * (8 if precision == 'tf32x3' else 4)
   modal = fields * M * L * 4
   fourier = fields * M * J * 4
   nodal = fields * I * J * 4
@@ -471,26 +472,26 @@ def run_ours(args):
 
   extra = {}
   if not args.no_extra and world == 1:
-    # The other Legendre form on the same workload, for the split-BF16 vs
-    # FP32 comparison.
-    other = 'fp32' if args.precision == 'bf16x3' else 'bf16x3'
-    g2 = make_grid(other)
-    for _ in range(args.warmup):
-      y2 = g2.plan.forward(g2.plan.inverse(x))
-    torch.cuda.synchronize()
-    rt2 = float(torch.linalg.vector_norm(y2 - x) / torch.linalg.vector_norm(x))
-    b0 = torch.cuda.Event(enable_timing=True)
-    b1 = torch.cuda.Event(enable_timing=True)
-    b0.record(stream)
-    for _ in range(args.steps):
-      y2 = g2.plan.forward(g2.plan.inverse(x))
-    b1.record(stream)
-    torch.cuda.synchronize()
-    ms2 = b0.elapsed_time(b1) / args.steps
-    extra['sht_' + other] = {'value': aggregate_tflops(sht_flops(fields), 1, ms2),
-                             'unit': 'TFLOP/s', 'ms_per_step': ms2,
-                             'round_trip_rel_l2': rt2}
-    del g2, y2
+    # The other Legendre forms on the same workload (plain FP32, split-BF16,
+    # split-TF32), for the comparison of speed and round-trip error.
+    for other in [f for f in ('fp32', 'bf16x3', 'tf32x3') if f != args.precision]:
+      g2 = make_grid(other)
+      for _ in range(args.warmup):
+        y2 = g2.plan.forward(g2.plan.inverse(x))
+      torch.cuda.synchronize()
+      rt2 = float(torch.linalg.vector_norm(y2 - x) / torch.linalg.vector_norm(x))
+      b0 = torch.cuda.Event(enable_timing=True)
+      b1 = torch.cuda.Event(enable_timing=True)
+      b0.record(stream)
+      for _ in range(args.steps):
+        y2 = g2.plan.forward(g2.plan.inverse(x))
+      b1.record(stream)
+      torch.cuda.synchronize()
+      ms2 = b0.elapsed_time(b1) / args.steps
+      extra['sht_' + other] = {'value': aggregate_tflops(sht_flops(fields), 1, ms2),
+                               'unit': 'TFLOP/s', 'ms_per_step': ms2,
+                               'round_trip_rel_l2': rt2}
+      del g2, y2
     extra.update(pe_extras(torch))
 
   if rank == 0:
@@ -499,7 +500,7 @@ def run_ours(args):
         'value': value, 'unit': 'TFLOP/s', 'n_gpus': world,
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_max,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-        'dtype': 'f32' if args.precision == 'fp32' else 'bf16x3->f32',
+        'dtype': 'f32' if args.precision == 'fp32' else args.precision + '->f32',
         'data': 'synthetic',
         'config': {'workload': 'SHT pair TL255 x 128 fields', 'grid': 'TL255',
                    'fields': fields, 'precision': args.precision,
@@ -539,7 +540,7 @@ def pe_extras(torch):
   Synthetic states near rest (seeded small modal noise); the moist case adds
   specific humidity (5 g/kg mean) and two passive tracers.  Each case runs
   with the plain FP32 and the split-BF16 Legendre contraction where both are
-  listed."""
+  listed (the dry TL255 case also with split-TF32)."""
   from dinosaur_b200 import coordinate_systems, held_suarez, primitive_equations as pe
   from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
   from dinosaur_b200 import time_integration as ti, units
@@ -550,6 +551,7 @@ def pe_extras(torch):
       ('T42_L24_x16_held_suarez_bf16x3', 'T42', 24, 16, True, False, 15, 'bf16x3'),
       ('TL255_L32_dry', 'TL255', 32, 1, False, False, 6, 'fp32'),
       ('TL255_L32_dry_bf16x3', 'TL255', 32, 1, False, False, 6, 'bf16x3'),
+      ('TL255_L32_dry_tf32x3', 'TL255', 32, 1, False, False, 6, 'tf32x3'),
       ('TL255_L32_moist3_x4', 'TL255', 32, 4, False, True, 6, 'fp32'),
       ('TL255_L32_moist3_x4_bf16x3', 'TL255', 32, 4, False, True, 6, 'bf16x3'),
   ]
@@ -733,7 +735,7 @@ def main():
   ap.add_argument('--warmup', type=int, default=5)
   ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
   ap.add_argument('--precision', default=os.environ.get('DINO_BENCH_PRECISION', 'bf16x3'),
-                  choices=['fp32', 'bf16x3'])
+                  choices=['fp32', 'bf16x3', 'tf32x3'])
   ap.add_argument('--no-extra', action='store_true')
   ap.add_argument('--no-cpu-baseline', action='store_true')
   ap.add_argument('--profile', action='store_true',

@@ -24,7 +24,7 @@ DINO_ERR_NAN = 5
 DINO_ERR_UNSUPPORTED = 6
 
 SPACING = {'gauss': 0, 'equiangular': 1, 'equiangular_with_poles': 2}
-PRECISION = {'fp32': 0, 'bf16x3': 1}
+PRECISION = {'fp32': 0, 'bf16x3': 1, 'tf32x3': 2}
 OPS = dict(d_dlon=0, cos_lat_d_dlat=1, sec_lat_d_dlat_cos2=2, laplacian=3,
            inverse_laplacian=4, clip=5)
 

@@ -1,22 +1,25 @@
-// Legendre contraction on tcgen05 tensor cores, split-BF16 with FP32
-// accumulation (DINO_PREC_BF16X3).
+// Legendre contraction on tcgen05 tensor cores, split-BF16 (DINO_PREC_BF16X3)
+// or split-TF32 (DINO_PREC_TF32X3) with FP32 accumulation.
 //
-// Every FP32 operand x is split into x_hi = bf16(x) and x_lo = bf16(x - x_hi);
-// each product is formed as hi*hi + hi*lo + lo*hi (the lo*lo term, ~2^-16
-// relative, is dropped) and accumulated in FP32 in tensor memory.  The
-// Legendre tables are split from their FP64 values.
+// Every FP32 operand x is split into x_hi = round(x) and x_lo = round(x - x_hi)
+// in the operand format (bf16: 8 significant bits, tf32: 11); each product is
+// formed as hi*hi + hi*lo + lo*hi (the lo*lo term, ~2^-16 relative for bf16
+// and ~2^-22 for tf32, is dropped) and accumulated in FP32 in tensor memory.
+// The Legendre tables are split from their FP64 values.  Both forms share
+// every tile shape: a 128-byte swizzled row holds one K block (64 bf16 or 32
+// tf32 entries) and one MMA instruction consumes 32 bytes of K (16 or 8).
 //
 // Per zonal wavenumber m the contraction is a GEMM
 //   inverse:  D[r, j]  = sum_{l'} X_p[r, l'] P_p[j, l']   (K = l', N = j)
 //   forward:  D[r, l'] = sum_j  G_p[r, j]  P_p[l', j]     (K = j,  N = l')
 // with r = (field, cos/sin) rows, p the parity of l - m (the N/S fold),
 // l = m + 2 l' + p, and G_0 / G_1 the symmetric / antisymmetric latitude
-// folds.  The tables P_p are K-major split bf16 in HBM, loaded by TMA (no
+// folds.  The tables P_p are K-major split operands in HBM, loaded by TMA (no
 // multicast) into 128-byte-swizzled shared memory tiles; the A operand is
 // produced in the same layout by six warps of the CTA straight from the FP32
 // modal coefficients (inverse) or Fourier coefficients (forward): one read of
 // the source gives both parities, folded and split.  One thread issues
-// tcgen05.mma (M = 128, N = latitudes or l', K = 16 per instruction) into two
+// tcgen05.mma (M = 128, N = latitudes or l', 32 bytes of K per instruction) into two
 // TMEM accumulators (one per parity); all eight warps read them back with
 // tcgen05.ld and write the unfolded FP32 result.  Only the K steps and N
 // columns that the triangular (m, l) range needs are issued.
@@ -37,11 +40,12 @@ namespace dino {
 typedef __nv_bfloat16 bf16;
 
 struct TcTables {
-  int Kp = 0;   // inverse K extent (l'), multiple of 64
+  int tf32 = 0; // operand format: 0 bf16 (2-byte entries), 1 tf32 (4-byte)
+  int Kp = 0;   // inverse K extent (l'), multiple of the K block
   int Np = 0;   // inverse N (latitudes), multiple of 16
-  int Kj = 0;   // forward K extent (latitudes), multiple of 64
+  int Kj = 0;   // forward K extent (latitudes), multiple of the K block
   int Nf = 0;   // forward N (l'), multiple of 16
-  bf16 *Bih = nullptr, *Bil = nullptr, *Bfh = nullptr, *Bfl = nullptr;
+  void *Bih = nullptr, *Bil = nullptr, *Bfh = nullptr, *Bfl = nullptr;
   CUtensorMap tBih, tBil, tBfh, tBfl;
   int* d_err = nullptr;
   int stages_inv = 0, stages_fwd = 0;
@@ -55,16 +59,64 @@ struct TcTables {
 
 __host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
+// Operand formats.  kKB: K entries per 128-byte swizzled row (one K block per
+// pipeline stage); kStep: K entries per MMA instruction (32 bytes); kChunk: K
+// entries per 16-byte chunk of a row; kFmt: the instruction descriptor's A / B
+// format code; kUnroll: producer tasks loaded before any is converted;
+// kSepAcc: the hi*lo + lo*hi corrections accumulate in TMEM accumulators of
+// their own, added to the hi*hi sums in FP32 by the epilogue.
+//
+// Each MMA instruction adds its products into the FP32 accumulator with a
+// rounding of its own, about one unit in the last place of the accumulator.
+// With exact accumulation the tf32 split would be ~1e-7 accurate (2^-22 per
+// term), so there these roundings dominate: the separate accumulators leave
+// one per K step on the large sums instead of three.  The bf16 split (~4e-6,
+// its dropped lo*lo term) dominates the roundings, so one accumulator serves.
+struct OpBf16 {
+  typedef bf16 T;
+  static constexpr int kKB = 64, kStep = 16, kChunk = 8, kUnroll = 3;
+  static constexpr uint32_t kFmt = 1;  // BF16
+  static constexpr bool kSepAcc = false;
+};
+struct OpTf32 {
+  typedef float T;  // tf32 in an FP32 container (low 13 mantissa bits zero)
+  static constexpr int kKB = 32, kStep = 8, kChunk = 4, kUnroll = 6;
+  static constexpr uint32_t kFmt = 2;  // TF32
+  static constexpr bool kSepAcc = true;
+};
+
+// TMEM accumulators (each Nsub columns) per CTA: one per parity, twice that
+// with separate correction accumulators.
+__host__ __device__ constexpr int tc_accumulators(bool sep) { return sep ? 4 : 2; }
+
 // ---------------------------------------------------------------------------
 // Operand preparation
 // ---------------------------------------------------------------------------
 
-// FP64 recurrence (as in plan.cu) written as split bf16 into the inverse
+// x rounded to tf32 (10 stored mantissa bits), to nearest, ties away from zero.
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void split_table(double v, bf16& hi, bf16& lo) {
+  hi = __double2bfloat16(v);
+  lo = __double2bfloat16(v - (double)__bfloat162float(hi));
+}
+
+__device__ __forceinline__ void split_table(double v, float& hi, float& lo) {
+  hi = tf32_rna((float)v);
+  lo = tf32_rna((float)(v - (double)hi));
+}
+
+// FP64 recurrence (as in plan.cu) written as split operands into the inverse
 // table [m][p][j][Kp] and the forward table [m][p][l'][Kj].
+template <class T>
 __global__ void tc_table_kernel(int lw, int L, int Jh, const double* __restrict__ x,
                                 int Kp, int Np, int Kj, int Nf,
-                                bf16* __restrict__ Bih, bf16* __restrict__ Bil,
-                                bf16* __restrict__ Bfh, bf16* __restrict__ Bfl) {
+                                T* __restrict__ Bih, T* __restrict__ Bil,
+                                T* __restrict__ Bfh, T* __restrict__ Bfl) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   int m = blockIdx.y;
   if (j >= Jh || m >= lw) return;
@@ -87,8 +139,8 @@ __global__ void tc_table_kernel(int lw, int L, int Jh, const double* __restrict_
       p2 = p1;
       p1 = cur;
     }
-    bf16 hi = __double2bfloat16(cur);
-    bf16 lo = __double2bfloat16(cur - (double)__bfloat162float(hi));
+    T hi, lo;
+    split_table(cur, hi, lo);
     int p = k & 1, kk = k >> 1;
     size_t ii = ((size_t)(m * 2 + p) * Np + j) * Kp + kk;
     size_t fi = ((size_t)(m * 2 + p) * Nf + kk) * Kj + j;
@@ -213,21 +265,34 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(const void* p) {
   return d;
 }
 
-// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major,
-// M = 128, N = n.
-__device__ __forceinline__ uint32_t umma_idesc_bf16(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+// Instruction descriptor: D = F32 (bits 4-5), A and B in the operand format
+// (bits 7-9, 10-12), both K-major, N = n (bits 17-22, n / 8), M = 128 (bits
+// 24-28, M / 16).
+template <class Op>
+__device__ __forceinline__ uint32_t umma_idesc(int n) {
+  return (1u << 4) | (Op::kFmt << 7) | (Op::kFmt << 10) | ((uint32_t)(n >> 3) << 17) |
          ((uint32_t)(128 >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b,
-                                          uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
-      "}\n" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+// D (+)= A B^T for one 32-byte K step: kind::f16 for bf16, kind::tf32.
+template <class Op>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b,
+                                     uint32_t idesc, uint32_t accumulate) {
+  if constexpr (Op::kFmt == OpBf16::kFmt) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+  }
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -284,6 +349,36 @@ __device__ __forceinline__ void tmem_ld_pair(uint32_t c0, uint32_t c1, bool odd,
   }
 }
 
+// Chunk c (16 columns) of both parities' results: accumulator p at column
+// p * ncol, and with separate corrections their sums with accumulator 2 + p.
+template <class Op>
+__device__ __forceinline__ void tc_ld_acc(uint32_t base, int ncol, int c, bool odd,
+                                          float (&e)[16], float (&o)[16]) {
+  const uint32_t c0 = base + (uint32_t)(c * 16);
+  if constexpr (Op::kSepAcc) {
+    uint32_t r0[16], r1[16], r2[16], r3[16];
+    tmem_ld16_issue(c0, r0);
+    tmem_ld16_issue(c0 + 2 * ncol, r2);
+    if (odd) {
+      tmem_ld16_issue(c0 + ncol, r1);
+      tmem_ld16_issue(c0 + 3 * ncol, r3);
+    }
+    tmem_wait16(r0);
+    tmem_tie16(r2);
+    if (odd) {
+      tmem_tie16(r1);
+      tmem_tie16(r3);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      e[i] = __uint_as_float(r0[i]) + __uint_as_float(r2[i]);
+      o[i] = odd ? __uint_as_float(r1[i]) + __uint_as_float(r3[i]) : 0.f;
+    }
+  } else {
+    tmem_ld_pair(c0, c0 + ncol, odd, e, o);
+  }
+}
+
 
 __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
   if (m == 0) {
@@ -295,10 +390,9 @@ __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
   }
 }
 
-// Byte offset of 16-byte chunk c (K entries 8c .. 8c+7) of row r in a
-// 128-row x 64-entry bf16 K-major tile with the 128-byte swizzle: the layout
-// that TMA writes for CU_TENSOR_MAP_SWIZZLE_128B and the UMMA descriptor
-// (umma_desc_sw128) reads.
+// Byte offset of 16-byte chunk c of row r in a 128-row K-major tile of
+// 128-byte rows with the 128-byte swizzle: the layout that TMA writes for
+// CU_TENSOR_MAP_SWIZZLE_128B and the UMMA descriptor (umma_desc_sw128) reads.
 __device__ __forceinline__ uint32_t sw128_off(int r, int c) {
   return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
 }
@@ -313,15 +407,26 @@ __device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uin
   lo = reinterpret_cast<const uint32_t&>(l);
 }
 
-// Splits eight values v[s0], v[s0 + st], ... into hi / lo bf16 and writes
-// them as one 16-byte chunk of each tile (shared memory).
-template <int N>
-__device__ __forceinline__ void put_split8(const float (&v)[N], int s0, int st,
-                                           uint8_t* hi, uint8_t* lo, uint32_t off) {
+// Splits Op::kChunk values v[s0], v[s0 + st], ... (8 for bf16, 4 for tf32)
+// into hi / lo and writes them as one 16-byte chunk of each tile (shared
+// memory).
+template <class Op, int N>
+__device__ __forceinline__ void put_split(const float (&v)[N], int s0, int st,
+                                          uint8_t* hi, uint8_t* lo, uint32_t off) {
   uint32_t h[4], l[4];
+  if constexpr (Op::kFmt == OpBf16::kFmt) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    split_pair(v[s0 + (2 * i) * st], v[s0 + (2 * i + 1) * st], h[i], l[i]);
+    for (int i = 0; i < 4; ++i)
+      split_pair(v[s0 + (2 * i) * st], v[s0 + (2 * i + 1) * st], h[i], l[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float x = v[s0 + i * st];
+      const float xh = tf32_rna(x);
+      h[i] = __float_as_uint(xh);
+      l[i] = __float_as_uint(tf32_rna(x - xh));
+    }
+  }
   *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
   *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
@@ -358,39 +463,43 @@ __device__ __forceinline__ void tc_seq(int i, int kb1, int& k, int& p) {
 
 // A operand of K block k for this CTA's 128 rows, both parities from one
 // read of the FP32 source, written split into the stage tiles t0 (parity 0)
-// and t1 (parity 1, null when absent): hi at t, lo at t + 16 KB.
-//   inverse: A_p[r][kk] = x[b][row][m + 2 (64 k + kk) + p]  (0 past l = L - 1)
-//   forward: A_p[r][jj] = G[j] + (-1)^p G[J - 1 - j], j = 64 k + jj  (0 past Jh)
-// A task is one (row, 16-byte chunk); each thread loads kTcUnroll tasks before
-// converting any, so that enough bytes are in flight to cover the latency.
-// S = m mod 4 places the 16 inverse entries inside five aligned float4.
+// and t1 (parity 1, null when absent): hi at t, lo at t + 16 KB.  With
+// B = Op::kKB (K entries per block) and C = Op::kChunk (per 16-byte chunk):
+//   inverse: A_p[r][kk] = x[b][row][m + 2 (B k + kk) + p]  (0 past l = L - 1)
+//   forward: A_p[r][jj] = G[j] + (-1)^p G[J - 1 - j], j = B k + jj  (0 past Jh)
+// A task is one (row, 16-byte chunk); each thread loads Op::kUnroll tasks
+// before converting any, so that enough bytes are in flight to cover the
+// latency.
 constexpr int kTcTasks = 128 * 8;
-constexpr int kTcUnroll = 3;
 
-template <int S>
+// Inverse: a task covers the 2C consecutive l = m + l0 .. m + l0 + 2C - 1
+// (both parities).  S = m mod 4 places them at entries S .. S + 2C - 1 of a
+// window of W = 2C + 4 floats that starts 16-byte aligned (W / 4 float4).
+template <class Op, int S>
 __device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int tile, int rows,
                                                    int k, uint8_t* t0, uint8_t* t1, int pt) {
   constexpr uint32_t kTile = 128u * 128u;
-  for (int q0 = pt; q0 < kTcTasks; q0 += kTcUnroll * kTcProducers) {
-    float w[kTcUnroll][20];
+  constexpr int C = Op::kChunk, W = 2 * C + 4, U = Op::kUnroll;
+  for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
+    float w[U][W];
 #pragma unroll
-    for (int u = 0; u < kTcUnroll; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
 #pragma unroll
-      for (int e = 0; e < 20; ++e) w[u][e] = 0.f;
+      for (int e = 0; e < W; ++e) w[u][e] = 0.f;
       if (q >= kTcTasks) continue;
       const int r = q >> 3, c = q & 7;
       const int rr = tile * 128 + r;
       if (rr >= rows) continue;
       int b, row;
       tc_row_map(m, rr, b, row);
-      const int l0 = 128 * k + 16 * c;  // relative to l = m
-      const int lim = (a.L - m) - l0;   // valid entries from l0
+      const int l0 = 2 * Op::kKB * k + 2 * C * c;  // relative to l = m
+      const int lim = (a.L - m) - l0;             // valid entries from l0
       const float* src = seg_field(a.in, b, (size_t)a.M * a.L) + (size_t)row * a.L + m + l0;
-      if (a.vec && lim >= 20) {
+      if (a.vec && lim >= W) {
         const float4* w4 = reinterpret_cast<const float4*>(src - S);
 #pragma unroll
-        for (int i = 0; i < 5; ++i) {
+        for (int i = 0; i < W / 4; ++i) {
           const float4 t = __ldg(w4 + i);
           w[u][4 * i] = t.x;
           w[u][4 * i + 1] = t.y;
@@ -399,32 +508,35 @@ __device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int t
         }
       } else {
 #pragma unroll
-        for (int e = 0; e < 16; ++e) w[u][e + S] = (e < lim) ? __ldg(src + e) : 0.f;
+        for (int e = 0; e < 2 * C; ++e) w[u][e + S] = (e < lim) ? __ldg(src + e) : 0.f;
       }
     }
 #pragma unroll
-    for (int u = 0; u < kTcUnroll; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
       if (q >= kTcTasks) continue;
       const uint32_t off = sw128_off(q >> 3, q & 7);
-      // Entries S .. S+15: even l - m are parity 0, odd ones parity 1.
-      put_split8(w[u], S, 2, t0, t0 + kTile, off);
-      if (t1) put_split8(w[u], S + 1, 2, t1, t1 + kTile, off);
+      // Entries S .. S+2C-1: even l - m are parity 0, odd ones parity 1.
+      put_split<Op>(w[u], S, 2, t0, t0 + kTile, off);
+      if (t1) put_split<Op>(w[u], S + 1, 2, t1, t1 + kTile, off);
     }
   }
 }
 
+// Forward: a task covers the C latitudes j0 .. j0 + C - 1 and their mirrors.
+template <class Op>
 __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int tile, int rows,
                                                    int k, uint8_t* t0, uint8_t* t1, int pt) {
   constexpr uint32_t kTile = 128u * 128u;
+  constexpr int C = Op::kChunk, U = Op::kUnroll;
   const bool vec = (a.J & 3) == 0;
-  for (int q0 = pt; q0 < kTcTasks; q0 += kTcUnroll * kTcProducers) {
-    float d[kTcUnroll][8], e[kTcUnroll][8];  // G[j0 + t], G[J - 1 - j0 - t]
+  for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
+    float d[U][C], e[U][C];  // G[j0 + t], G[J - 1 - j0 - t]
 #pragma unroll
-    for (int u = 0; u < kTcUnroll; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
 #pragma unroll
-      for (int t = 0; t < 8; ++t) d[u][t] = e[u][t] = 0.f;
+      for (int t = 0; t < C; ++t) d[u][t] = e[u][t] = 0.f;
       if (q >= kTcTasks) continue;
       const int r = q >> 3, c = q & 7;
       const int rr = tile * 128 + r;
@@ -432,20 +544,20 @@ __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int t
       int b, row;
       tc_row_map(m, rr, b, row);
       const float* gr = a.G + ((size_t)b * a.M + row) * a.J;
-      const int j0 = 64 * k + 8 * c;
-      if (vec && j0 + 8 <= a.Jh) {
-        // j0 .. j0+7 and J-8-j0 .. J-1-j0 are float4 pairs.
-        const float4 a0 = __ldg(reinterpret_cast<const float4*>(gr + j0));
-        const float4 a1 = __ldg(reinterpret_cast<const float4*>(gr + j0 + 4));
-        const float4 b0 = __ldg(reinterpret_cast<const float4*>(gr + a.J - 8 - j0));
-        const float4 b1 = __ldg(reinterpret_cast<const float4*>(gr + a.J - 4 - j0));
-        d[u][0] = a0.x; d[u][1] = a0.y; d[u][2] = a0.z; d[u][3] = a0.w;
-        d[u][4] = a1.x; d[u][5] = a1.y; d[u][6] = a1.z; d[u][7] = a1.w;
-        e[u][0] = b1.w; e[u][1] = b1.z; e[u][2] = b1.y; e[u][3] = b1.x;
-        e[u][4] = b0.w; e[u][5] = b0.z; e[u][6] = b0.y; e[u][7] = b0.x;
+      const int j0 = Op::kKB * k + C * c;
+      if (vec && j0 + C <= a.Jh) {
+        // j0 + 4i .. j0 + 4i + 3 and J - 4(i+1) - j0 .. J - 1 - 4i - j0 are
+        // float4 (J and j0 are multiples of 4).
+#pragma unroll
+        for (int i = 0; i < C / 4; ++i) {
+          const float4 f = __ldg(reinterpret_cast<const float4*>(gr + j0 + 4 * i));
+          const float4 g = __ldg(reinterpret_cast<const float4*>(gr + a.J - 4 * (i + 1) - j0));
+          d[u][4 * i] = f.x; d[u][4 * i + 1] = f.y; d[u][4 * i + 2] = f.z; d[u][4 * i + 3] = f.w;
+          e[u][4 * i] = g.w; e[u][4 * i + 1] = g.z; e[u][4 * i + 2] = g.y; e[u][4 * i + 3] = g.x;
+        }
       } else {
 #pragma unroll
-        for (int t = 0; t < 8; ++t) {
+        for (int t = 0; t < C; ++t) {
           const int j = j0 + t;
           if (j < a.Jh) {
             const int jm = a.J - 1 - j;
@@ -456,33 +568,33 @@ __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int t
       }
     }
 #pragma unroll
-    for (int u = 0; u < kTcUnroll; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
       if (q >= kTcTasks) continue;
       const uint32_t off = sw128_off(q >> 3, q & 7);
-      float sv[8], dv[8];
+      float sv[C], dv[C];
 #pragma unroll
-      for (int t = 0; t < 8; ++t) {
+      for (int t = 0; t < C; ++t) {
         sv[t] = d[u][t] + e[u][t];
         dv[t] = d[u][t] - e[u][t];
       }
-      put_split8(sv, 0, 1, t0, t0 + kTile, off);
-      if (t1) put_split8(dv, 0, 1, t1, t1 + kTile, off);
+      put_split<Op>(sv, 0, 1, t0, t0 + kTile, off);
+      if (t1) put_split<Op>(dv, 0, 1, t1, t1 + kTile, off);
     }
   }
 }
 
-template <bool kForward>
+template <bool kForward, class Op>
 __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int rows, int k,
                                            uint8_t* t0, uint8_t* t1, int pt) {
   if (kForward) {
-    tc_produce_forward(a, m, tile, rows, k, t0, t1, pt);
+    tc_produce_forward<Op>(a, m, tile, rows, k, t0, t1, pt);
   } else {
     switch (m & 3) {
-      case 0: tc_produce_inverse<0>(a, m, tile, rows, k, t0, t1, pt); break;
-      case 1: tc_produce_inverse<1>(a, m, tile, rows, k, t0, t1, pt); break;
-      case 2: tc_produce_inverse<2>(a, m, tile, rows, k, t0, t1, pt); break;
-      default: tc_produce_inverse<3>(a, m, tile, rows, k, t0, t1, pt); break;
+      case 0: tc_produce_inverse<Op, 0>(a, m, tile, rows, k, t0, t1, pt); break;
+      case 1: tc_produce_inverse<Op, 1>(a, m, tile, rows, k, t0, t1, pt); break;
+      case 2: tc_produce_inverse<Op, 2>(a, m, tile, rows, k, t0, t1, pt); break;
+      default: tc_produce_inverse<Op, 3>(a, m, tile, rows, k, t0, t1, pt); break;
     }
   }
 }
@@ -491,7 +603,7 @@ __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int
 // and its lane 0 issues the MMAs, warps 2-7 produce the A tiles; all eight
 // warps drain TMEM in the epilogue (warp w reads lane quarter w mod 4 and
 // every other 16-column chunk).
-template <bool kForward>
+template <bool kForward, class Op>
 __global__ void __launch_bounds__(kTcThreads, 2)
 legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
                    const __grid_constant__ CUtensorMap tBl,
@@ -516,14 +628,14 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     if (!kForward) {
-      kblk[p] = (n_par[p] + 63) / 64;
-      ksteps[p] = (n_par[p] + 15) / 16;
+      kblk[p] = (n_par[p] + Op::kKB - 1) / Op::kKB;
+      ksteps[p] = (n_par[p] + Op::kStep - 1) / Op::kStep;
       ncols[p] = a.Nsub;
       cnt[p] = n_par[p];
     } else {
       cnt[p] = max(0, min(n_par[p] - lo, a.Nsub));
-      kblk[p] = cnt[p] ? (a.Jh + 63) / 64 : 0;
-      ksteps[p] = (a.Jh + 15) / 16;
+      kblk[p] = cnt[p] ? (a.Jh + Op::kKB - 1) / Op::kKB : 0;
+      ksteps[p] = (a.Jh + Op::kStep - 1) / Op::kStep;
       ncols[p] = round_up(cnt[p] > 0 ? cnt[p] : 16, 16);
     }
   }
@@ -531,8 +643,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
   if (kForward && cnt[0] == 0) return;
   if (!kForward && lo >= a.Jh) return;
   const int nblocks = kblk[0] + kblk[1];
-  const uint32_t tile_a = 128u * 128u;             // 128 rows x 64 bf16
-  const uint32_t tile_b = (uint32_t)a.Nsub * 128u;  // Nsub rows x 64 bf16
+  const uint32_t tile_a = 128u * 128u;             // 128 rows x 128 bytes of K
+  const uint32_t tile_b = (uint32_t)a.Nsub * 128u;  // Nsub rows x 128 bytes of K
   const uint32_t stage_bytes = 2 * tile_a + 2 * tile_b;
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
   uint8_t* base = smem_raw + pad;
@@ -560,7 +672,9 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
-  const int acc_cols = a.Nsub;  // parity p accumulates at column p * Nsub
+  // Parity p accumulates at column p * Nsub (its corrections, when separate,
+  // at (2 + p) * Nsub).
+  const int acc_cols = a.Nsub;
 
   if (threadIdx.x == 0) {
     // B producer (TMA).
@@ -573,11 +687,11 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       uint8_t* st = base + (size_t)s * stage_bytes;
       mbar_expect_tx(&full_bar[s], 2 * tile_b);
       const int yb = (m * 2 + p) * a.Nrows + lo;
-      tma_load_2d(st + 2 * tile_a, &tBh, &full_bar[s], k * 64, yb);
-      tma_load_2d(st + 2 * tile_a + tile_b, &tBl, &full_bar[s], k * 64, yb);
+      tma_load_2d(st + 2 * tile_a, &tBh, &full_bar[s], k * Op::kKB, yb);
+      tma_load_2d(st + 2 * tile_a + tile_b, &tBl, &full_bar[s], k * Op::kKB, yb);
     }
   } else if (threadIdx.x == 32) {
-    // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 16.
+    // MMA issuer: hi*hi + hi*lo + lo*hi per 32-byte K step.
     for (int i = 0; i < nblocks; ++i) {
       const int s = i % a.stages;
       const int use = i / a.stages;
@@ -587,7 +701,9 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       tc_seq(i, kblk[1], k, p);
       const int steps = min(4, (p ? ksteps[1] : ksteps[0]) - k * 4);
       const uint32_t d = tmem + (uint32_t)(p * acc_cols);
-      const uint32_t idesc = umma_idesc_bf16(p ? ncols[1] : ncols[0]);
+      // Corrections: their own accumulator, or the same one.
+      const uint32_t dc = Op::kSepAcc ? tmem + (uint32_t)((2 + p) * acc_cols) : d;
+      const uint32_t idesc = umma_idesc<Op>(p ? ncols[1] : ncols[0]);
       uint8_t* st = base + (size_t)s * stage_bytes;
       const uint64_t dah = umma_desc_sw128(st);
       const uint64_t dal = umma_desc_sw128(st + tile_a);
@@ -596,9 +712,9 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       for (int q = 0; q < steps; ++q) {
         const uint64_t off = (uint64_t)(2 * q);  // 32 bytes per K step, in 16 B units
         const uint32_t acc = (k > 0 || q > 0) ? 1u : 0u;
-        umma_bf16(d, dah + off, dbh + off, idesc, acc);
-        umma_bf16(d, dah + off, dbl + off, idesc, 1u);
-        umma_bf16(d, dal + off, dbh + off, idesc, 1u);
+        umma<Op>(d, dah + off, dbh + off, idesc, acc);
+        umma<Op>(dc, dah + off, dbl + off, idesc, Op::kSepAcc ? acc : 1u);
+        umma<Op>(dc, dal + off, dbh + off, idesc, 1u);
       }
       umma_commit(&empty_bar[s]);
     }
@@ -616,7 +732,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       if (two && u1 > 0 && !mbar_wait(&empty_bar[s1], (u1 - 1) & 1, a.err, 4)) break;
       uint8_t* t0 = base + (size_t)s0 * stage_bytes;
       uint8_t* t1 = two ? base + (size_t)s1 * stage_bytes : nullptr;
-      tc_produce<kForward>(a, m, tile, rows, k, t0, t1, pt);
+      tc_produce<kForward, Op>(a, m, tile, rows, k, t0, t1, pt);
       // Make the generic-proxy stores visible to the tensor cores.
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full_bar[s0]);
@@ -647,7 +763,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       int nb = 0;  // TMA-stored chunks of this warp (buffer nb & 1)
       for (int c = half; c < a.Nsub / 16; c += 2) {
         float e[16], od[16];
-        tmem_ld_pair(lane_base + c * 16, lane_base + acc_cols + c * 16, n_par[1] > 0, e, od);
+        tc_ld_acc<Op>(lane_base, acc_cols, c, n_par[1] > 0, e, od);
         const int jb = lo + 16 * c;
         const int jm = a.J - jb - 16;
         if (a.tma_out && jb + 16 <= a.Jh && jm >= a.Jh) {
@@ -744,7 +860,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       const int nchunks = (max(cnt[0], cnt[1]) + 15) / 16;
       for (int c = half; c < nchunks; c += 2) {
         float e[16], od[16];
-        tmem_ld_pair(lane_base + c * 16, lane_base + acc_cols + c * 16, cnt[1] > 0, e, od);
+        tc_ld_acc<Op>(lane_base, acc_cols, c, cnt[1] > 0, e, od);
         // Interleave parities: l = m + 32c + 2t + p.
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
@@ -795,18 +911,23 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-static int make_map(CUtensorMap* tm, const bf16* ptr, int inner, long long rows,
+// Table [rows][inner] of bf16 (tf32 = 0) or tf32-in-FP32 (tf32 = 1) entries;
+// the box is one 128-byte K block of box_rows rows, swizzled for the MMA.
+static int make_map(CUtensorMap* tm, const void* ptr, int tf32, int inner, long long rows,
                     int box_rows) {
   auto fn = encode_fn();
+  const int esz = tf32 ? 4 : 2;
+  const int kb = 128 / esz;
   DINO_REQUIRE(fn != nullptr, DINO_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
   DINO_REQUIRE(((uintptr_t)ptr & 15) == 0, DINO_ERR_ARG, "TMA base must be 16-byte aligned");
-  DINO_REQUIRE(inner % 64 == 0 && box_rows >= 8 && box_rows <= 256, DINO_ERR_ARG,
+  DINO_REQUIRE(inner % kb == 0 && box_rows >= 8 && box_rows <= 256, DINO_ERR_ARG,
                "bad TMA box");
   cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)inner * sizeof(bf16)};
-  cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+  cuuint64_t strides[1] = {(cuuint64_t)inner * esz};
+  cuuint32_t box[2] = {(cuuint32_t)kb, (cuuint32_t)box_rows};
   cuuint32_t elem[2] = {1u, 1u};
-  CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)ptr, dims, strides, box,
+  CUresult r = fn(tm, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16,
+                  2, (void*)ptr, dims, strides, box,
                   elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -858,13 +979,13 @@ struct TcShape {
   size_t smem;
 };
 
-static void tc_candidates(int nfull, std::vector<TcShape>* out) {
+static void tc_candidates(int nfull, int accs, std::vector<TcShape>* out) {
   int last_nsub = -1;
   for (int nsplit : {1, 2, 4}) {
     const int nsub = round_up((nfull + nsplit - 1) / nsplit, 16);
     if (nsub == last_nsub || (nsplit > 1 && nsub * (nsplit - 1) >= nfull)) continue;
     last_nsub = nsub;
-    if (tmem_cols_for(2 * nsub) > 512) continue;
+    if (tmem_cols_for(accs * nsub) > 512) continue;
     const size_t stage = 2 * 128 * 128 + 2 * (size_t)nsub * 128;
     for (int stages = 2; stages <= kMaxStages; ++stages) {
       const size_t smem = stage * stages + 1024;
@@ -893,9 +1014,20 @@ static TcArgs tc_args(const dino_plan* p, const TcTables* t, bool forward, int n
   a.Nrows = forward ? t->Nf : t->Np;
   a.Nsub = forward ? t->Nsub_fwd : t->Nsub_inv;
   a.stages = forward ? t->stages_fwd : t->stages_inv;
-  a.tmem_cols = tmem_cols_for(2 * a.Nsub);
+  a.tmem_cols = tmem_cols_for(tc_accumulators(t->tf32) * a.Nsub);
   a.err = t->d_err;
   return a;
+}
+
+// One launch of the contraction in the plan's operand format.
+template <bool kForward>
+static void tc_launch(const TcTables* t, dim3 grid, size_t smem, cudaStream_t st,
+                      const CUtensorMap& bh, const CUtensorMap& bl, const CUtensorMap& o2,
+                      const CUtensorMap& o1, const TcArgs& a) {
+  if (t->tf32)
+    legendre_tc_kernel<kForward, OpTf32><<<grid, kTcThreads, smem, st>>>(bh, bl, o2, o1, a);
+  else
+    legendre_tc_kernel<kForward, OpBf16><<<grid, kTcThreads, smem, st>>>(bh, bl, o2, o1, a);
 }
 
 template <bool kForward>
@@ -905,16 +1037,16 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
   const size_t lw2 = (size_t)p->lw * 2;
   CUtensorMap bh, bl;
   if (!kForward) {
-    DINO_TRY(make_map(&bh, t->Bih, t->Kp, (long long)lw2 * t->Np, c.Nsub));
-    DINO_TRY(make_map(&bl, t->Bil, t->Kp, (long long)lw2 * t->Np, c.Nsub));
+    DINO_TRY(make_map(&bh, t->Bih, t->tf32, t->Kp, (long long)lw2 * t->Np, c.Nsub));
+    DINO_TRY(make_map(&bl, t->Bil, t->tf32, t->Kp, (long long)lw2 * t->Np, c.Nsub));
   } else {
-    DINO_TRY(make_map(&bh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
-    DINO_TRY(make_map(&bl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
+    DINO_TRY(make_map(&bh, t->Bfh, t->tf32, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
+    DINO_TRY(make_map(&bl, t->Bfl, t->tf32, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
   }
   TcArgs a = tc_args(p, t, kForward, nf);
   a.Nsub = c.Nsub;
   a.stages = c.stages;
-  a.tmem_cols = tmem_cols_for(2 * c.Nsub);
+  a.tmem_cols = tmem_cols_for(tc_accumulators(t->tf32) * c.Nsub);
   a.out = out;
   CUtensorMap o2, o1;
   memset(&o2, 0, sizeof(o2));
@@ -930,7 +1062,7 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
   constexpr int kReps = 3;
   for (int r = 0; r <= kReps; ++r) {
     if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
-    legendre_tc_kernel<kForward><<<grid, kTcThreads, c.smem, 0>>>(bh, bl, o2, o1, a);
+    tc_launch<kForward>(t, grid, c.smem, 0, bh, bl, o2, o1, a);
     DINO_TRY(check_launch("legendre_tc (autotune)"));
   }
   DINO_CHECK_CUDA(cudaEventRecord(e1, 0));
@@ -959,7 +1091,7 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
   DINO_CHECK_CUDA(cudaEventCreate(&e1));
   auto tune = [&](bool forward) -> int {
     std::vector<TcShape> cands;
-    tc_candidates(forward ? t->Nf : t->Np, &cands);
+    tc_candidates(forward ? t->Nf : t->Np, tc_accumulators(t->tf32), &cands);
     float best = 1e30f;
     TcShape pick = cands.front();
     for (const TcShape& c : cands) {
@@ -981,8 +1113,8 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
       t->smem_fwd = pick.smem;
       t->us_fwd = best;
       t->tried_fwd = (int)cands.size();
-      DINO_TRY(make_map(&t->tBfh, t->Bfh, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
-      DINO_TRY(make_map(&t->tBfl, t->Bfl, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
+      DINO_TRY(make_map(&t->tBfh, t->Bfh, t->tf32, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
+      DINO_TRY(make_map(&t->tBfl, t->Bfl, t->tf32, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
     } else {
       t->nsplit_inv = pick.nsplit;
       t->Nsub_inv = pick.Nsub;
@@ -990,8 +1122,8 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
       t->smem_inv = pick.smem;
       t->us_inv = best;
       t->tried_inv = (int)cands.size();
-      DINO_TRY(make_map(&t->tBih, t->Bih, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
-      DINO_TRY(make_map(&t->tBil, t->Bil, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
+      DINO_TRY(make_map(&t->tBih, t->Bih, t->tf32, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
+      DINO_TRY(make_map(&t->tBil, t->Bil, t->tf32, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
     }
     return DINO_OK;
   };
@@ -1009,10 +1141,10 @@ std::string tc_describe(dino_plan* p) {
   if (!t) return "";
   char buf[512];
   snprintf(buf, sizeof(buf),
-           "tcgen05 split-BF16 Legendre autotuned on %d fields: inverse %d N ranges of "
+           "tcgen05 %s Legendre autotuned on %d fields: inverse %d N ranges of "
            "%d rows, %d stages (%.1f us, %d shapes tried); forward %d N ranges of %d rows, "
            "%d stages (%.1f us, %d shapes tried)",
-           t->tuned_fields, t->nsplit_inv, t->Nsub_inv, t->stages_inv, t->us_inv,
+           t->tf32 ? "split-TF32" : "split-BF16", t->tuned_fields, t->nsplit_inv, t->Nsub_inv, t->stages_inv, t->us_inv,
            t->tried_inv, t->nsplit_fwd, t->Nsub_fwd, t->stages_fwd, t->us_fwd, t->tried_fwd);
   return buf;
 }
@@ -1024,33 +1156,52 @@ int tc_tables_build(dino_plan* p) {
                "tensor-core path supports at most 512 total wavenumbers");
   TcTables* t = new TcTables();
   p->tc = t;
+  t->tf32 = p->precision == DINO_PREC_TF32X3;
+  const int kb = t->tf32 ? OpTf32::kKB : OpBf16::kKB;
+  const size_t esz = t->tf32 ? sizeof(float) : sizeof(bf16);
   const int half_l = (p->L + 1) / 2;
-  t->Kp = round_up(half_l, 64);
+  t->Kp = round_up(half_l, kb);
   t->Np = round_up(p->Jh, 16);
-  t->Kj = round_up(p->Jh, 64);
+  t->Kj = round_up(p->Jh, kb);
   t->Nf = round_up(half_l, 16);
   const size_t lw2 = (size_t)p->lw * 2;
   const size_t nBi = lw2 * t->Np * t->Kp, nBf = lw2 * t->Nf * t->Kj;
-  DINO_CHECK_CUDA(cudaMalloc(&t->Bih, nBi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Bil, nBi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Bfh, nBf * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMalloc(&t->Bfl, nBf * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Bih, 0, nBi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Bil, 0, nBi * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Bfh, 0, nBf * sizeof(bf16)));
-  DINO_CHECK_CUDA(cudaMemset(t->Bfl, 0, nBf * sizeof(bf16)));
+  DINO_CHECK_CUDA(cudaMalloc(&t->Bih, nBi * esz));
+  DINO_CHECK_CUDA(cudaMalloc(&t->Bil, nBi * esz));
+  DINO_CHECK_CUDA(cudaMalloc(&t->Bfh, nBf * esz));
+  DINO_CHECK_CUDA(cudaMalloc(&t->Bfl, nBf * esz));
+  DINO_CHECK_CUDA(cudaMemset(t->Bih, 0, nBi * esz));
+  DINO_CHECK_CUDA(cudaMemset(t->Bil, 0, nBi * esz));
+  DINO_CHECK_CUDA(cudaMemset(t->Bfh, 0, nBf * esz));
+  DINO_CHECK_CUDA(cudaMemset(t->Bfl, 0, nBf * esz));
   DINO_CHECK_CUDA(cudaMalloc(&t->d_err, sizeof(int)));
   DINO_CHECK_CUDA(cudaMemset(t->d_err, 0, sizeof(int)));
   dim3 grid(ceil_div(p->Jh, 128), p->lw);
-  tc_table_kernel<<<grid, 128>>>(p->lw, p->L, p->Jh, p->d_x64, t->Kp, t->Np, t->Kj, t->Nf,
-                                 t->Bih, t->Bil, t->Bfh, t->Bfl);
+  if (t->tf32) {
+    tc_table_kernel<float><<<grid, 128>>>(
+        p->lw, p->L, p->Jh, p->d_x64, t->Kp, t->Np, t->Kj, t->Nf, (float*)t->Bih,
+        (float*)t->Bil, (float*)t->Bfh, (float*)t->Bfl);
+  } else {
+    tc_table_kernel<bf16><<<grid, 128>>>(p->lw, p->L, p->Jh, p->d_x64, t->Kp, t->Np, t->Kj,
+                                         t->Nf, (bf16*)t->Bih, (bf16*)t->Bil, (bf16*)t->Bfh,
+                                         (bf16*)t->Bfl);
+  }
   DINO_TRY(check_launch("tc_table"));
-  DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kTcSmemLimit));
-  DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kTcSmemLimit));
+  if (t->tf32) {
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<false, OpTf32>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmemLimit));
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<true, OpTf32>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmemLimit));
+  } else {
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<false, OpBf16>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmemLimit));
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(legendre_tc_kernel<true, OpBf16>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmemLimit));
+  }
   DINO_CHECK_CUDA(cudaDeviceSynchronize());
   return tc_autotune(p, t);
 }
@@ -1085,8 +1236,7 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
   CUtensorMap o2, o1;
   tc_out_maps(p, &a, out, nf, &o2, &o1);
   dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_inv);
-  legendre_tc_kernel<false><<<grid, kTcThreads, t->smem_inv, st>>>(t->tBih, t->tBil, o2, o1,
-                                                                   a);
+  tc_launch<false>(t, grid, t->smem_inv, st, t->tBih, t->tBil, o2, o1, a);
   return check_launch("legendre_tc_inverse");
 }
 
@@ -1101,8 +1251,7 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
   CUtensorMap unused;  // the forward epilogue uses row stores
   memset(&unused, 0, sizeof(unused));
   dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_fwd);
-  legendre_tc_kernel<true><<<grid, kTcThreads, t->smem_fwd, st>>>(t->tBfh, t->tBfl, unused,
-                                                                  unused, a);
+  tc_launch<true>(t, grid, t->smem_fwd, st, t->tBfh, t->tBfl, unused, unused, a);
   return check_launch("legendre_tc_forward");
 }
 
@@ -1125,7 +1274,9 @@ extern "C" int dino_plan_describe(dino_plan* p, char* buf, size_t len) {
   snprintf(head, sizeof(head),
            "grid %d x %d nodes, %d x %d modal, Legendre %s, batch capacity %d fields",
            p->I, p->J, p->M, p->L,
-           p->precision == DINO_PREC_BF16X3 ? "split-BF16 (tcgen05)" : "FP32 (SIMT)",
+           p->precision == DINO_PREC_BF16X3   ? "split-BF16 (tcgen05)"
+           : p->precision == DINO_PREC_TF32X3 ? "split-TF32 (tcgen05)"
+                                              : "FP32 (SIMT)",
            p->max_fields);
   std::string s = head;
   const std::string tc = dino::tc_describe(p);

@@ -298,7 +298,7 @@ static int plan_build(dino_plan* p, const dino_grid_desc* d) {
   DINO_CHECK_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
   DINO_CHECK_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
 
-  if (p->precision == DINO_PREC_BF16X3) DINO_TRY(tc_tables_build(p));
+  if (p->precision != DINO_PREC_FP32) DINO_TRY(tc_tables_build(p));
   DINO_CHECK_CUDA(cudaDeviceSynchronize());
   return DINO_OK;
 }
@@ -330,7 +330,8 @@ int dino_plan_create(const dino_grid_desc* d, int32_t max_fields,
                "`real_basis` requires nodes >= wavenumbers");
   DINO_REQUIRE(d->latitude_spacing >= 0 && d->latitude_spacing <= 2,
                DINO_ERR_ARG, "unknown latitude spacing");
-  DINO_REQUIRE(precision == DINO_PREC_FP32 || precision == DINO_PREC_BF16X3,
+  DINO_REQUIRE(precision == DINO_PREC_FP32 || precision == DINO_PREC_BF16X3 ||
+                   precision == DINO_PREC_TF32X3,
                DINO_ERR_ARG, "unknown precision");
   DINO_REQUIRE(max_fields >= 1, DINO_ERR_ARG, "max_fields must be >= 1");
   dino_plan* p = new dino_plan();

@@ -344,7 +344,7 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 
 int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
                      cudaStream_t st) {
-  if (p->precision == DINO_PREC_BF16X3)
+  if (p->precision != DINO_PREC_FP32)
     return tc_legendre_inverse(p, in, out, nf, st);
   dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
@@ -354,7 +354,7 @@ int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
 
 int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
                      cudaStream_t st) {
-  if (p->precision == DINO_PREC_BF16X3)
+  if (p->precision != DINO_PREC_FP32)
     return tc_legendre_forward(p, G, out, nf, st);
   if (p->L > 64) {
     dim3 grid(ceil_div(p->L, 64), ceil_div(2 * nf, kLegTB), p->lw);
@@ -889,7 +889,7 @@ int l2_chunk(dino_plan* p, int nf, int work_fields) {
   int cap = (int)((48ull << 20) / (per_field ? per_field : 1));
   if (cap < 1) cap = 1;
   if (cap > work_fields) cap = work_fields;
-  if (p->precision == DINO_PREC_BF16X3 && cap >= 64) {
+  if (p->precision != DINO_PREC_FP32 && cap >= 64) {
     cap = cap / 64 * 64;
     const int chunks = (nf + cap - 1) / cap;
     const int even = (nf + chunks - 1) / chunks;

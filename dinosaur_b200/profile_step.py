@@ -27,7 +27,7 @@ def main():
   ap.add_argument('--held-suarez', action='store_true')
   ap.add_argument('--moist', action='store_true',
                   help='specific humidity and two passive tracers')
-  ap.add_argument('--precision', default='fp32', choices=['fp32', 'bf16x3'])
+  ap.add_argument('--precision', default='fp32', choices=['fp32', 'bf16x3', 'tf32x3'])
   ap.add_argument('--steps', type=int, default=3)
   ap.add_argument('--dt-minutes', type=float, default=15.0)
   args = ap.parse_args()

@@ -297,8 +297,9 @@ class CudaSphericalHarmonics(SphericalHarmonics):
   """Real-layout spherical harmonics on sm_100a (same layout as
   RealSphericalHarmonics, spherical_harmonic.py:161-283).
 
-  ``precision`` selects the Legendre contraction: 'fp32' (SIMT FMA) or
-  'bf16x3' (tcgen05 tensor cores, split-BF16 with FP32 accumulation).
+  ``precision`` selects the Legendre contraction: 'fp32' (SIMT FMA),
+  'bf16x3' or 'tf32x3' (tcgen05 tensor cores, operands split into bf16 or
+  tf32 hi / lo pairs, three products per pair, FP32 accumulation).
   """
 
   precision: str = 'fp32'

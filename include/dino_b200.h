@@ -67,6 +67,7 @@ extern "C" {
 /* Legendre-contraction arithmetic. */
 #define DINO_PREC_FP32 0    /* SIMT FP32 FMA (plain form)                          */
 #define DINO_PREC_BF16X3 1  /* tcgen05 kind::f16, hi*hi + hi*lo + lo*hi, FP32 accum */
+#define DINO_PREC_TF32X3 2  /* tcgen05 kind::tf32, hi*hi + hi*lo + lo*hi, FP32 accum */
 
 /* Modal operators for dino_modal_op. */
 #define DINO_OP_D_DLON 0
@@ -113,7 +114,7 @@ DINO_API int dino_plan_legendre_column(const dino_plan* plan, int32_t m, int32_t
                               double* host_out);
 
 /* A one-line description of the plan (shapes, Legendre form, and for the
- * split-BF16 form the launch shapes its autotuner chose at creation and
+ * tensor-core forms the launch shapes its autotuner chose at creation and
  * their measured times), NUL-terminated and truncated to len bytes.  No
  * counterpart in the reference. */
 DINO_API int dino_plan_describe(dino_plan* plan, char* buf, size_t len);

@@ -4,7 +4,7 @@
 * a field's result does not depend on the batch around it: ragged batch
   sizes that split into L2-sized chunks (TL255: 64 fields per chunk) and
   batches larger than a plan's workspace give bit-identical results to
-  single-field calls, in both Legendre forms;
+  single-field calls, in every Legendre form;
 * grids with nodes at the poles ('equiangular_with_poles') match the FP64
   oracle (<= 2e-6 max-abs relative, as the other one-way transforms).
 """
@@ -29,7 +29,7 @@ def grid(name, precision='fp32', **kw):
   return getattr(sh.Grid, name)(spherical_harmonics_impl=impl, **kw)
 
 
-@pytest.mark.parametrize('precision', ['fp32', 'bf16x3'])
+@pytest.mark.parametrize('precision', ['fp32', 'bf16x3', 'tf32x3'])
 def test_empty_batches(precision):
   g = grid('T42', precision)
   x = torch.empty((0,) + g.modal_shape, device='cuda')
@@ -40,7 +40,7 @@ def test_empty_batches(precision):
   _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
 
 
-@pytest.mark.parametrize('precision', ['fp32', 'bf16x3'])
+@pytest.mark.parametrize('precision', ['fp32', 'bf16x3', 'tf32x3'])
 def test_fields_do_not_depend_on_their_batch(precision):
   g = grid('TL255', precision)
   og = osht.Grid.TL255()
