@@ -32,6 +32,9 @@ sys.path.insert(0, ROOT)
 
 GRID = dict(name='TL255', max_wavenumber=255, gaussian_nodes=128)
 FIELDS = 128
+# (longitude wavenumbers, total wavenumbers, longitude nodes, latitude nodes)
+GRIDS = {'TL255': (256, 257, 512, 256), 'T85': (86, 87, 256, 128)}
+FORMS = ('fp32', 'bf16x3', 'tf32x3')
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
@@ -45,27 +48,27 @@ PHASE_TRAFFIC = {
     ('fp32', 'legendre_inverse'): 58467584 + 19169536,
     ('fp32', 'fourier_inverse'): 67018752 + 23803136,
     ('fp32', 'fourier_forward'): 67136000 + 25746688,
-    ('fp32', 'legendre_forward'): 84814592 + 29821696,
+    ('fp32', 'legendre_forward'): 84916224 + 27469824,
+    ('tf32x3', 'legendre_inverse'): 118548480 + 34110976,
+    ('tf32x3', 'legendre_forward'): 151210240 + 43932416,
 }
 
 
-def workload_dims():
-  lw = GRID['max_wavenumber'] + 1
-  L = GRID['max_wavenumber'] + 2
-  I, J = 4 * GRID['gaussian_nodes'], 2 * GRID['gaussian_nodes']
+def workload_dims(name=GRID['name']):
+  lw, L, I, J = GRIDS[name]
   M = 2 * lw - 1
   n_tri = L + 2 * sum(L - m for m in range(1, lw))
   return lw, L, I, J, M, n_tri
 
 
-def sht_flops(fields):
-  _, _, _, J, _, n_tri = workload_dims()
+def sht_flops(fields, name=GRID['name']):
+  _, _, _, J, _, n_tri = workload_dims(name)
   return 2.0 * 2.0 * J * n_tri * fields  # 2 directions x 2 flops x J x N_tri
 
 
-def modal_input(fields, seed=0):
+def modal_input(fields, seed=0, name=GRID['name']):
   """Seeded complex Gaussians (Re -> cos row, Im -> sin row) * (l+1)^-1.5."""
-  lw, L, _, _, M, _ = workload_dims()
+  lw, L, _, _, M, _ = workload_dims(name)
   rng = np.random.default_rng(seed)
   re = rng.standard_normal((fields, lw, L))
   im = rng.standard_normal((fields, lw, L))
@@ -287,8 +290,8 @@ def aggregate_tflops(flops_per_rank, world, ms_max):
 # GPU arm
 # ---------------------------------------------------------------------------
 
-def phase_bytes(phase, fields, precision):
-  lw, L, I, J, M, n_tri = workload_dims()
+def phase_bytes(phase, fields, precision, name=GRID['name']):
+  lw, L, I, J, M, n_tri = workload_dims(name)
   Jh = J // 2
   table_elems = Jh * sum(L - m for m in range(lw))
   # fp32 table, bf16 hi + lo (4 bytes per entry) or tf32 hi + lo (8 bytes)
@@ -300,6 +303,125 @@ def phase_bytes(phase, fields, precision):
           'fourier_inverse': fourier + nodal,
           'fourier_forward': nodal + fourier,
           'legendre_forward': fourier + modal + table_bytes}[phase]
+
+
+def time_phases(torch, plan, x, name, reps):
+  """Milliseconds per launch of each transform phase over x's fields (CUDA
+  events on the launching stream, after two untimed launches)."""
+  from dinosaur_b200 import _lib
+  from dinosaur_b200 import spherical_harmonic as sh
+  lw, L, I, J, M, _ = workload_dims(name)
+  fields = x.shape[0]
+  stream = torch.cuda.current_stream()
+  buf_f = torch.empty((fields, M, J), device='cuda')
+  buf_n = torch.empty((fields, I, J), device='cuda')
+  buf_m = torch.empty((fields, M, L), device='cuda')
+  phases = [('legendre_inverse', 0, x, buf_f), ('fourier_inverse', 1, buf_f, buf_n),
+            ('fourier_forward', 2, buf_n, buf_f), ('legendre_forward', 3, buf_f, buf_m)]
+  phase_ms = {}
+  for pname, code, src, dst in phases:
+    for _ in range(2):
+      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
+                                           fields, sh.stream_handle()))
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(reps):
+      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
+                                           fields, sh.stream_handle()))
+    a1.record(stream)
+    torch.cuda.synchronize()
+    phase_ms[pname] = a0.elapsed_time(a1) / reps
+  return phase_ms
+
+
+def compute_peaks(torch, measured):
+  """Compute-roofline denominators measured on this device: the FP32 FMA rate
+  (the library's microbenchmark; the SIMT Legendre's bound) and a cuBLAS TF32
+  GEMM (the split-TF32 form's), best of three; BF16 and HBM from the
+  measured-peaks file."""
+  from dinosaur_b200 import _lib
+  import ctypes
+  fma = []
+  for _ in range(3):
+    v = ctypes.c_double(0.0)
+    _lib.check(_lib.lib().dino_measure_fp32_fma_peak(1 << 14, ctypes.byref(v)))
+    fma.append(v.value)
+  n = 8192
+  a = torch.randn(n, n, device='cuda')
+  b = torch.randn(n, n, device='cuda')
+  old = torch.backends.cuda.matmul.allow_tf32
+  torch.backends.cuda.matmul.allow_tf32 = True
+  try:
+    tf32 = []
+    for _ in range(3):
+      for _ in range(3):
+        c = a @ b
+      e0 = torch.cuda.Event(enable_timing=True)
+      e1 = torch.cuda.Event(enable_timing=True)
+      e0.record()
+      for _ in range(10):
+        c = a @ b
+      e1.record()
+      torch.cuda.synchronize()
+      tf32.append(10 * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+  finally:
+    torch.backends.cuda.matmul.allow_tf32 = old
+  del a, b, c
+  return {'fp32_fma_tflops': max(fma), 'tf32_gemm_tflops': max(tf32),
+          'bf16_gemm_tflops': measured.get('bf16_tflops'),
+          'hbm_gbs': measured.get('hbm_gbs'),
+          'how': 'fp32: dino_measure_fp32_fma_peak (2048 threads x 8 FMA chains per SM); '
+                 'tf32: cuBLAS 8192^3 GEMM via torch, allow_tf32; bf16 / hbm: '
+                 'MEASURED_PEAKS.json'}
+
+
+def legendre_forms(torch, args, peaks):
+  """Each Legendre form (plain FP32 SIMT, split-BF16, split-TF32) on the SHT
+  microbenchmark at TL255 and T85 x 128 fields: pair time and TFLOP/s,
+  round-trip error, per-phase times, and each Legendre phase against the HBM
+  roofline (algorithmic bytes) and its arithmetic pipe's peak (folded
+  2 Jh N_tri flops per field, times the 3 products of a split form)."""
+  from dinosaur_b200 import spherical_harmonic as sh
+  pipes = {'fp32': ('fp32 FMA (SIMT)', peaks.get('fp32_fma_tflops'), 1),
+           'bf16x3': ('bf16 tensor', peaks.get('bf16_gemm_tflops'), 3),
+           'tf32x3': ('tf32 tensor', peaks.get('tf32_gemm_tflops'), 3)}
+  stream = torch.cuda.current_stream()
+  out = {}
+  for name in ('TL255', 'T85'):
+    lw, L, I, J, M, n_tri = workload_dims(name)
+    x = torch.as_tensor(modal_input(FIELDS, 0, name), device='cuda')
+    for form in FORMS:
+      impl = functools.partial(sh.CudaSphericalHarmonics, precision=form)
+      plan = getattr(sh.Grid, name)(spherical_harmonics_impl=impl).plan
+      for _ in range(args.warmup):
+        y = plan.forward(plan.inverse(x))
+      torch.cuda.synchronize()
+      rt = float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x))
+      b0 = torch.cuda.Event(enable_timing=True)
+      b1 = torch.cuda.Event(enable_timing=True)
+      b0.record(stream)
+      for _ in range(args.steps):
+        y = plan.forward(plan.inverse(x))
+      b1.record(stream)
+      torch.cuda.synchronize()
+      ms = b0.elapsed_time(b1) / args.steps
+      phase_ms = time_phases(torch, plan, x, name, max(5, args.steps))
+      label, peak, mult = pipes[form]
+      folded = FIELDS * 2.0 * ((J + 1) // 2) * n_tri
+      entry = {'ms_per_pair': ms, 'tflops': aggregate_tflops(sht_flops(FIELDS, name), 1, ms),
+               'round_trip_rel_l2': rt, 'phase_ms': phase_ms, 'pipe': label}
+      for ph in ('legendre_inverse', 'legendre_forward'):
+        t = phase_ms[ph] * 1e-3
+        entry[ph] = {
+            'hbm_frac': (phase_bytes(ph, FIELDS, form, name) / t / 1e9 / peaks['hbm_gbs']
+                         if peaks.get('hbm_gbs') else None),
+            'pipe_frac': mult * folded / t / 1e12 / peak if peak else None}
+      out.setdefault(name, {})[form] = entry
+      del plan, y
+    del x
+    torch.cuda.empty_cache()
+  return out
 
 
 def run_ours(args):
@@ -433,26 +555,7 @@ def run_ours(args):
                   torch.linalg.vector_norm(y))
 
   # Per-phase kernel timing (live CUDA events on the launching stream).
-  buf_f = torch.empty((fields, M, J), device='cuda')
-  buf_n = torch.empty((fields, I, J), device='cuda')
-  buf_m = torch.empty((fields, M, L), device='cuda')
-  phases = [('legendre_inverse', 0, x, buf_f), ('fourier_inverse', 1, buf_f, buf_n),
-            ('fourier_forward', 2, buf_n, buf_f), ('legendre_forward', 3, buf_f, buf_m)]
-  phase_ms = {}
-  reps = max(5, args.steps)
-  for name, code, src, dst in phases:
-    for _ in range(2):
-      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
-                                           fields, sh.stream_handle()))
-    a0 = torch.cuda.Event(enable_timing=True)
-    a1 = torch.cuda.Event(enable_timing=True)
-    a0.record(stream)
-    for _ in range(reps):
-      _lib.check(_lib.lib().dino_sht_phase(plan.handle, code, sh.ptr(src), sh.ptr(dst),
-                                           fields, sh.stream_handle()))
-    a1.record(stream)
-    torch.cuda.synchronize()
-    phase_ms[name] = a0.elapsed_time(a1) / reps
+  phase_ms = time_phases(torch, plan, x, GRID['name'], max(5, args.steps))
   dominant = max(phase_ms, key=phase_ms.get)
   peaks = {}
   try:
@@ -467,31 +570,20 @@ def run_ours(args):
   cap = max(1, (48 << 20) // per_field)
   chunks = -(-fields // min(cap, plan.max_fields))
   # Per chunk: inverse Legendre, inverse FFT, forward FFT, forward Legendre
-  # (the split-BF16 operand split and fold run inside the Legendre kernels).
+  # (the split forms' operand split and fold run inside the Legendre kernels).
   launches_per_step = chunks * 4
 
   extra = {}
   if not args.no_extra and world == 1:
-    # The other Legendre forms on the same workload (plain FP32, split-BF16,
-    # split-TF32), for the comparison of speed and round-trip error.
-    for other in [f for f in ('fp32', 'bf16x3', 'tf32x3') if f != args.precision]:
-      g2 = make_grid(other)
-      for _ in range(args.warmup):
-        y2 = g2.plan.forward(g2.plan.inverse(x))
-      torch.cuda.synchronize()
-      rt2 = float(torch.linalg.vector_norm(y2 - x) / torch.linalg.vector_norm(x))
-      b0 = torch.cuda.Event(enable_timing=True)
-      b1 = torch.cuda.Event(enable_timing=True)
-      b0.record(stream)
-      for _ in range(args.steps):
-        y2 = g2.plan.forward(g2.plan.inverse(x))
-      b1.record(stream)
-      torch.cuda.synchronize()
-      ms2 = b0.elapsed_time(b1) / args.steps
-      extra['sht_' + other] = {'value': aggregate_tflops(sht_flops(fields), 1, ms2),
-                               'unit': 'TFLOP/s', 'ms_per_step': ms2,
-                               'round_trip_rel_l2': rt2}
-      del g2, y2
+    # Every Legendre form at TL255 and T85 with its rooflines; the other
+    # forms' TL255 pairs are also listed as sht_<form>.
+    extra['peaks'] = compute_peaks(torch, peaks)
+    extra['legendre_forms'] = legendre_forms(torch, args, extra['peaks'])
+    for other in [f for f in FORMS if f != args.precision]:
+      e = extra['legendre_forms']['TL255'][other]
+      extra['sht_' + other] = {'value': e['tflops'], 'unit': 'TFLOP/s',
+                               'ms_per_step': e['ms_per_pair'],
+                               'round_trip_rel_l2': e['round_trip_rel_l2']}
     extra.update(pe_extras(torch))
 
   if rank == 0:

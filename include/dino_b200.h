@@ -289,6 +289,13 @@ DINO_API int dino_pe_step_vjp(dino_pe* pe, const float* d_state,
                               const float* d_out_ct, float* d_in_ct, double dt,
                               const double* host_filter, void* stream);
 
+/* Measures the device's peak FP32 FMA rate, the compute roofline of the
+ * plain FP32 Legendre contraction: every SM runs 2048 threads of 8
+ * independent FMA chains for `iters` iterations, timed with CUDA events
+ * after one warm-up launch; *tflops = 2 x FMAs / time.  Synchronizes the
+ * device.  No counterpart in the reference. */
+DINO_API int dino_measure_fp32_fma_peak(int32_t iters, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif
