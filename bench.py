@@ -632,8 +632,10 @@ def pe_extras(torch):
   Synthetic states near rest (seeded small modal noise); the moist case adds
   specific humidity (5 g/kg mean) and two passive tracers.  Each case runs
   with the plain FP32 and the split-BF16 Legendre contraction where both are
-  listed (the dry TL255 case also with split-TF32)."""
+  listed (the dry TL255 case also with split-TF32, and on 32 analytic hybrid
+  sigma-pressure levels with split-BF16)."""
   from dinosaur_b200 import coordinate_systems, held_suarez, primitive_equations as pe
+  from dinosaur_b200 import hybrid_coordinates
   from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
   from dinosaur_b200 import time_integration as ti, units
   out = {}
@@ -644,19 +646,22 @@ def pe_extras(torch):
       ('TL255_L32_dry', 'TL255', 32, 1, False, False, 6, 'fp32'),
       ('TL255_L32_dry_bf16x3', 'TL255', 32, 1, False, False, 6, 'bf16x3'),
       ('TL255_L32_dry_tf32x3', 'TL255', 32, 1, False, False, 6, 'tf32x3'),
+      ('TL255_L32_hybrid_dry_bf16x3', 'TL255', 32, 1, False, False, 6, 'bf16x3'),
       ('TL255_L32_moist3_x4', 'TL255', 32, 4, False, True, 6, 'fp32'),
       ('TL255_L32_moist3_x4_bf16x3', 'TL255', 32, 4, False, True, 6, 'bf16x3'),
   ]
   for name, grid_name, layers, members, hs, moist, dt_min, precision in cases:
     impl = functools.partial(sh.CudaSphericalHarmonics, precision=precision)
     g = getattr(sh.Grid, grid_name)(spherical_harmonics_impl=impl)
-    vert = sigma_coordinates.SigmaCoordinates.equidistant(layers)
+    hybrid = 'hybrid' in name
+    vert = (hybrid_coordinates.HybridCoordinates.analytic_levels(layers) if hybrid
+            else sigma_coordinates.SigmaCoordinates.equidistant(layers))
     coords = coordinate_systems.CoordinateSystem(g, vert)
     ps = units.SimUnits()
     tref = np.full(layers, 285.0) if hs else np.linspace(220.0, 288.0, layers)
-    eq = pe.PrimitiveEquationsSigma(
-        tref, np.zeros(g.modal_shape, np.float32), coords, ps,
-        humidity_key='specific_humidity' if moist else None)
+    eq_cls = pe.PrimitiveEquationsHybrid if hybrid else pe.PrimitiveEquationsSigma
+    eq = eq_cls(tref, np.zeros(g.modal_shape, np.float32), coords, ps,
+                humidity_key='specific_humidity' if moist else None)
     if hs:
       eq = ti.compose_equations([eq, held_suarez.HeldSuarezForcingSigma(coords, ps, tref)])
     dt = units.nondim_time(dt_min * 60.0)
@@ -680,8 +685,13 @@ def pe_extras(torch):
       tracers = {'specific_humidity': t(5e-3 * const + noise(shape, 1e-6)),
                  'tracer_a': t(const + noise(shape)),
                  'tracer_b': t(const + noise(shape))}
+    lnps = noise(lshape)
+    if hybrid:
+      # Hybrid levels need a physical surface pressure: 1e5 Pa as the l = 0
+      # term (the constant field 1 has the coefficient 2 sqrt(pi)).
+      lnps[..., 0, 0] += np.log(units.nondim_pressure(1e5)) * 2.0 * np.sqrt(np.pi)
     state = pe.State(t(noise(shape)), t(noise(shape)), t(noise(shape)),
-                     t(noise(lshape)), tracers=tracers)
+                     t(lnps), tracers=tracers)
     eng = eq.engine(state)
     buf = eng.pack(state)
     eng.step_(buf, dt, step.filter_scaling, 3, graph=True)

@@ -97,6 +97,12 @@ class PEDesc(ctypes.Structure):
       ('hs_maxT', ctypes.c_double),
       ('hs_dTy', ctypes.c_double),
       ('hs_dThz', ctypes.c_double),
+      ('vertical_scheme', ctypes.c_int32),
+      ('hybrid_a_boundaries', _DP),
+      ('hybrid_b_boundaries', _DP),
+      ('reference_surface_pressure', ctypes.c_double),
+      ('implicit_lnps_column', _DP),
+      ('implicit_thickness', _DP),
   ]
 
 

@@ -64,6 +64,14 @@ struct dino_pe {
          hs_minT = 0, hs_maxT = 0, hs_dTy = 0, hs_dThz = 0;
   // Host copies (FP64).
   std::vector<double> dsig, c2c, alpha, tref, sumsig, sigma, G, H;
+  // The implicit operator's ln ps column and ln ps row: R T_ref and the
+  // sigma thickness on sigma levels; on hybrid levels the Simmons-Burridge
+  // pressure-gradient coefficient and da / p_s_ref + db at p_s_ref.
+  std::vector<double> imp_col, imp_row;
+  // Hybrid sigma-pressure levels (vertical_scheme 1).
+  int hybrid = 0, hum_hyb = -1;
+  double ps_ref = 0;
+  float* d_hyb = nullptr;  // per-level constants of pe_nodal_hybrid_kernel
   // Device constants.
   float* d_levpack = nullptr;  // per-level constants, packed per level (kLevPack)
   int sms = 148;               // multiprocessors of the device
@@ -144,6 +152,8 @@ struct PrepArgs {
   int M, L, lw;
   int p_div, p_vort, p_lnps, p_hum;  // state planes
   int a_u, a_v, a_gqx, a_gqy, a_gx, a_gy, a_laplnps;  // aux planes (-1 = unused)
+  // Hybrid levels: ln p_s without its l = 0 coefficient (-1 = unused).
+  int a_lnpsdev = -1;
   const float* deriv;
   const float* lap;
   const float* invlap;
@@ -231,6 +241,8 @@ __global__ void __launch_bounds__(kModalTX * kModalTY) pe_prep_kernel(PrepArgs a
       a.aux[((size_t)a.a_gy + mb) * ML + idx] = nu.dlat(lnps) * ir;
       if (a.hum >= 0)
         a.aux[((size_t)a.a_laplnps + mb) * ML + idx] = lnps[idx] * a.lap[l];
+      if (a.a_lnpsdev >= 0)
+        a.aux[((size_t)a.a_lnpsdev + mb) * ML + idx] = idx == 0 ? 0.f : lnps[idx];
     }
   }
 }
@@ -648,6 +660,261 @@ __global__ void __launch_bounds__(kNodalCols * kNodalMaxChunks)
 #pragma unroll
     for (int i = 0; i < V; ++i) l[i] = -Fe[i];
     st_vec(a.fwd + ((size_t)a.o_lnps + mb) * IJ + col, l);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nodal column kernel on hybrid sigma-pressure levels (Simmons & Burridge)
+// ---------------------------------------------------------------------------
+
+// Per-level constants of pe_nodal_hybrid_kernel, kHybPack floats per level k
+// (0 = top), all at the reference surface pressure p_s_ref except a, b:
+//   0 a_{k-1/2}  1 b_{k-1/2}  2 da_k  3 db_k  4 T_ref,k  5 alpha_k
+//   6 log(p_{k+1/2} / p_{k-1/2})  7 s_k = W_k p_s / max(dp_k, 1e-6 p_s)
+//   8 p_{k-1/2}  9 dp_k  10 W_k = log-ratio_k b_{k-1/2} + alpha_k db_k
+// followed by a, b and p (at p_s_ref) of the lowest interface.
+constexpr int kHybPack = 12;
+constexpr int kHybThreads = 128;
+
+struct HybridArgs {
+  const float* nod;         // nodal inverse-transform planes
+  float* fwd;               // nodal forward-transform planes
+  const float* lev;         // [K][kHybPack], a_K, b_K, p_K
+  const float* lat;         // sec^2 [J], 2 Omega sin [J]
+  const float* lnps_modal;  // modal ln p_s of the state, [mem][M][L]
+  unsigned ML;
+  int K, mem, nT, hum, vadv, tref_varies, I, J;
+  int p_vort, p_div, p_temp, p_tr, p_u, p_v, p_gx, p_gy, p_lnps;
+  int o_Au, o_Av, o_KE, o_uT, o_vT, o_Tn, o_tr, o_lnps;
+  float R, kappa, ps_ref, Rv_over_R, Cpv_over_Cp;
+  double ln_ps_ref, inv_y00;  // FP64: their difference below is ~1e-2 of each
+};
+
+// One thread per column (member blockIdx.y): the nodal explicit terms of
+// PrimitiveEquationsHybrid (primitive_equations.py:1536-1603, :2058-2360).
+//
+// FP32 accuracy.  Nodal ln p_s is ~45 (nondimensional pressure ~3e19) with
+// variations of ~1e-3, beyond FP32's resolution of ~4e-6 there; so ln p_s
+// arrives as the transform of its coefficients without the l = 0 term (the
+// p_lnps plane) plus that term's nodal value c_00 / (2 sqrt(pi)), and
+// p_s = p_s_ref exp(rel) with rel = ln(p_s / p_s_ref) formed from them.  The
+// pressure-gradient and geopotential residuals subtract terms at p_s_ref
+// from terms at p_s; they are written as the reference value plus
+// deviations proportional to p_s - p_s_ref (the log pressure ratios through
+// log1p, alpha, W and W p_s / dp), so nothing large cancels.  The geopotential
+// residual omits its horizontally uniform part R (sum_{j>k} T_ref,j lr_j +
+// alpha_k T_ref,k) at p_s_ref, which the Laplacian of the divergence
+// tendency removes.
+//
+// Passes over the levels:
+//   A (top-down): column totals of the layer mass-flux divergences
+//     D_k = dp_k div_k + db_k p_s (v . grad ln p_s) and of their advective
+//     part, and the ln p_s tendency.
+//   B (bottom-up): kinetic energy plus the geopotential residual
+//     (get_geopotential_diff_hybrid, :1628-1675) through suffix sums.
+//   C (top-down): mass fluxes M_{k+1/2} = -sum_{r<=k} D_r + b_{k+1/2} sum D
+//     at both interfaces of the level, vertical advection
+//     (hybrid_vertical_advection, :1941-1958), the pressure-gradient
+//     residual (:1826-1856), the temperature tendency with the omega / p
+//     terms (:2124-2224, whose integrands are the same D_k) and the tracers.
+// Outputs use the planes of pe_nodal_kernel, so the modal post-pass is shared.
+__global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs a) {
+  extern __shared__ float s_hyb[];
+  const int K = a.K;
+  for (int i = threadIdx.x; i < K * kHybPack + 3; i += blockDim.x) s_hyb[i] = a.lev[i];
+  __syncthreads();
+  const unsigned IJ = (unsigned)a.I * (unsigned)a.J;
+  const unsigned col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= IJ) return;
+  const int mb = blockIdx.y;
+  const int mK = a.mem * K;
+  const int j = (int)(col % (unsigned)a.J);
+  const float sec2 = a.lat[j];
+  const float fcor = a.lat[a.J + j];
+  auto ld = [&](int base, int k) -> float {
+    return a.nod[((size_t)base + (size_t)mb * K + k) * IJ + col];
+  };
+  auto st = [&](int base, int k, float v) {
+    a.fwd[((size_t)base + (size_t)mb * K + k) * IJ + col] = v;
+  };
+  auto lev = [&](int k, int i) -> float { return s_hyb[k * kHybPack + i]; };
+  auto a_if = [&](int i) -> float { return i < K ? lev(i, 0) : s_hyb[K * kHybPack]; };
+  auto b_if = [&](int i) -> float { return i < K ? lev(i, 1) : s_hyb[K * kHybPack + 1]; };
+  auto pr_if = [&](int i) -> float { return i < K ? lev(i, 8) : s_hyb[K * kHybPack + 2]; };
+  const float gx = a.nod[((size_t)a.p_gx + mb) * IJ + col];
+  const float gy = a.nod[((size_t)a.p_gy + mb) * IJ + col];
+  const float psr = a.ps_ref;
+  // The uniform part c_00 / (2 sqrt(pi)) - ln p_s_ref in FP64: both terms
+  // are ~45 and their FP32 roundings would be ~5e-6 of a difference ~1e-2.
+  const float rel = (float)((double)a.lnps_modal[(size_t)mb * a.ML] * a.inv_y00 - a.ln_ps_ref) +
+                    a.nod[((size_t)a.p_lnps + mb) * IJ + col];
+  const float ps = psr * expf(rel);
+  const float dps = psr * expm1f(rel);  // p_s - p_s_ref
+  const float floor_s = 1e-6f * ps, floor_r = 1e-6f * psr;
+  const int hum = a.hum;
+  auto hum_at = [&](int k) -> float { return hum >= 0 ? ld(a.p_tr + hum * mK, k) : 0.f; };
+  // Virtual-temperature factor 1 + (R_v / R - 1) q.
+  auto adj_of = [&](float q) -> float { return hum >= 0 ? 1.f + (a.Rv_over_R - 1.f) * q : 1.f; };
+  // (P_i - P_i,ref) / P_i,ref of the floored interface pressure max(p, 1e-6 p_s).
+  auto x_if = [&](int i) -> float {
+    const float p = a_if(i) + b_if(i) * ps, pr = pr_if(i);
+    float dP;
+    if (p >= floor_s && pr >= floor_r)
+      dP = b_if(i) * dps;
+    else if (p < floor_s && pr < floor_r)
+      dP = 1e-6f * dps;
+    else
+      dP = fmaxf(p, floor_s) - fmaxf(pr, floor_r);
+    return dP / fmaxf(pr, floor_r);
+  };
+  // Level k at this column: deviations of the log ratio and alpha
+  // (_get_vertical_discretization_coeffs, :1507-1533), W and
+  // s - s_ref = W p_s / dp - (W p_s / dp)_ref.
+  struct Lev {
+    float dlr, dal, W, ds;
+  };
+  auto level = [&](int k) -> Lev {
+    Lev o;
+    o.dlr = log1pf(x_if(k + 1)) - log1pf(x_if(k));
+    const float da = lev(k, 2), db = lev(k, 3), dpr = lev(k, 9);
+    const float dp = da + db * ps;
+    const float r = (a_if(k) + b_if(k) * ps) / dp;
+    const float dr = dps * (b_if(k) * da - a_if(k) * db) / (dp * dpr);
+    o.dal = -(dr * lev(k, 6) + r * o.dlr);
+    const float dW = o.dlr * b_if(k) + o.dal * db;
+    o.W = lev(k, 10) + dW;
+    if (dp >= floor_s && dpr >= floor_r)
+      o.ds = lev(k, 10) * da * dps / (dp * dpr) + dW * ps / dp;
+    else
+      o.ds = o.W * ps / fmaxf(dp, floor_s) - lev(k, 7);
+    return o;
+  };
+
+  // Pass A.
+  float totF = 0.f, totE = 0.f, lp_a = 0.f, lp_b = 0.f;
+  const float inv_ps_diff = -dps / ps / psr;  // 1 / p_s - 1 / p_s_ref
+  for (int k = 0; k < K; ++k) {
+    const float u = ld(a.p_u, k), v = ld(a.p_v, k), d = ld(a.p_div, k);
+    const float da = lev(k, 2), db = lev(k, 3);
+    const float udg = (u * gx + v * gy) * sec2;
+    const float dp = da + db * ps;
+    const float DE = db * ps * udg;
+    totF += dp * d + DE;
+    totE += DE;
+    lp_a += d * da * inv_ps_diff;
+    lp_b += udg * db;
+  }
+  a.fwd[((size_t)a.o_lnps + mb) * IJ + col] = -(lp_a + lp_b);
+
+  // Pass B: KE + R (sum_{j>k} t_j ((adj_j - 1) lr_ref,j + adj_j dlr_j)
+  //                 + t_k ((adj_k - 1) alpha_ref,k + adj_k dalpha_k)), t = T' + T_ref.
+  {
+    float suf = 0.f;
+    for (int k = K - 1; k >= 0; --k) {
+      const float T = ld(a.p_temp, k), u = ld(a.p_u, k), v = ld(a.p_v, k);
+      const Lev L = level(k);
+      const float t = T + lev(k, 4);
+      const float adj = adj_of(hum_at(k));
+      const float ke = (u * u + v * v) * sec2 * 0.5f;
+      st(a.o_KE, k, ke + a.R * (suf + t * ((adj - 1.f) * lev(k, 5) + adj * L.dal)));
+      suf += t * ((adj - 1.f) * lev(k, 6) + adj * L.dlr);
+    }
+  }
+
+  // Pass C.
+  float cumF = 0.f, cumE = 0.f;  // sum_{r<k} D_r
+  float fF_prev = 0.f, fE_prev = 0.f, alr_prev = 0.f;
+  float u_p = 0.f, v_p = 0.f, T_p = 0.f, u_c = ld(a.p_u, 0), v_c = ld(a.p_v, 0),
+        T_c = ld(a.p_temp, 0);
+  float q_p[kMaxTracers], q_c[kMaxTracers];
+#pragma unroll
+  for (int t = 0; t < kMaxTracers; ++t) {
+    q_p[t] = 0.f;
+    q_c[t] = t < a.nT ? ld(a.p_tr + t * mK, 0) : 0.f;
+  }
+  for (int k = 0; k < K; ++k) {
+    const bool has_up = k > 0, has_dn = k + 1 < K;
+    const float u_n = has_dn ? ld(a.p_u, k + 1) : 0.f;
+    const float v_n = has_dn ? ld(a.p_v, k + 1) : 0.f;
+    const float T_n = has_dn ? ld(a.p_temp, k + 1) : 0.f;
+    const float zeta = ld(a.p_vort, k), d = ld(a.p_div, k);
+    const float da = lev(k, 2), db = lev(k, 3), tr = lev(k, 4), alr = lev(k, 5);
+    const float udg = (u_c * gx + v_c * gy) * sec2;
+    const float dp = da + db * ps;
+    const float DE = db * ps * udg;
+    const float DF = dp * d + DE;
+    // Mass fluxes at the level's upper (k - 1/2) and lower (k + 1/2) interfaces.
+    const float MF_up = -cumF + b_if(k) * totF, MF_dn = -(cumF + DF) + b_if(k + 1) * totF;
+    const float ME_up = -cumE + b_if(k) * totE, ME_dn = -(cumE + DE) + b_if(k + 1) * totE;
+    const float inv_dp = 1.f / dp;
+    // hybrid_vertical_advection(M, x)_k; only interior interfaces carry flux.
+    auto vadv = [&](float mu, float md, float xp, float xc, float xn) -> float {
+      const float fu = has_up ? mu * (xc - xp) : 0.f;
+      const float fd = has_dn ? md * (xn - xc) : 0.f;
+      return -0.5f * (fu + fd) * inv_dp;
+    };
+    const Lev L = level(k);
+    const float q_h = hum >= 0 ? q_c[hum] : 0.f;
+    const float adj = adj_of(q_h);
+    const float t = T_c + tr;
+    // Pressure-gradient residual C_k(T, p_s) adj - C_k(T_ref, p_s_ref)
+    // = R (t adj (s - s_ref) + (t (adj - 1) + T') s_ref).
+    const float pgf = a.R * (t * adj * L.ds + (t * (adj - 1.f) + T_c) * lev(k, 7));
+    float sdu = 0.f, sdv = 0.f;
+    if (a.vadv) {
+      sdu = -vadv(MF_up, MF_dn, u_p, u_c, u_n);
+      sdv = -vadv(MF_up, MF_dn, v_p, v_c, v_n);
+    }
+    const float tv = zeta + fcor;
+    st(a.o_Au, k, -v_c * tv * sec2 + (sdu + pgf * gx) * sec2);
+    st(a.o_Av, k, u_c * tv * sec2 + (sdv + pgf * gy) * sec2);
+    st(a.o_uT, k, u_c * T_c * sec2);
+    st(a.o_vT, k, v_c * T_c * sec2);
+    // Temperature: T' div, vertical advection, omega / p terms
+    // (_t_omega_over_p_hybrid, :2032-2056, with alpha at p_s_ref).
+    float Tn = T_c * d;
+    if (a.vadv) Tn += vadv(MF_up, MF_dn, T_p, T_c, T_n);
+    if (a.tref_varies) {
+      const float tr_up = has_up ? lev(k - 1, 4) : 0.f;
+      const float tr_dn = has_dn ? lev(k + 1, 4) : 0.f;
+      Tn += vadv(ME_up, ME_dn, tr_up, tr, tr_dn);
+    }
+    const float fF = cumF + DF, fE = cumE + DE;
+    const float gF = (alr * fF + alr_prev * fF_prev) * inv_dp;
+    const float gE = (alr * fE + alr_prev * fE_prev) * inv_dp;
+    const float sudg = udg * ps * L.W / fmaxf(dp, floor_s);
+    const float mean_part = tr * (sudg - gE);
+    float var_part;
+    if (hum < 0) {
+      var_part = T_c * (sudg - gF);
+    } else {
+      const float den = 1.f + (a.Cpv_over_Cp - 1.f) * q_h;
+      const float tvar = T_c * ((1.f + (a.Rv_over_R - 1.f) * q_h) / den);
+      const float tref_q = tr * (((a.Rv_over_R - a.Cpv_over_Cp) * q_h) / den);
+      var_part = (tvar + tref_q) * (sudg - gF);
+    }
+    st(a.o_Tn, k, Tn + a.kappa * (mean_part + var_part));
+    // Tracers: u q, v q (times sec^2) and q div + vertical advection.
+#pragma unroll
+    for (int t2 = 0; t2 < kMaxTracers; ++t2) {
+      if (t2 >= a.nT) break;
+      const float q_n = has_dn ? ld(a.p_tr + t2 * mK, k + 1) : 0.f;
+      const int ob = a.o_tr + 3 * t2 * mK;
+      st(ob, k, u_c * q_c[t2] * sec2);
+      st(ob + mK, k, v_c * q_c[t2] * sec2);
+      float qn = q_c[t2] * d;
+      if (a.vadv) qn += vadv(MF_up, MF_dn, q_p[t2], q_c[t2], q_n);
+      st(ob + 2 * mK, k, qn);
+      q_p[t2] = q_c[t2];
+      q_c[t2] = q_n;
+    }
+    cumF += DF;
+    cumE += DE;
+    fF_prev = fF;
+    fE_prev = fE;
+    alr_prev = alr;
+    u_p = u_c; v_p = v_c; T_p = T_c;
+    u_c = u_n; v_c = v_n; T_c = T_n;
   }
 }
 
@@ -1240,11 +1507,11 @@ constexpr int kMaxLevels = 48;
 
 struct MatBuildArgs {
   int K, kind, RP, nin, transposed;
-  double eta, R;
+  double eta;
   const double* G;       // K x K
   const double* H;       // K x K
-  const double* tref;    // K
-  const double* dsig;    // K
+  const double* lcol;    // K: the ln ps column of L's divergence rows
+  const double* trow;    // K: L's ln ps row (d ln ps / dt = -trow . div)
   const double* lam;     // L
   const double* filter;  // L, or null
   float* out;            // [L][n][RP]
@@ -1265,10 +1532,10 @@ __global__ void pe_matrix_build_kernel(MatBuildArgs a) {
     if (r < K) {
       if (c < K) return 0.0;
       if (c < 2 * K) return -lm * a.G[r * K + (c - K)];
-      return -lm * a.R * a.tref[r];
+      return -lm * a.lcol[r];
     }
     if (r < 2 * K) return c < K ? -a.H[(r - K) * K + c] : 0.0;
-    return c < K ? -a.dsig[c] : 0.0;
+    return c < K ? -a.trow[c] : 0.0;
   };
   if (a.kind == kMatL) {
     for (int e = tid; e < a.nin * a.RP; e += nt) {
@@ -1322,13 +1589,13 @@ __global__ void pe_matrix_build_kernel(MatBuildArgs a) {
     double s = 0.0;
     if (r < K) {
       for (int j = 0; j < K; ++j) s += a.G[r * K + j] * inv(K + j, c);
-      return -lm * (s + a.R * a.tref[r] * inv(2 * K, c));
+      return -lm * (s + a.lcol[r] * inv(2 * K, c));
     }
     if (r < 2 * K) {
       for (int j = 0; j < K; ++j) s += a.H[(r - K) * K + j] * inv(j, c);
       return -s;
     }
-    for (int j = 0; j < K; ++j) s += a.dsig[j] * inv(j, c);
+    for (int j = 0; j < K; ++j) s += a.trow[j] * inv(j, c);
     return -s;
   };
   const double f = a.filter ? a.filter[l] : 1.0;
@@ -1726,8 +1993,8 @@ static int get_matrix(dino_pe* pe, int kind, double eta, const double* host_filt
   std::vector<double> consts;
   consts.insert(consts.end(), pe->G.begin(), pe->G.end());
   consts.insert(consts.end(), pe->H.begin(), pe->H.end());
-  consts.insert(consts.end(), pe->tref.begin(), pe->tref.end());
-  consts.insert(consts.end(), pe->dsig.begin(), pe->dsig.end());
+  consts.insert(consts.end(), pe->imp_col.begin(), pe->imp_col.end());
+  consts.insert(consts.end(), pe->imp_row.begin(), pe->imp_row.end());
   consts.insert(consts.end(), lam.begin(), lam.end());
   if (host_filter) consts.insert(consts.end(), host_filter, host_filter + L);
   double* dc = nullptr;
@@ -1744,11 +2011,10 @@ static int get_matrix(dino_pe* pe, int kind, double eta, const double* host_filt
     b.nin = m.nin;
     b.transposed = transposed ? 1 : 0;
     b.eta = eta;
-    b.R = pe->R;
     b.G = dc;
     b.H = dc + K * K;
-    b.tref = dc + 2 * K * K;
-    b.dsig = dc + 2 * K * K + K;
+    b.lcol = dc + 2 * K * K;
+    b.trow = dc + 2 * K * K + K;
     b.lam = dc + 2 * K * K + 2 * K;
     b.filter = host_filter ? dc + 2 * K * K + 2 * K + L : nullptr;
     b.out = m.d;
@@ -1829,6 +2095,9 @@ static int pe_nodal_inputs(dino_pe* pe, const float* state, cudaStream_t st) {
     if (pe->hum >= 0) {
       a.a_laplnps = q; q += mem;
     }
+    if (pe->hybrid) {
+      a.a_lnpsdev = q; q += mem;
+    }
     a.deriv = p->d_deriv;
     a.lap = p->d_lap;
     a.invlap = p->d_invlap;
@@ -1895,7 +2164,55 @@ static int nodal_prepare(int K) {
 
 static NodalArgs make_nodal_args(dino_pe* pe);
 
-static int launch_nodal(dino_pe* pe, cudaStream_t st) {
+static int launch_nodal_hybrid(dino_pe* pe, const float* state, cudaStream_t st) {
+  const int K = pe->K, mK = pe->mem * K;
+  HybridArgs a{};
+  a.nod = pe->d_nodal;
+  a.fwd = pe->d_fwd_in;
+  a.lev = pe->d_hyb;
+  a.lat = pe->d_lat;
+  a.lnps_modal = state + (size_t)(3 + pe->nT) * mK * pe->ML;
+  a.ML = (unsigned)pe->ML;
+  a.K = K;
+  a.mem = pe->mem;
+  a.nT = pe->nT;
+  a.hum = pe->hum_hyb;
+  a.vadv = pe->vadv;
+  a.tref_varies = pe->tref_varies;
+  a.I = pe->I;
+  a.J = pe->J;
+  a.p_vort = 0;
+  a.p_div = mK;
+  a.p_temp = 2 * mK;
+  a.p_tr = 3 * mK;
+  a.p_u = pe->p_u;
+  a.p_v = pe->p_v;
+  a.p_gx = pe->p_gx;
+  a.p_gy = pe->p_gy;
+  a.p_lnps = pe->p_lnps;
+  a.o_Au = pe->o_Au;
+  a.o_Av = pe->o_Av;
+  a.o_KE = pe->o_KE;
+  a.o_uT = pe->o_uT;
+  a.o_vT = pe->o_vT;
+  a.o_Tn = pe->o_Tn;
+  a.o_tr = pe->o_tr;
+  a.o_lnps = pe->o_lnps;
+  a.R = (float)pe->R;
+  a.kappa = (float)pe->kappa;
+  a.ps_ref = (float)pe->ps_ref;
+  a.ln_ps_ref = std::log(pe->ps_ref);
+  // The constant field 1 has the modal coefficient 2 sqrt(pi) at l = m = 0.
+  a.inv_y00 = 0.5 / std::sqrt(3.14159265358979323846);
+  a.Rv_over_R = (float)(pe->Rv / pe->R);
+  a.Cpv_over_Cp = (float)(pe->Cpv / (pe->R / pe->kappa));
+  const dim3 grid(ceil_div((int)pe->IJ, kHybThreads), pe->mem);
+  const size_t smem = sizeof(float) * ((size_t)K * kHybPack + 3);
+  pe_nodal_hybrid_kernel<<<grid, kHybThreads, smem, st>>>(a);
+  return check_launch("pe_nodal_hybrid");
+}
+static int launch_nodal(dino_pe* pe, const float* state, cudaStream_t st) {
+  if (pe->hybrid) return launch_nodal_hybrid(pe, state, st);
   const NodalArgs a = make_nodal_args(pe);
   const int V = nodal_vec(pe);
   const dim3 grid(ceil_div((int)(pe->IJ / V), kNodalCols), pe->mem);
@@ -1977,7 +2294,7 @@ static int pe_explicit_impl(dino_pe* pe, const float* state, float* tend,
   DINO_TRY(pe_nodal_inputs(pe, state, st));
   // 3. fused nodal column kernel
   {
-    DINO_TRY(launch_nodal(pe, st));
+    DINO_TRY(launch_nodal(pe, state, st));
   }
   // 4. forward SHT
   DINO_TRY(sht_forward_to(p, pe->d_fwd_in, pe->d_fwd_out, pe->n_fwd, pe->d_work,
@@ -2292,6 +2609,7 @@ static void pe_free(dino_pe* pe) {
   for (auto& e : pe->mat_cache) cudaFree(e.d);
   for (auto& e : pe->filter_cache) cudaFree(e.d_filter);
   cudaFree(pe->d_levpack);
+  cudaFree(pe->d_hyb);
   cudaFree(pe->d_lat);
   cudaFree(pe->d_orog);
   cudaFree(pe->d_aux);
@@ -2332,6 +2650,47 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
   pe->tref_varies = 0;
   for (int k = 1; k < K; ++k)
     if (pe->tref[k] != pe->tref[0]) pe->tref_varies = 1;
+  pe->imp_col.resize(K);
+  pe->imp_row.resize(K);
+  for (int k = 0; k < K; ++k) {
+    pe->imp_col[k] = d->implicit_lnps_column ? d->implicit_lnps_column[k] : pe->R * pe->tref[k];
+    pe->imp_row[k] = d->implicit_thickness ? d->implicit_thickness[k] : pe->dsig[k];
+  }
+  if (pe->hybrid) {
+    // pe_nodal_hybrid_kernel's level constants at p_s_ref, in FP64: alpha and
+    // the log pressure ratio as _get_vertical_discretization_coeffs_numpy
+    // (primitive_equations.py:1483-1504) forms them, W and W p_s / dp
+    // (_get_pgf_lps_coefficient_numpy, :1859-1887).
+    const double* A = d->hybrid_a_boundaries;
+    const double* B = d->hybrid_b_boundaries;
+    const double psr = pe->ps_ref;
+    std::vector<float> hp((size_t)K * kHybPack + 3, 0.f);
+    for (int k = 0; k < K; ++k) {
+      const double pu = A[k] + B[k] * psr, pd = A[k + 1] + B[k + 1] * psr;
+      DINO_REQUIRE(pd - pu > 0, DINO_ERR_ARG, "Pressure must decrease monotonically with height.");
+      const double lr = std::log(std::max(pd, 1e-6 * psr) / std::max(pu, 1e-6 * psr));
+      const double al = 1.0 - (pu / (pd - pu)) * lr;
+      const double da = A[k + 1] - A[k], db = B[k + 1] - B[k];
+      const double dp = da + db * psr;
+      const double W = lr * B[k] + al * db;
+      float* q = hp.data() + (size_t)k * kHybPack;
+      q[0] = (float)A[k];
+      q[1] = (float)B[k];
+      q[2] = (float)da;
+      q[3] = (float)db;
+      q[4] = (float)pe->tref[k];
+      q[5] = (float)al;
+      q[6] = (float)lr;
+      q[7] = (float)(W * psr / std::max(dp, 1e-6 * psr));
+      q[8] = (float)pu;
+      q[9] = (float)dp;
+      q[10] = (float)W;
+    }
+    hp[(size_t)K * kHybPack] = (float)A[K];
+    hp[(size_t)K * kHybPack + 1] = (float)B[K];
+    hp[(size_t)K * kHybPack + 2] = (float)(A[K] + B[K] * psr);
+    DINO_TRY(upload_vec(&pe->d_hyb, hp));
+  }
 
   // Level constants.
   LevOff lo = lev_offsets(K);
@@ -2401,7 +2760,9 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
   // Field bookkeeping.
   const bool moist = pe->hum >= 0;
   pe->n_state = (3 + nT) * mK + mem;
-  pe->n_aux = 2 * mK + (moist ? 2 * mK : 0) + 2 * mem + (moist ? mem : 0);
+  // Hybrid levels add ln p_s without its l = 0 term to the aux planes.
+  pe->n_aux = 2 * mK + (moist ? 2 * mK : 0) + 2 * mem + (moist ? mem : 0) +
+              (pe->hybrid ? mem : 0);
   pe->n_inv = (3 + nT) * mK + pe->n_aux + (pe->hs ? mem : 0);
   {
     int q = (3 + nT) * mK;  // nodal planes follow the inverse field order
@@ -2416,7 +2777,8 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
     if (moist) {
       pe->p_laplnps = q; q += mem;
     }
-    if (pe->hs) {
+    if (pe->hybrid || pe->hs) {
+      // hybrid: the deviation plane (aux); Held-Suarez: ln p_s itself
       pe->p_lnps = q; q += mem;
     }
   }
@@ -2489,6 +2851,17 @@ int dino_pe_create(dino_plan* plan, const dino_pe_desc* d, dino_pe** out) {
                DINO_ERR_ARG, "dino_pe_create: missing vertical arrays");
   DINO_REQUIRE(!(d->held_suarez && d->n_tracers > 0), DINO_ERR_UNSUPPORTED,
                "Held-Suarez forcing composes with tracer-free states only");
+  DINO_REQUIRE(d->vertical_scheme == 0 || d->vertical_scheme == 1, DINO_ERR_ARG,
+               "vertical_scheme must be 0 (sigma) or 1 (hybrid)");
+  if (d->vertical_scheme == 1) {
+    DINO_REQUIRE(d->hybrid_a_boundaries && d->hybrid_b_boundaries &&
+                     d->implicit_lnps_column && d->implicit_thickness,
+                 DINO_ERR_ARG, "dino_pe_create: missing hybrid-level arrays");
+    DINO_REQUIRE(d->reference_surface_pressure > 0, DINO_ERR_ARG,
+                 "`reference_surface_pressure` must be positive.");
+    DINO_REQUIRE(!d->held_suarez, DINO_ERR_UNSUPPORTED,
+                 "Held-Suarez forcing is defined on sigma levels only");
+  }
   DINO_REQUIRE((int64_t)d->layers * plan->I * plan->J < ((int64_t)1 << 31),
                DINO_ERR_UNSUPPORTED, "layers x nodal points must be below 2^31");
   dino_pe* pe = new dino_pe();
@@ -2497,6 +2870,14 @@ int dino_pe_create(dino_plan* plan, const dino_pe_desc* d, dino_pe** out) {
   pe->mem = d->members;
   pe->nT = d->n_tracers;
   pe->hum = d->humidity_tracer;
+  pe->hybrid = d->vertical_scheme == 1 ? 1 : 0;
+  if (pe->hybrid) {
+    // Humidity enters the hybrid column kernel only; the sigma-form moist
+    // planes (humidity gradients, corrections) stay off.
+    pe->hum_hyb = pe->hum;
+    pe->hum = -1;
+    pe->ps_ref = d->reference_surface_pressure;
+  }
   pe->vadv = d->include_vertical_advection ? 1 : 0;
   pe->hs = d->held_suarez ? 1 : 0;
   pe->M = plan->M;
@@ -2634,6 +3015,8 @@ int dino_pe_explicit_vjp(dino_pe* pe, const float* state, const float* tend_ct,
                          float* state_ct, void* stream) {
   DINO_REQUIRE(pe && state && tend_ct && state_ct, DINO_ERR_ARG,
                "dino_pe_explicit_vjp: null argument");
+  DINO_REQUIRE(!pe->hybrid, DINO_ERR_UNSUPPORTED,
+               "the explicit-term VJP is built for sigma levels only");
   DINO_REQUIRE(state_ct != state && state_ct != tend_ct, DINO_ERR_ARG,
                "dino_pe_explicit_vjp: state_ct must not alias the inputs");
   DINO_TRY(pe_ensure_adjoint(pe));
@@ -2669,6 +3052,8 @@ int dino_pe_step_vjp(dino_pe* pe, const float* state, const float* out_ct,
                      void* stream) {
   DINO_REQUIRE(pe && state && out_ct && in_ct, DINO_ERR_ARG,
                "dino_pe_step_vjp: null argument");
+  DINO_REQUIRE(!pe->hybrid, DINO_ERR_UNSUPPORTED,
+               "the step VJP is built for sigma levels only");
   DINO_REQUIRE(in_ct != state, DINO_ERR_ARG, "dino_pe_step_vjp: in_ct must not alias state");
   DINO_TRY(pe_ensure_adjoint(pe));
   DINO_TRY(sht_prepare(pe->plan));

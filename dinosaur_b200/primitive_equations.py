@@ -22,6 +22,7 @@ import torch
 
 from dinosaur_b200 import _lib
 from dinosaur_b200 import coordinate_systems
+from dinosaur_b200 import hybrid_coordinates
 from dinosaur_b200 import pytree
 from dinosaur_b200 import sigma_coordinates
 from dinosaur_b200 import spherical_harmonic as sh
@@ -185,20 +186,43 @@ class _Engine:
                          f'{tracer_names}.')
       hum = tracer_names.index(eq.humidity_key)
     K = self.K
+    f64 = lambda x: np.ascontiguousarray(x, np.float64)
+    hybrid = isinstance(eq, PrimitiveEquationsHybrid)
     # Host constants, kept alive for the duration of the create call.
-    self._arrays = dict(
-        bounds=np.ascontiguousarray(vert.boundaries, np.float64),
-        centers=np.ascontiguousarray(vert.centers, np.float64),
-        thick=np.ascontiguousarray(vert.layer_thickness, np.float64),
-        inv_c2c=np.ascontiguousarray(
-            (1 / vert.center_to_center) if K > 1 else np.zeros(1), np.float64),
-        tref=np.ascontiguousarray(eq.reference_temperature, np.float64),
-        G=np.ascontiguousarray(get_geopotential_weights_sigma(vert, ps.R),
-                               np.float64),
-        H=np.ascontiguousarray(get_temperature_implicit_weights_sigma(
-            vert, eq.reference_temperature, ps.kappa), np.float64),
-        alpha=np.ascontiguousarray(get_sigma_ratios(vert), np.float64),
-    )
+    if not hybrid:
+      self._arrays = dict(
+          bounds=f64(vert.boundaries),
+          centers=f64(vert.centers),
+          thick=f64(vert.layer_thickness),
+          inv_c2c=f64((1 / vert.center_to_center) if K > 1 else np.zeros(1)),
+          tref=f64(eq.reference_temperature),
+          G=f64(get_geopotential_weights_sigma(vert, ps.R)),
+          H=f64(get_temperature_implicit_weights_sigma(
+              vert, eq.reference_temperature, ps.kappa)),
+          alpha=f64(get_sigma_ratios(vert)),
+      )
+    else:
+      lev, psr = eq.nondim_levels, eq.p_s_ref
+      # The implicit operator at p_s_ref (_get_implicit_term_matrix_hybrid,
+      # primitive_equations.py:1890-1938); the sigma-only arrays are
+      # placeholders of the right sizes.
+      thick = lev.pressure_thickness / psr + lev.sigma_thickness
+      self._arrays = dict(
+          bounds=f64(lev.b_boundaries),
+          centers=f64(lev.b_centers),
+          thick=f64(thick),
+          inv_c2c=f64(np.zeros(max(K - 1, 1))),
+          tref=f64(eq.reference_temperature),
+          G=f64(get_geopotential_weights_hybrid(lev, ps.R, psr)),
+          H=f64(get_temperature_implicit_weights_hybrid(
+              lev, eq.reference_temperature, ps.kappa, psr)),
+          alpha=f64(np.zeros(K)),
+          a_b=f64(lev.a_boundaries),
+          b_b=f64(lev.b_boundaries),
+          col=f64(pgf_lps_coefficient_hybrid(eq.reference_temperature, psr, lev,
+                                             ps.R)),
+          row=f64(thick),
+      )
     orog = eq.orography
     if sh.is_fast_layout(grid):
       orog = sh.to_real_layout(grid, torch.as_tensor(np.asarray(orog, np.float32)
@@ -226,6 +250,13 @@ class _Engine:
         orography_modal=self._orog.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
         angular_velocity=ps.angular_velocity, gravity=ps.g, R=ps.R,
         R_vapor=ps.R_vapor, Cp_vapor=ps.Cp_vapor, kappa=ps.kappa)
+    if hybrid:
+      desc.vertical_scheme = 1
+      desc.hybrid_a_boundaries = _lib.dptr(a['a_b'])
+      desc.hybrid_b_boundaries = _lib.dptr(a['b_b'])
+      desc.reference_surface_pressure = eq.p_s_ref
+      desc.implicit_lnps_column = _lib.dptr(a['col'])
+      desc.implicit_thickness = _lib.dptr(a['row'])
     if hs is not None:
       desc.hs_p0 = hs.p0
       desc.hs_sigma_b = hs.sigma_b
@@ -529,6 +560,119 @@ class PrimitiveEquationsSigma(time_integration.ImplicitExplicitODE):
     out = (_InverseFn.apply(buf, eng, eta) if _needs_grad(buf)
            else eng.inverse(buf, eta))
     return eng.unpack(out, state, state.sim_time)
+
+
+
+# ---------------------------------------------------------------------------
+# Hybrid sigma-pressure levels (primitive_equations.py:1467-2533)
+# ---------------------------------------------------------------------------
+
+
+def _hybrid_vertical_coeffs(levels: hybrid_coordinates.HybridCoordinates,
+                            p_s_ref: float):
+  """alpha_k and log(p_{k+1/2} / p_{k-1/2}) at a uniform surface pressure
+  (Simmons & Burridge 1981; _get_vertical_discretization_coeffs_numpy,
+  primitive_equations.py:1483-1504)."""
+  p_half = levels.a_boundaries + levels.b_boundaries * p_s_ref
+  dp = np.diff(p_half)
+  if np.any(dp <= 0):
+    raise ValueError('Pressure must decrease monotonically with height.')
+  upper, lower = p_half[:-1], p_half[1:]
+  log_ratio = np.log(np.maximum(lower, 1e-6 * p_s_ref)
+                     / np.maximum(upper, 1e-6 * p_s_ref))
+  return 1 - (upper / dp) * log_ratio, log_ratio
+
+
+def get_geopotential_weights_hybrid(levels, ideal_gas_constant, p_s_ref):
+  """G with Phi'_k = R (alpha_k T_k + sum_{j>k} log-ratio_j T_j) (:1605-1625)."""
+  alpha, log_ratio = _hybrid_vertical_coeffs(levels, p_s_ref)
+  k = levels.layers
+  return ideal_gas_constant * (np.diag(alpha)
+                               + np.triu(np.broadcast_to(log_ratio, (k, k)), 1))
+
+
+def get_temperature_implicit_weights_hybrid(levels, reference_temperature, kappa,
+                                            p_s_ref):
+  """H of the implicit temperature term on hybrid levels (:1736-1783)."""
+  tref = np.asarray(reference_temperature)
+  if tref.ndim != 1 or tref.shape[-1] != levels.layers:
+    raise ValueError(
+        '`reference_temp` must be a vector of length `coordinates.layers`; '
+        f'got shape {tref.shape} and {levels.layers} layers.')
+  k = levels.layers
+  lower = np.tril(np.ones([k, k]))
+  alpha, _ = _hybrid_vertical_coeffs(levels, p_s_ref)
+  p_alpha = lower * alpha[:, None]
+  p_alpha_up = np.concatenate([np.zeros([1, k]), p_alpha[:-1]], axis=0)
+  dp_ref = levels.pressure_thickness + levels.sigma_thickness * p_s_ref
+  h0 = kappa * tref[:, None] * (p_alpha + p_alpha_up) / dp_ref[:, None]
+  k0 = np.concatenate((np.diff(tref) / (dp_ref[:-1] + dp_ref[1:]), [0]))[:, None]
+  k1 = lower - np.cumsum(levels.sigma_thickness)[:, None]
+  kk = k0 * k1
+  kk_up = np.concatenate([np.zeros([1, k]), kk[:-1]], axis=0)
+  return (h0 - kk - kk_up) * dp_ref[None, :]
+
+
+def pgf_lps_coefficient_hybrid(temperature, surface_pressure, levels,
+                               ideal_gas_constant):
+  """C_k = (R T_k / dp_k) (log-ratio_k b_{k-1/2} + alpha_k db_k) p_s at a
+  uniform surface pressure (_get_pgf_lps_coefficient_numpy, :1859-1887)."""
+  alpha, log_ratio = _hybrid_vertical_coeffs(levels, surface_pressure)
+  b = levels.b_boundaries
+  dp = np.maximum(np.diff(levels.a_boundaries + b * surface_pressure),
+                  1e-6 * surface_pressure)
+  weight = log_ratio * b[:-1] + alpha * np.diff(b)
+  return (ideal_gas_constant * np.asarray(temperature) / dp) * weight * surface_pressure
+
+
+@dataclasses.dataclass(eq=False)
+class PrimitiveEquationsHybrid(PrimitiveEquationsSigma):
+  """Primitive equations on hybrid sigma-pressure levels
+  (primitive_equations.py:1961-2533).
+
+  ``coords.vertical`` is a ``HybridCoordinates`` with ``a_boundaries`` in
+  units of ``hpa_quantity`` pascals (hPa by default);
+  ``reference_surface_pressure`` (pascals) is where the implicit terms are
+  linearised.  The explicit terms run in one CUDA column kernel
+  (Simmons & Burridge discretisation, surface pressure varying per column);
+  the implicit terms and their inverse, the fused imex_rk_sil3 step and CUDA
+  graphs are the sigma engine's with the hybrid operators.  Reverse mode
+  through the explicit terms and Held-Suarez forcing are sigma-only.
+  """
+
+  reference_surface_pressure: float = dataclasses.field(default=101325.0,
+                                                        kw_only=True)
+  hpa_quantity: float = dataclasses.field(default=100.0, kw_only=True)
+
+  def __post_init__(self):
+    super().__post_init__()
+    if self.held_suarez is not None:
+      raise NotImplementedError('Held-Suarez forcing is defined on sigma levels')
+    if not isinstance(self.coords.vertical, hybrid_coordinates.HybridCoordinates):
+      raise TypeError('PrimitiveEquationsHybrid needs HybridCoordinates levels')
+    p_s_ref = units.nondim_pressure(float(self.reference_surface_pressure))
+    if p_s_ref <= 0:
+      raise ValueError('`reference_surface_pressure` must be positive.')
+    self._p_s_ref = p_s_ref
+    vert = self.coords.vertical
+    self.nondim_levels = hybrid_coordinates.HybridCoordinates(
+        a_boundaries=units.nondim_pressure(
+            np.asarray(vert.a_boundaries, np.float64) * self.hpa_quantity),
+        b_boundaries=vert.b_boundaries)
+
+  @property
+  def p_s_ref(self) -> float:
+    return self._p_s_ref
+
+  def explicit_terms(self, state: State) -> State:
+    """primitive_equations.py:2249-2360."""
+    eng = self.engine(state)
+    buf = eng.pack(state)
+    if _needs_grad(buf):
+      raise NotImplementedError(
+          'reverse mode through the explicit terms is built for sigma levels only')
+    return eng.unpack(eng.explicit(buf), state,
+                      None if state.sim_time is None else 1.0)
 
 
 PrimitiveEquations = PrimitiveEquationsSigma

@@ -199,6 +199,23 @@ typedef struct dino_pe_desc {
   /* Held-Suarez constants (nondimensional), used when held_suarez = 1. */
   double hs_p0, hs_sigma_b, hs_kf, hs_ka, hs_ks, hs_minT, hs_maxT, hs_dTy,
       hs_dThz;
+  /* Vertical coordinate: 0 sigma levels (PrimitiveEquationsSigma), 1 hybrid
+   * sigma-pressure levels p = a + b p_s (PrimitiveEquationsHybrid,
+   * primitive_equations.py:1961-2533; no Held-Suarez, no explicit-term or
+   * step VJP).  For hybrid levels geopotential_weights and
+   * temperature_weights hold the hybrid G and H at p_s_ref, and the
+   * sigma-only arrays above are placeholders of their sizes (layer_thickness
+   * must be positive). */
+  int32_t vertical_scheme;
+  const double* hybrid_a_boundaries;  /* host, K+1, nondimensional pressure  */
+  const double* hybrid_b_boundaries;  /* host, K+1                           */
+  double reference_surface_pressure;  /* nondimensional p_s_ref              */
+  /* The implicit operator's ln ps column c and ln ps row w
+   * (d div_k/dt = -lap(sum_j G_kj T_j + c_k ln ps), d ln ps/dt = -sum_k w_k
+   * div_k); NULL gives the sigma values R T_ref and layer_thickness.  Hybrid:
+   * the pressure-gradient coefficient at p_s_ref and da / p_s_ref + db. */
+  const double* implicit_lnps_column; /* host, K, or NULL                    */
+  const double* implicit_thickness;   /* host, K, or NULL                    */
 } dino_pe_desc;
 
 DINO_API int dino_pe_create(dino_plan* plan, const dino_pe_desc* desc, dino_pe** out);

@@ -1,0 +1,80 @@
+"""The FP64 hybrid-coordinate oracle (oracle/hybrid.py) against the pins
+that the reference's own tests give it (primitive_equations_test.py:739-905):
+
+* on sigma-like hybrid levels (a = 0, b = sigma) the explicit and implicit
+  terms equal the sigma equations' to atol 1e-3 (test_equivalence_sigma_like,
+  :785-848; the sigma oracle is pinned to golden vectors of the reference);
+* implicit_inverse inverts (1 - eta implicit_terms) to atol 1e-5
+  (test_implicit_inverse_sigma_like, :850-896), here also on analytic
+  (non-sigma) levels;
+* the package's HybridCoordinates constructors give the oracle's levels.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import dycore as od
+from oracle import hybrid as oh
+from oracle import sht as osht
+from oracle import states as ost
+
+
+def jw_case(layers, amplitude=0.0):
+  og = osht.Grid.with_wavenumbers(21)
+  st, tref, orog, vert = ost.baroclinic_config(og, layers, seed=0, amplitude=amplitude)
+  return og, st, tref, orog, vert
+
+
+def assert_close(a, b, atol):
+  for k in od.STATE_KEYS:
+    np.testing.assert_allclose(a[k], b[k], atol=atol, rtol=0, err_msg=k)
+
+
+@pytest.mark.parametrize('layers', [20, 40])
+def test_sigma_like_levels_match_sigma_equations(layers):
+  # The explicit terms agree to ~1e-11; the implicit divergence differs by
+  # the top level's geopotential coefficient (alpha_0 = 1 on hybrid levels),
+  # 5.5e-4 at 20 layers and 9e-5 at the reference test's 40.
+  og, st, tref, orog, vert = jw_case(layers)
+  sig = od.PrimitiveEquationsSigma(tref, orog, og, vert, od.SimUnits())
+  hyb = oh.PrimitiveEquationsHybrid(tref, orog, og,
+                                    oh.HybridCoordinates.from_sigma_levels(vert),
+                                    od.SimUnits())
+  assert_close(hyb.explicit_terms(st), sig.explicit_terms(st), 1e-3)
+  assert_close(hyb.implicit_terms(st), sig.implicit_terms(st), 1e-3)
+
+
+def random_state(og, layers, seed):
+  rng = np.random.default_rng(seed)
+  _, l = og.modal_mesh
+  f = lambda n: rng.standard_normal((n,) + og.modal_shape) * og.mask / (l + 1.0)
+  return od.make_state(f(layers), f(layers), f(layers), f(1))
+
+
+@pytest.mark.parametrize('levels', ['sigma_like', 'analytic'])
+def test_implicit_inverse_inverts(levels):
+  og = osht.Grid.with_wavenumbers(16)
+  layers = 5
+  vert = od.SigmaCoordinates.equidistant(layers)
+  lev = (oh.HybridCoordinates.from_sigma_levels(vert) if levels == 'sigma_like'
+         else oh.HybridCoordinates.analytic_levels(layers))
+  eq = oh.PrimitiveEquationsHybrid(280 * np.ones(layers), np.zeros(og.modal_shape),
+                                   og, lev, od.SimUnits())
+  st = random_state(og, layers, 0)
+  eta = 0.1
+  rhs = od.tree_axpy((1.0, st), (-eta, eq.implicit_terms(st)))
+  assert_close(eq.implicit_inverse(rhs, eta), st, 1e-5)
+
+
+def test_package_levels_match_oracle():
+  from dinosaur_b200 import hybrid_coordinates as hc
+  from dinosaur_b200 import sigma_coordinates as sc
+  a = hc.HybridCoordinates.analytic_levels(17)
+  b = oh.HybridCoordinates.analytic_levels(17)
+  np.testing.assert_array_equal(a.a_boundaries, b.a_boundaries)
+  np.testing.assert_array_equal(a.b_boundaries, b.b_boundaries)
+  s = hc.HybridCoordinates.from_sigma_levels(sc.SigmaCoordinates.equidistant(8))
+  assert s.layers == 8 and np.all(s.a_boundaries == 0)
+  np.testing.assert_allclose(s.layer_thickness(2.0), 2.0 / 8)
+  with pytest.raises(ValueError):
+    hc.HybridCoordinates(np.zeros(3), np.zeros(4))
