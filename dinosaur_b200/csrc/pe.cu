@@ -672,6 +672,7 @@ __global__ void __launch_bounds__(kNodalCols * kNodalMaxChunks)
 //   0 a_{k-1/2}  1 b_{k-1/2}  2 da_k  3 db_k  4 T_ref,k  5 alpha_k
 //   6 log(p_{k+1/2} / p_{k-1/2})  7 s_k = W_k p_s / max(dp_k, 1e-6 p_s)
 //   8 p_{k-1/2}  9 dp_k  10 W_k = log-ratio_k b_{k-1/2} + alpha_k db_k
+//   11 1 / dp_k
 // followed by a, b and p (at p_s_ref) of the lowest interface.
 constexpr int kHybPack = 12;
 constexpr int kHybThreads = 128;
@@ -707,11 +708,10 @@ struct HybridArgs {
 // tendency removes.
 //
 // Passes over the levels:
-//   A (top-down): column totals of the layer mass-flux divergences
+//   A+B (bottom-up): column totals of the layer mass-flux divergences
 //     D_k = dp_k div_k + db_k p_s (v . grad ln p_s) and of their advective
-//     part, and the ln p_s tendency.
-//   B (bottom-up): kinetic energy plus the geopotential residual
-//     (get_geopotential_diff_hybrid, :1628-1675) through suffix sums.
+//     part, the ln p_s tendency, and kinetic energy plus the geopotential
+//     residual (get_geopotential_diff_hybrid, :1628-1675) through suffix sums.
 //   C (top-down): mass fluxes M_{k+1/2} = -sum_{r<=k} D_r + b_{k+1/2} sum D
 //     at both interfaces of the level, vertical advection
 //     (hybrid_vertical_advection, :1941-1958), the pressure-gradient
@@ -731,8 +731,10 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
   const int j = (int)(col % (unsigned)a.J);
   const float sec2 = a.lat[j];
   const float fcor = a.lat[a.J + j];
+  // The inputs are read-only for the kernel's duration: read-only loads may
+  // run ahead of the output stores.
   auto ld = [&](int base, int k) -> float {
-    return a.nod[((size_t)base + (size_t)mb * K + k) * IJ + col];
+    return __ldg(a.nod + ((size_t)base + (size_t)mb * K + k) * IJ + col);
   };
   auto st = [&](int base, int k, float v) {
     a.fwd[((size_t)base + (size_t)mb * K + k) * IJ + col] = v;
@@ -741,13 +743,13 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
   auto a_if = [&](int i) -> float { return i < K ? lev(i, 0) : s_hyb[K * kHybPack]; };
   auto b_if = [&](int i) -> float { return i < K ? lev(i, 1) : s_hyb[K * kHybPack + 1]; };
   auto pr_if = [&](int i) -> float { return i < K ? lev(i, 8) : s_hyb[K * kHybPack + 2]; };
-  const float gx = a.nod[((size_t)a.p_gx + mb) * IJ + col];
-  const float gy = a.nod[((size_t)a.p_gy + mb) * IJ + col];
+  const float gx = __ldg(a.nod + ((size_t)a.p_gx + mb) * IJ + col);
+  const float gy = __ldg(a.nod + ((size_t)a.p_gy + mb) * IJ + col);
   const float psr = a.ps_ref;
   // The uniform part c_00 / (2 sqrt(pi)) - ln p_s_ref in FP64: both terms
   // are ~45 and their FP32 roundings would be ~5e-6 of a difference ~1e-2.
   const float rel = (float)((double)a.lnps_modal[(size_t)mb * a.ML] * a.inv_y00 - a.ln_ps_ref) +
-                    a.nod[((size_t)a.p_lnps + mb) * IJ + col];
+                    __ldg(a.nod + ((size_t)a.p_lnps + mb) * IJ + col);
   const float ps = psr * expf(rel);
   const float dps = psr * expm1f(rel);  // p_s - p_s_ref
   const float floor_s = 1e-6f * ps, floor_r = 1e-6f * psr;
@@ -767,58 +769,60 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
       dP = fmaxf(p, floor_s) - fmaxf(pr, floor_r);
     return dP / fmaxf(pr, floor_r);
   };
-  // Level k at this column: deviations of the log ratio and alpha
-  // (_get_vertical_discretization_coeffs, :1507-1533), W and
-  // s - s_ref = W p_s / dp - (W p_s / dp)_ref.
+  // Level k at this column, given log1p(x) of its upper and lower interfaces
+  // (each interface's value is carried to the next level): deviations of the
+  // log ratio and alpha (_get_vertical_discretization_coeffs, :1507-1533), W
+  // and s - s_ref = W p_s / dp - (W p_s / dp)_ref.
   struct Lev {
     float dlr, dal, W, ds;
   };
-  auto level = [&](int k) -> Lev {
+  auto level = [&](int k, float l1_up, float l1_dn) -> Lev {
     Lev o;
-    o.dlr = log1pf(x_if(k + 1)) - log1pf(x_if(k));
-    const float da = lev(k, 2), db = lev(k, 3), dpr = lev(k, 9);
+    o.dlr = l1_dn - l1_up;
+    const float da = lev(k, 2), db = lev(k, 3), dpr = lev(k, 9), idpr = lev(k, 11);
     const float dp = da + db * ps;
-    const float r = (a_if(k) + b_if(k) * ps) / dp;
-    const float dr = dps * (b_if(k) * da - a_if(k) * db) / (dp * dpr);
+    const float idp = 1.f / dp;
+    const float r = (a_if(k) + b_if(k) * ps) * idp;
+    const float dr = dps * (b_if(k) * da - a_if(k) * db) * (idp * idpr);
     o.dal = -(dr * lev(k, 6) + r * o.dlr);
     const float dW = o.dlr * b_if(k) + o.dal * db;
     o.W = lev(k, 10) + dW;
     if (dp >= floor_s && dpr >= floor_r)
-      o.ds = lev(k, 10) * da * dps / (dp * dpr) + dW * ps / dp;
+      o.ds = lev(k, 10) * da * dps * (idp * idpr) + dW * ps * idp;
     else
       o.ds = o.W * ps / fmaxf(dp, floor_s) - lev(k, 7);
     return o;
   };
 
-  // Pass A.
-  float totF = 0.f, totE = 0.f, lp_a = 0.f, lp_b = 0.f;
-  const float inv_ps_diff = -dps / ps / psr;  // 1 / p_s - 1 / p_s_ref
-  for (int k = 0; k < K; ++k) {
-    const float u = ld(a.p_u, k), v = ld(a.p_v, k), d = ld(a.p_div, k);
-    const float da = lev(k, 2), db = lev(k, 3);
-    const float udg = (u * gx + v * gy) * sec2;
-    const float dp = da + db * ps;
-    const float DE = db * ps * udg;
-    totF += dp * d + DE;
-    totE += DE;
-    lp_a += d * da * inv_ps_diff;
-    lp_b += udg * db;
-  }
-  a.fwd[((size_t)a.o_lnps + mb) * IJ + col] = -(lp_a + lp_b);
-
-  // Pass B: KE + R (sum_{j>k} t_j ((adj_j - 1) lr_ref,j + adj_j dlr_j)
-  //                 + t_k ((adj_k - 1) alpha_ref,k + adj_k dalpha_k)), t = T' + T_ref.
+  // Pass A+B (bottom-up): the column totals and the ln p_s tendency, and
+  // KE + R (sum_{j>k} t_j ((adj_j - 1) lr_ref,j + adj_j dlr_j)
+  //         + t_k ((adj_k - 1) alpha_ref,k + adj_k dalpha_k)), t = T' + T_ref.
+  float totF = 0.f, totE = 0.f;
   {
-    float suf = 0.f;
+    float lp_a = 0.f, lp_b = 0.f, suf = 0.f;
+    const float inv_ps_diff = -dps / ps / psr;  // 1 / p_s - 1 / p_s_ref
+    float l1_dn = log1pf(x_if(K));
     for (int k = K - 1; k >= 0; --k) {
-      const float T = ld(a.p_temp, k), u = ld(a.p_u, k), v = ld(a.p_v, k);
-      const Lev L = level(k);
+      const float u = ld(a.p_u, k), v = ld(a.p_v, k), d = ld(a.p_div, k);
+      const float T = ld(a.p_temp, k);
+      const float da = lev(k, 2), db = lev(k, 3);
+      const float udg = (u * gx + v * gy) * sec2;
+      const float dp = da + db * ps;
+      const float DE = db * ps * udg;
+      totF += dp * d + DE;
+      totE += DE;
+      lp_a += d * da * inv_ps_diff;
+      lp_b += udg * db;
+      const float l1_up = log1pf(x_if(k));
+      const Lev L = level(k, l1_up, l1_dn);
+      l1_dn = l1_up;
       const float t = T + lev(k, 4);
       const float adj = adj_of(hum_at(k));
       const float ke = (u * u + v * v) * sec2 * 0.5f;
       st(a.o_KE, k, ke + a.R * (suf + t * ((adj - 1.f) * lev(k, 5) + adj * L.dal)));
       suf += t * ((adj - 1.f) * lev(k, 6) + adj * L.dlr);
     }
+    a.fwd[((size_t)a.o_lnps + mb) * IJ + col] = -(lp_a + lp_b);
   }
 
   // Pass C.
@@ -832,6 +836,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
     q_p[t] = 0.f;
     q_c[t] = t < a.nT ? ld(a.p_tr + t * mK, 0) : 0.f;
   }
+  float l1_up = log1pf(x_if(0));
   for (int k = 0; k < K; ++k) {
     const bool has_up = k > 0, has_dn = k + 1 < K;
     const float u_n = has_dn ? ld(a.p_u, k + 1) : 0.f;
@@ -853,8 +858,13 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
       const float fd = has_dn ? md * (xn - xc) : 0.f;
       return -0.5f * (fu + fd) * inv_dp;
     };
-    const Lev L = level(k);
-    const float q_h = hum >= 0 ? q_c[hum] : 0.f;
+    const float l1_dn = log1pf(x_if(k + 1));
+    const Lev L = level(k, l1_up, l1_dn);
+    l1_up = l1_dn;
+    float q_h = 0.f;  // selected without a dynamic index (keeps q_c in registers)
+#pragma unroll
+    for (int t2 = 0; t2 < kMaxTracers; ++t2)
+      if (t2 == hum) q_h = q_c[t2];
     const float adj = adj_of(q_h);
     const float t = T_c + tr;
     // Pressure-gradient residual C_k(T, p_s) adj - C_k(T_ref, p_s_ref)
@@ -2685,6 +2695,7 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
       q[8] = (float)pu;
       q[9] = (float)dp;
       q[10] = (float)W;
+      q[11] = (float)(1.0 / dp);
     }
     hp[(size_t)K * kHybPack] = (float)A[K];
     hp[(size_t)K * kHybPack + 1] = (float)B[K];

@@ -14,7 +14,8 @@ import argparse
 import numpy as np
 import torch
 
-from dinosaur_b200 import coordinate_systems, held_suarez, primitive_equations as pe
+from dinosaur_b200 import coordinate_systems, held_suarez, hybrid_coordinates
+from dinosaur_b200 import primitive_equations as pe
 from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
 from dinosaur_b200 import time_integration as ti, units
 
@@ -28,17 +29,21 @@ def main():
   ap.add_argument('--moist', action='store_true',
                   help='specific humidity and two passive tracers')
   ap.add_argument('--precision', default='fp32', choices=['fp32', 'bf16x3', 'tf32x3'])
+  ap.add_argument('--hybrid', action='store_true',
+                  help='analytic hybrid sigma-pressure levels (PrimitiveEquationsHybrid)')
   ap.add_argument('--steps', type=int, default=3)
   ap.add_argument('--dt-minutes', type=float, default=15.0)
   args = ap.parse_args()
   impl = lambda **kw: sh.CudaSphericalHarmonics(precision=args.precision, **kw)
   g = getattr(sh.Grid, args.grid)(spherical_harmonics_impl=impl)
-  vert = sigma_coordinates.SigmaCoordinates.equidistant(args.layers)
+  vert = (hybrid_coordinates.HybridCoordinates.analytic_levels(args.layers) if args.hybrid
+          else sigma_coordinates.SigmaCoordinates.equidistant(args.layers))
   coords = coordinate_systems.CoordinateSystem(g, vert)
   ps = units.SimUnits()
   tref = np.full(args.layers, 285.0) if args.held_suarez else np.linspace(
       220.0, 288.0, args.layers)
-  eq = pe.PrimitiveEquationsSigma(
+  eq_cls = pe.PrimitiveEquationsHybrid if args.hybrid else pe.PrimitiveEquationsSigma
+  eq = eq_cls(
       tref, np.zeros(g.modal_shape, np.float32), coords, ps,
       humidity_key='specific_humidity' if args.moist else None)
   if args.held_suarez:
@@ -61,8 +66,11 @@ def main():
     dev = lambda a: torch.as_tensor(a, device='cuda')
     tracers = {'specific_humidity': dev(5e-3 * const) + 1e-2 * t(shape),
                'tracer_a': dev(const) + t(shape), 'tracer_b': dev(const) + t(shape)}
-  state = pe.State(t(shape), t(shape), t(shape), t(lead + (1,) + g.modal_shape),
-                   tracers=tracers)
+  lnps = t(lead + (1,) + g.modal_shape)
+  if args.hybrid:
+    # A physical surface pressure (1e5 Pa) as the l = 0 term.
+    lnps[..., 0, 0] += float(np.log(units.nondim_pressure(1e5)) * 2.0 * np.sqrt(np.pi))
+  state = pe.State(t(shape), t(shape), t(shape), lnps, tracers=tracers)
   eng = eq.engine(state)
   buf = eng.pack(state)
   eng.step_(buf, dt, step.filter_scaling, 1, graph=False)
@@ -73,7 +81,8 @@ def main():
   e1.record()
   torch.cuda.synchronize()
   print(f'{args.grid} K={args.layers} members={args.members} '
-        f'hs={args.held_suarez} moist={args.moist} {args.precision}: '
+        f'hs={args.held_suarez} moist={args.moist} hybrid={args.hybrid} '
+        f'{args.precision}: '
         f'{e0.elapsed_time(e1) / args.steps * 1e3:.1f} us/step, '
         f'finite={bool(torch.isfinite(buf).all())}')
 
