@@ -802,9 +802,18 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
     float lp_a = 0.f, lp_b = 0.f, suf = 0.f;
     const float inv_ps_diff = -dps / ps / psr;  // 1 / p_s - 1 / p_s_ref
     float l1_dn = log1pf(x_if(K));
+    // Level k's inputs were loaded during level k + 1 (one level ahead).
+    float u_x = ld(a.p_u, K - 1), v_x = ld(a.p_v, K - 1), d_x = ld(a.p_div, K - 1),
+          T_x = ld(a.p_temp, K - 1), q_x = hum_at(K - 1);
     for (int k = K - 1; k >= 0; --k) {
-      const float u = ld(a.p_u, k), v = ld(a.p_v, k), d = ld(a.p_div, k);
-      const float T = ld(a.p_temp, k);
+      const float u = u_x, v = v_x, d = d_x, T = T_x, q = q_x;
+      if (k > 0) {
+        u_x = ld(a.p_u, k - 1);
+        v_x = ld(a.p_v, k - 1);
+        d_x = ld(a.p_div, k - 1);
+        T_x = ld(a.p_temp, k - 1);
+        q_x = hum_at(k - 1);
+      }
       const float da = lev(k, 2), db = lev(k, 3);
       const float udg = (u * gx + v * gy) * sec2;
       const float dp = da + db * ps;
@@ -817,7 +826,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
       const Lev L = level(k, l1_up, l1_dn);
       l1_dn = l1_up;
       const float t = T + lev(k, 4);
-      const float adj = adj_of(hum_at(k));
+      const float adj = adj_of(q);
       const float ke = (u * u + v * v) * sec2 * 0.5f;
       st(a.o_KE, k, ke + a.R * (suf + t * ((adj - 1.f) * lev(k, 5) + adj * L.dal)));
       suf += t * ((adj - 1.f) * lev(k, 6) + adj * L.dlr);
@@ -837,12 +846,26 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
     q_c[t] = t < a.nT ? ld(a.p_tr + t * mK, 0) : 0.f;
   }
   float l1_up = log1pf(x_if(0));
+  // zeta, div of level k and u, v, T of level k + 1 were loaded during
+  // level k - 1.
+  float zeta_x = ld(a.p_vort, 0), d_x = ld(a.p_div, 0);
+  float u_x = K > 1 ? ld(a.p_u, 1) : 0.f, v_x = K > 1 ? ld(a.p_v, 1) : 0.f,
+        T_x = K > 1 ? ld(a.p_temp, 1) : 0.f;
   for (int k = 0; k < K; ++k) {
     const bool has_up = k > 0, has_dn = k + 1 < K;
-    const float u_n = has_dn ? ld(a.p_u, k + 1) : 0.f;
-    const float v_n = has_dn ? ld(a.p_v, k + 1) : 0.f;
-    const float T_n = has_dn ? ld(a.p_temp, k + 1) : 0.f;
-    const float zeta = ld(a.p_vort, k), d = ld(a.p_div, k);
+    const float u_n = u_x, v_n = v_x, T_n = T_x;
+    const float zeta = zeta_x, d = d_x;
+    if (has_dn) {
+      zeta_x = ld(a.p_vort, k + 1);
+      d_x = ld(a.p_div, k + 1);
+      if (k + 2 < K) {
+        u_x = ld(a.p_u, k + 2);
+        v_x = ld(a.p_v, k + 2);
+        T_x = ld(a.p_temp, k + 2);
+      } else {
+        u_x = v_x = T_x = 0.f;
+      }
+    }
     const float da = lev(k, 2), db = lev(k, 3), tr = lev(k, 4), alr = lev(k, 5);
     const float udg = (u_c * gx + v_c * gy) * sec2;
     const float dp = da + db * ps;
