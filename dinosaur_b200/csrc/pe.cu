@@ -672,9 +672,11 @@ __global__ void __launch_bounds__(kNodalCols * kNodalMaxChunks)
 //   0 a_{k-1/2}  1 b_{k-1/2}  2 da_k  3 db_k  4 T_ref,k  5 alpha_k
 //   6 log(p_{k+1/2} / p_{k-1/2})  7 s_k = W_k p_s / max(dp_k, 1e-6 p_s)
 //   8 p_{k-1/2}  9 dp_k  10 W_k = log-ratio_k b_{k-1/2} + alpha_k db_k
-//   11 1 / dp_k
-// followed by a, b and p (at p_s_ref) of the lowest interface.
-constexpr int kHybPack = 12;
+//   11 1 / dp_k  12 1 / P_{k-1/2}  13 b_{k-1/2} / P_{k-1/2}
+// (P = max(p, 1e-6 p_s_ref), the floored interface pressure), followed by
+// a, b, p, 1 / P and b / P of the lowest interface.
+constexpr int kHybPack = 16;
+constexpr int kHybTail = 5;
 constexpr int kHybThreads = 128;
 
 struct HybridArgs {
@@ -721,7 +723,7 @@ struct HybridArgs {
 __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs a) {
   extern __shared__ float s_hyb[];
   const int K = a.K;
-  for (int i = threadIdx.x; i < K * kHybPack + 3; i += blockDim.x) s_hyb[i] = a.lev[i];
+  for (int i = threadIdx.x; i < K * kHybPack + kHybTail; i += blockDim.x) s_hyb[i] = a.lev[i];
   __syncthreads();
   const unsigned IJ = (unsigned)a.I * (unsigned)a.J;
   const unsigned col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -743,6 +745,8 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
   auto a_if = [&](int i) -> float { return i < K ? lev(i, 0) : s_hyb[K * kHybPack]; };
   auto b_if = [&](int i) -> float { return i < K ? lev(i, 1) : s_hyb[K * kHybPack + 1]; };
   auto pr_if = [&](int i) -> float { return i < K ? lev(i, 8) : s_hyb[K * kHybPack + 2]; };
+  auto ipr_if = [&](int i) -> float { return i < K ? lev(i, 12) : s_hyb[K * kHybPack + 3]; };
+  auto bpr_if = [&](int i) -> float { return i < K ? lev(i, 13) : s_hyb[K * kHybPack + 4]; };
   const float gx = __ldg(a.nod + ((size_t)a.p_gx + mb) * IJ + col);
   const float gy = __ldg(a.nod + ((size_t)a.p_gy + mb) * IJ + col);
   const float psr = a.ps_ref;
@@ -758,16 +762,13 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
   // Virtual-temperature factor 1 + (R_v / R - 1) q.
   auto adj_of = [&](float q) -> float { return hum >= 0 ? 1.f + (a.Rv_over_R - 1.f) * q : 1.f; };
   // (P_i - P_i,ref) / P_i,ref of the floored interface pressure max(p, 1e-6 p_s).
+  // Unfloored: b dps / P_ref; floored both ways: dps / p_s_ref.
+  const float inv_psr = 1.f / psr;
   auto x_if = [&](int i) -> float {
     const float p = a_if(i) + b_if(i) * ps, pr = pr_if(i);
-    float dP;
-    if (p >= floor_s && pr >= floor_r)
-      dP = b_if(i) * dps;
-    else if (p < floor_s && pr < floor_r)
-      dP = 1e-6f * dps;
-    else
-      dP = fmaxf(p, floor_s) - fmaxf(pr, floor_r);
-    return dP / fmaxf(pr, floor_r);
+    if (p >= floor_s && pr >= floor_r) return dps * bpr_if(i);
+    if (p < floor_s && pr < floor_r) return dps * inv_psr;
+    return (fmaxf(p, floor_s) - fmaxf(pr, floor_r)) * ipr_if(i);
   };
   // Level k at this column, given log1p(x) of its upper and lower interfaces
   // (each interface's value is carried to the next level): deviations of the
@@ -915,7 +916,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
     const float fF = cumF + DF, fE = cumE + DE;
     const float gF = (alr * fF + alr_prev * fF_prev) * inv_dp;
     const float gE = (alr * fE + alr_prev * fE_prev) * inv_dp;
-    const float sudg = udg * ps * L.W / fmaxf(dp, floor_s);
+    const float sudg = udg * ps * L.W * (dp >= floor_s ? inv_dp : 1.f / floor_s);
     const float mean_part = tr * (sudg - gE);
     float var_part;
     if (hum < 0) {
@@ -2240,7 +2241,7 @@ static int launch_nodal_hybrid(dino_pe* pe, const float* state, cudaStream_t st)
   a.Rv_over_R = (float)(pe->Rv / pe->R);
   a.Cpv_over_Cp = (float)(pe->Cpv / (pe->R / pe->kappa));
   const dim3 grid(ceil_div((int)pe->IJ, kHybThreads), pe->mem);
-  const size_t smem = sizeof(float) * ((size_t)K * kHybPack + 3);
+  const size_t smem = sizeof(float) * ((size_t)K * kHybPack + kHybTail);
   pe_nodal_hybrid_kernel<<<grid, kHybThreads, smem, st>>>(a);
   return check_launch("pe_nodal_hybrid");
 }
@@ -2697,7 +2698,7 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
     const double* A = d->hybrid_a_boundaries;
     const double* B = d->hybrid_b_boundaries;
     const double psr = pe->ps_ref;
-    std::vector<float> hp((size_t)K * kHybPack + 3, 0.f);
+    std::vector<float> hp((size_t)K * kHybPack + kHybTail, 0.f);
     for (int k = 0; k < K; ++k) {
       const double pu = A[k] + B[k] * psr, pd = A[k + 1] + B[k + 1] * psr;
       DINO_REQUIRE(pd - pu > 0, DINO_ERR_ARG, "Pressure must decrease monotonically with height.");
@@ -2719,10 +2720,15 @@ static int pe_build(dino_pe* pe, const dino_pe_desc* d) {
       q[9] = (float)dp;
       q[10] = (float)W;
       q[11] = (float)(1.0 / dp);
+      q[12] = (float)(1.0 / std::max(pu, 1e-6 * psr));
+      q[13] = (float)(B[k] / std::max(pu, 1e-6 * psr));
     }
+    const double pK = A[K] + B[K] * psr;
     hp[(size_t)K * kHybPack] = (float)A[K];
     hp[(size_t)K * kHybPack + 1] = (float)B[K];
-    hp[(size_t)K * kHybPack + 2] = (float)(A[K] + B[K] * psr);
+    hp[(size_t)K * kHybPack + 2] = (float)pK;
+    hp[(size_t)K * kHybPack + 3] = (float)(1.0 / std::max(pK, 1e-6 * psr));
+    hp[(size_t)K * kHybPack + 4] = (float)(B[K] / std::max(pK, 1e-6 * psr));
     DINO_TRY(upload_vec(&pe->d_hyb, hp));
   }
 

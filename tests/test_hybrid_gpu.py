@@ -184,3 +184,28 @@ def test_graph_replay_equals_eager():
   graph = ti.FusedSIL3Step(eq, dt, n_steps=3, use_graph=True)(s)
   for k in KEYS:
     assert torch.equal(getattr(eager, k), getattr(graph, k)), k
+
+
+def test_implicit_vjps_pass_the_dot_test():
+  # The implicit terms and their inverse are linear; their VJPs (transposed
+  # per-wavenumber operators with the hybrid ln p_s column and thickness row)
+  # satisfy <w, A v> = <A^T w, v> to FP32 rounding (<= 1e-5 relative).
+  og, oeq, st, g, eq = make_hybrid(8)
+  rng = np.random.default_rng(3)
+  _, l = og.modal_mesh
+  def rand_state():
+    f = lambda n: torch.as_tensor(
+        (rng.standard_normal((n,) + og.modal_shape) * og.mask / (l + 1.0)).astype(np.float32),
+        device='cuda')
+    return pe.State(f(8), f(8), f(8), f(1))
+  dot = lambda a, b: sum(float((getattr(a, k).double() * getattr(b, k).double()).sum())
+                         for k in KEYS)
+  for op in (eq.implicit_terms, lambda s: eq.implicit_inverse(s, 0.05)):
+    v, w = rand_state(), rand_state()
+    x = pe.State(*[getattr(v, k).clone().requires_grad_() for k in KEYS])
+    y = op(x)
+    loss = sum((getattr(y, k) * getattr(w, k)).sum() for k in KEYS)
+    loss.backward()
+    lhs = dot(w, op(v))
+    rhs = sum(float((getattr(x, k).grad.double() * getattr(v, k).double()).sum()) for k in KEYS)
+    assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs)), (lhs, rhs)
