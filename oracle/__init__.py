@@ -3,15 +3,16 @@
 TEST INFRASTRUCTURE ONLY. This package restates, in double precision NumPy,
 the algorithm of neuralgcm/dinosaur 1.3.6 for the hot path that
 ``dinosaur_b200`` implements in CUDA: the spherical-harmonic transform pair,
-the spectral operators, the sigma-coordinate primitive equations (explicit
-terms, implicit terms, implicit inverse), the ``imex_rk_sil3`` integrator with
+the spectral operators, the sigma-coordinate and hybrid-coordinate primitive
+equations (explicit terms, implicit terms, implicit inverse), the
+``imex_rk_sil3`` integrator with
 its exponential step filter, Held-Suarez forcing and the initial states used
 as fixtures.  Every function cites the reference file and line range it
 follows.
 
 Only the test suite, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` /
 ``--impl reference`` legs of ``bench.py`` may import this package, and only as
-the checker or the timed CPU baseline.  The product path (``dinosaur_b200``)
+the reference values a result is compared with, or as the timed CPU baseline.  The product path (``dinosaur_b200``)
 never imports it and fails loudly when its CUDA library is missing.
 
 Parity pins: ``tests/golden/make_golden.py`` imports the reference's own
