@@ -305,6 +305,41 @@ def phase_bytes(phase, fields, precision, name=GRID['name']):
           'legendre_forward': fourier + modal + table_bytes}[phase]
 
 
+def host_link(torch, h_in, d_in, d_out, h_out, s_in, s_out, stream, reps=5):
+  """The host link under the end-to-end loop: each direction alone, and one
+  step's input copied in while one step's output is copied out (two
+  streams, the same pinned buffers), CUDA events on the launching stream.
+  The duplex time is the floor of a pipelined end-to-end step."""
+  def timed(h2d, d2h):
+    for r in range(reps + 1):
+      if r == 1:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s_in.wait_stream(stream)
+        s_out.wait_stream(stream)
+      if h2d:
+        with torch.cuda.stream(s_in):
+          d_in.copy_(h_in, non_blocking=True)
+      if d2h:
+        with torch.cuda.stream(s_out):
+          h_out.copy_(d_out, non_blocking=True)
+    stream.wait_stream(s_in)
+    stream.wait_stream(s_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+  nbytes = h_in.numel() * h_in.element_size()
+  ms_in, ms_out, ms_both = timed(True, False), timed(False, True), timed(True, True)
+  return {'h2d_gbs': nbytes / (ms_in * 1e-3) / 1e9,
+          'd2h_gbs': nbytes / (ms_out * 1e-3) / 1e9,
+          'duplex_gbs': 2 * nbytes / (ms_both * 1e-3) / 1e9,
+          'step_ms': ms_both,
+          'what': 'bound_tflops = algorithmic flops per step / duplex copy time of one '
+                  'step\'s input and output; frac = e2e value / bound'}
+
+
 def time_phases(torch, plan, x, name, reps):
   """Milliseconds per launch of each transform phase over x's fields (CUDA
   events on the launching stream, after two untimed launches)."""
@@ -553,6 +588,9 @@ def run_ours(args):
   e2e_value = aggregate_tflops(sht_flops(fields), world, ms_e2e)
   e2e_err = float(torch.linalg.vector_norm(out_host.cuda() - y) /
                   torch.linalg.vector_norm(y))
+  link = host_link(torch, x_host, xs[0], ys[1], out_host, s_in, s_out, stream)
+  link['bound_tflops'] = aggregate_tflops(sht_flops(fields), world, link['step_ms'])
+  link['frac'] = e2e_value / link['bound_tflops']
 
   # Per-phase kernel timing (live CUDA events on the launching stream).
   phase_ms = time_phases(torch, plan, x, GRID['name'], max(5, args.steps))
@@ -606,7 +644,8 @@ def run_ours(args):
                 'host_buffers': ('pinned, on the GPU NUMA node'
                                  if gpu_local_cpus(torch, torch.cuda.current_device())
                                  else 'pinned'),
-                'result_matches_device_run': e2e_err == 0.0},
+                'result_matches_device_run': e2e_err == 0.0,
+                'link': link},
         'roofline': {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved,
                      'peak': hbm_peak, 'unit': 'GB/s',
                      'frac': achieved / hbm_peak, 'peak_source': peak_src,
