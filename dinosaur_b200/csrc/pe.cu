@@ -724,6 +724,9 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
   extern __shared__ float s_hyb[];
   const int K = a.K;
   for (int i = threadIdx.x; i < K * kHybPack + kHybTail; i += blockDim.x) s_hyb[i] = a.lev[i];
+  // log1p(x) of this column's K + 1 interfaces, computed in the bottom-up
+  // pass and reused top-down (interface i at s_l1[i * blockDim.x + tid]).
+  float* s_l1 = s_hyb + K * kHybPack + kHybTail;
   __syncthreads();
   const unsigned IJ = (unsigned)a.I * (unsigned)a.J;
   const unsigned col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -803,6 +806,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
     float lp_a = 0.f, lp_b = 0.f, suf = 0.f;
     const float inv_ps_diff = -dps / ps / psr;  // 1 / p_s - 1 / p_s_ref
     float l1_dn = log1pf(x_if(K));
+    s_l1[K * blockDim.x + threadIdx.x] = l1_dn;
     // Level k's inputs were loaded during level k + 1 (one level ahead).
     float u_x = ld(a.p_u, K - 1), v_x = ld(a.p_v, K - 1), d_x = ld(a.p_div, K - 1),
           T_x = ld(a.p_temp, K - 1), q_x = hum_at(K - 1);
@@ -824,6 +828,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
       lp_a += d * da * inv_ps_diff;
       lp_b += udg * db;
       const float l1_up = log1pf(x_if(k));
+      s_l1[k * blockDim.x + threadIdx.x] = l1_up;
       const Lev L = level(k, l1_up, l1_dn);
       l1_dn = l1_up;
       const float t = T + lev(k, 4);
@@ -846,7 +851,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
     q_p[t] = 0.f;
     q_c[t] = t < a.nT ? ld(a.p_tr + t * mK, 0) : 0.f;
   }
-  float l1_up = log1pf(x_if(0));
+  float l1_up = s_l1[threadIdx.x];
   // zeta, div of level k and u, v, T of level k + 1 were loaded during
   // level k - 1.
   float zeta_x = ld(a.p_vort, 0), d_x = ld(a.p_div, 0);
@@ -882,7 +887,7 @@ __global__ void __launch_bounds__(kHybThreads) pe_nodal_hybrid_kernel(HybridArgs
       const float fd = has_dn ? md * (xn - xc) : 0.f;
       return -0.5f * (fu + fd) * inv_dp;
     };
-    const float l1_dn = log1pf(x_if(k + 1));
+    const float l1_dn = s_l1[(k + 1) * blockDim.x + threadIdx.x];
     const Lev L = level(k, l1_up, l1_dn);
     l1_up = l1_dn;
     float q_h = 0.f;  // selected without a dynamic index (keeps q_c in registers)
@@ -2241,7 +2246,8 @@ static int launch_nodal_hybrid(dino_pe* pe, const float* state, cudaStream_t st)
   a.Rv_over_R = (float)(pe->Rv / pe->R);
   a.Cpv_over_Cp = (float)(pe->Cpv / (pe->R / pe->kappa));
   const dim3 grid(ceil_div((int)pe->IJ, kHybThreads), pe->mem);
-  const size_t smem = sizeof(float) * ((size_t)K * kHybPack + kHybTail);
+  const size_t smem = sizeof(float) * ((size_t)K * kHybPack + kHybTail +
+                                       (size_t)(K + 1) * kHybThreads);
   pe_nodal_hybrid_kernel<<<grid, kHybThreads, smem, st>>>(a);
   return check_launch("pe_nodal_hybrid");
 }
