@@ -55,3 +55,32 @@ def test_plan_rejects_bad_shapes_without_gpu():
   rc = lib.dino_plan_create(ctypes.byref(desc), 8, 0, ctypes.byref(h))
   assert rc == _lib.DINO_ERR_SHAPE
   assert 'n_m <= n_l' in _lib.last_error()
+
+
+@pytest.mark.parametrize('cname,pyname', [('dino_grid_desc', 'GridDesc'),
+                                          ('dino_pe_desc', 'PEDesc'),
+                                          ('dino_swe_desc', 'SWEDesc')])
+def test_descriptor_layouts_match_the_header(cname, pyname, tmp_path):
+  """The ctypes mirrors of the descriptor structs have the header's size and
+  field offsets (a C program compiled against include/dino_b200.h prints
+  them)."""
+  import shutil
+  import subprocess
+  gcc = shutil.which('gcc') or shutil.which('cc')
+  if gcc is None:
+    pytest.skip('no C compiler')
+  py = getattr(_lib, pyname)
+  fields = [f[0] for f in py._fields_]
+  src = tmp_path / 'layout.c'
+  lines = ['#include <stdio.h>', '#include "dino_b200.h"', 'int main(void) {',
+           f'  printf("%zu\\n", sizeof({cname}));']
+  lines += [f'  printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+  lines += ['  return 0;', '}']
+  src.write_text('\n'.join(lines) + '\n')
+  exe = tmp_path / 'layout'
+  subprocess.run([gcc, '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(exe)],
+                 check=True, capture_output=True)
+  out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                        text=True).stdout.split()]
+  assert out[0] == ctypes.sizeof(py), (out[0], ctypes.sizeof(py))
+  assert out[1:] == [getattr(py, f).offset for f in fields]
