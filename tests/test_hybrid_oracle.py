@@ -78,3 +78,36 @@ def test_package_levels_match_oracle():
   np.testing.assert_allclose(s.layer_thickness(2.0), 2.0 / 8)
   with pytest.raises(ValueError):
     hc.HybridCoordinates(np.zeros(3), np.zeros(4))
+
+
+@pytest.mark.parametrize('levels', ['analytic', 'sigma_like', 'ecmwf_like'])
+def test_package_hybrid_matrices_match_oracle(levels):
+  """The FP64 host matrices that the CUDA engine's implicit operators are
+  built from (geopotential G, temperature H, the ln p_s column) equal the
+  oracle's restatement."""
+  from dinosaur_b200 import hybrid_coordinates as hc
+  from dinosaur_b200 import primitive_equations as pe
+  from dinosaur_b200 import sigma_coordinates as sc
+  from dinosaur_b200 import units
+  k = 12
+  lev = {'analytic': lambda: hc.HybridCoordinates.analytic_levels(k),
+         'sigma_like': lambda: hc.HybridCoordinates.from_sigma_levels(
+             sc.SigmaCoordinates.equidistant(k)),
+         'ecmwf_like': lambda: hc.HybridCoordinates.analytic_ecmwf_like(k)}[levels]()
+  # FP64 levels on both sides: the formulas are compared, not dtype rules
+  # (sigma levels are float32, and NumPy keeps b * p_s float32 then, as the
+  # reference does).
+  nd = hc.HybridCoordinates(
+      units.nondim_pressure(np.asarray(lev.a_boundaries, np.float64) * 100.0),
+      np.asarray(lev.b_boundaries, np.float64))
+  olev = oh.HybridCoordinates(nd.a_boundaries, nd.b_boundaries)
+  psr = units.nondim_pressure(101325.0)
+  tref = np.linspace(210.0, 290.0, k)
+  R, kappa = 0.5, 2 / 7
+  np.testing.assert_allclose(pe.get_geopotential_weights_hybrid(nd, R, psr),
+                             oh.geopotential_weights(olev, R, psr), rtol=1e-12, atol=0)
+  np.testing.assert_allclose(pe.get_temperature_implicit_weights_hybrid(nd, tref, kappa, psr),
+                             oh.temperature_implicit_weights(olev, tref, kappa, psr),
+                             rtol=1e-12, atol=1e-12)
+  np.testing.assert_allclose(pe.pgf_lps_coefficient_hybrid(tref, psr, nd, R),
+                             oh.pgf_coefficient(tref, psr, olev, R), rtol=1e-12, atol=0)
