@@ -45,8 +45,15 @@ def make_hybrid(layers=8, levels='analytic', with_tracers=False, humidity=None,
   st['divergence'] = st['divergence'] + 1e-3 * noise(layers)
   st['log_surface_pressure'] = st['log_surface_pressure'] + 1e-3 * noise(1)
   st = od.tree_map(lambda x: np.asarray(x, np.float32).astype(np.float64), st)
-  olev = (oh.HybridCoordinates.analytic_levels(layers) if levels == 'analytic'
-          else oh.HybridCoordinates.from_sigma_levels(vert))
+  if levels == 'analytic':
+    olev = oh.HybridCoordinates.analytic_levels(layers)
+  elif levels == 'ecmwf_like':
+    # pure-pressure layers (b = 0) above 80 hPa, hybrid below
+    e = hc.HybridCoordinates.analytic_ecmwf_like(layers)
+    olev = oh.HybridCoordinates(np.asarray(e.a_boundaries, np.float64),
+                                np.asarray(e.b_boundaries, np.float64))
+  else:
+    olev = oh.HybridCoordinates.from_sigma_levels(vert)
   oeq = oh.PrimitiveEquationsHybrid(tref, orog, og, olev, od.SimUnits(),
                                     humidity_key=humidity)
   g = getattr(sh.Grid, grid_name)()
@@ -57,9 +64,10 @@ def make_hybrid(layers=8, levels='analytic', with_tracers=False, humidity=None,
   return og, oeq, st, g, eq
 
 
-@pytest.mark.parametrize('layers', [8, 20])
-def test_explicit_terms_match_oracle(layers):
-  og, oeq, st, g, eq = make_hybrid(layers)
+@pytest.mark.parametrize('layers,levels', [(8, 'analytic'), (20, 'analytic'),
+                                           (20, 'ecmwf_like')])
+def test_explicit_terms_match_oracle(layers, levels):
+  og, oeq, st, g, eq = make_hybrid(layers, levels=levels)
   got = eq.explicit_terms(to_state(st))
   assert_state(got, oeq.explicit_terms(st), 1e-4)
   for k in KEYS:
