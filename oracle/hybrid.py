@@ -8,6 +8,13 @@ the Simmons & Burridge helpers and ``PrimitiveEquationsHybrid``,
 orography, horizontal advection, virtual temperature) come from
 ``oracle.dycore.PrimitiveEquationsSigma``, which follows the same base class
 (:670-833).
+
+Parity pins: ``tests/golden/pe_hybrid_T21_L6.npz`` holds the reference's own
+PrimitiveEquationsHybrid outputs (explicit, implicit, implicit inverse, one
+filtered SIL3 step on 6 analytic levels, written by
+``tests/golden/make_golden.py``), checked in ``tests/test_oracle_golden.py``;
+the reference test suite's sigma-like equivalence and implicit-inverse
+identity are checked in ``tests/test_hybrid_oracle.py``.
 """
 
 from __future__ import annotations

@@ -381,6 +381,9 @@ def _dims_mul(a, b, sign=1):
 
 
 class Quantity:
+  # NumPy defers ndarray * Quantity to __rmul__ (as with pint's quantities).
+  __array_ufunc__ = None
+
   def __init__(self, magnitude, dims=None):
     self.magnitude = magnitude
     self.dimensionality = _Dims(dims or {})

@@ -38,6 +38,7 @@ def main(reference_root='/root/reference'):
   from dinosaur import filtering
   from dinosaur import fourier
   from dinosaur import held_suarez
+  from dinosaur import hybrid_coordinates
   from dinosaur import primitive_equations
   from dinosaur import primitive_equations_states
   from dinosaur import sigma_coordinates
@@ -154,6 +155,23 @@ def main(reference_root='/root/reference'):
         **pack('in', state), **pack('explicit', expl),
         **pack('implicit', impl), **pack('inverse', inv),
         **pack('step1', s1), **pack('step2', s2))
+
+  # -- hybrid sigma-pressure levels (primitive_equations.py:1961-2533) -----
+  # The same input state on 6 analytic hybrid levels (a in hPa).
+  hyb_levels = hybrid_coordinates.HybridCoordinates.analytic_levels(layers)
+  hyb_coords = coordinate_systems.CoordinateSystem(horizontal=grid,
+                                                   vertical=hyb_levels)
+  hyb_eq = primitive_equations.PrimitiveEquationsHybrid(
+      ref_temps, orography, hyb_coords, physics_specs)
+  hyb_step = time_integration.step_with_filters(
+      time_integration.imex_rk_sil3(hyb_eq, dt),
+      [time_integration.exponential_step_filter(grid, dt)])
+  _save('pe_hybrid_T21_L6.npz',
+        a_boundaries=hyb_levels.a_boundaries, b_boundaries=hyb_levels.b_boundaries,
+        **pack('explicit', hyb_eq.explicit_terms(state)),
+        **pack('implicit', hyb_eq.implicit_terms(state)),
+        **pack('inverse', hyb_eq.implicit_inverse(state, 0.05)),
+        **pack('step1', hyb_step(state)))
 
   # -- digital filter initialisation (time_integration.py:645-712) ---------
   dfi_dt = dt

@@ -260,3 +260,25 @@ def test_digital_filter_initialization_matches_reference(pe_setup):
       eq, dycore.imex_rk_sil3, [dycore.exponential_step_filter(grid, dt)],
       8 * dt, 8 * dt, dt)
   assert_state_close(dfi(s), unpack(d, 'dfi'), atol=1e-10)
+
+
+def test_hybrid_terms_and_step_match_reference(pe_setup):
+  """PrimitiveEquationsHybrid on 6 analytic hybrid levels, same input state
+  (pe_hybrid_T21_L6.npz).  The reference differences its float32 reference
+  temperatures in float32 (get_temperature_implicit_weights_hybrid's
+  np.diff), 1.1e-7 of the implicit temperature term; hence 1e-6 for the
+  implicit terms, 1e-8 elsewhere (the step measures 1e-9)."""
+  from oracle import hybrid
+  g0, grid, _, _ = pe_setup
+  g = load('pe_hybrid_T21_L6.npz')
+  eq = hybrid.PrimitiveEquationsHybrid(
+      g0['ref_temps'], g0['orography'], grid,
+      hybrid.HybridCoordinates(g['a_boundaries'], g['b_boundaries']), dycore.SimUnits())
+  s = unpack(g0, 'in')
+  assert_state_close(eq.explicit_terms(s), unpack(g, 'explicit'), atol=1e-8)
+  assert_state_close(eq.implicit_terms(s), unpack(g, 'implicit'), atol=1e-6)
+  assert_state_close(eq.implicit_inverse(s, 0.05), unpack(g, 'inverse'), atol=1e-8)
+  dt = 0.175008
+  step = dycore.step_with_filters(dycore.imex_rk_sil3(eq, dt),
+                                  [dycore.exponential_step_filter(grid, dt)])
+  assert_state_close(step(s), unpack(g, 'step1'), atol=1e-8)
