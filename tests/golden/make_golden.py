@@ -204,6 +204,14 @@ def main(reference_root='/root/reference'):
         **pack('explicit', expl_m),
         explicit_humidity=expl_m.tracers['specific_humidity'],
         explicit_tracer=expl_m.tracers['tracer'])
+  # the same moist state on the 6 analytic hybrid levels
+  hyb_eq_moist = primitive_equations.PrimitiveEquationsHybrid(
+      ref_temps, orography, hyb_coords, physics_specs,
+      humidity_key='specific_humidity')
+  expl_hm = hyb_eq_moist.explicit_terms(moist_state)
+  _save('pe_hybrid_moist_T21_L6.npz', **pack('explicit', expl_hm),
+        explicit_humidity=expl_hm.tracers['specific_humidity'],
+        explicit_tracer=expl_hm.tracers['tracer'])
 
   # -- Held-Suarez forcing composed with the primitive equations ---------
   hs_coords = coordinate_systems.CoordinateSystem(

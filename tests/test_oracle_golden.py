@@ -282,3 +282,25 @@ def test_hybrid_terms_and_step_match_reference(pe_setup):
   step = dycore.step_with_filters(dycore.imex_rk_sil3(eq, dt),
                                   [dycore.exponential_step_filter(grid, dt)])
   assert_state_close(step(s), unpack(g, 'step1'), atol=1e-8)
+
+
+def test_moist_hybrid_terms_match_reference(pe_setup):
+  """Moist PrimitiveEquationsHybrid with a passive tracer on the 6 analytic
+  levels (pe_hybrid_moist_T21_L6.npz; inputs of pe_moist_T21_L6.npz)."""
+  from oracle import hybrid
+  g0, grid, _, _ = pe_setup
+  g = load('pe_hybrid_T21_L6.npz')
+  gm = load('pe_moist_T21_L6.npz')
+  ghm = load('pe_hybrid_moist_T21_L6.npz')
+  eq = hybrid.PrimitiveEquationsHybrid(
+      g0['ref_temps'], g0['orography'], grid,
+      hybrid.HybridCoordinates(g['a_boundaries'], g['b_boundaries']), dycore.SimUnits(),
+      humidity_key='specific_humidity')
+  s = unpack(g0, 'in', tracers={'specific_humidity': gm['humidity'],
+                                'tracer': gm['tracer']})
+  out = eq.explicit_terms(s)
+  assert_state_close(out, unpack(ghm, 'explicit'), atol=1e-8)
+  for k, ref in (('specific_humidity', ghm['explicit_humidity']),
+                 ('tracer', ghm['explicit_tracer'])):
+    scale = np.abs(ref).max()
+    close(out['tracers'][k] / scale, ref / scale, atol=1e-8)
