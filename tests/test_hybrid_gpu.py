@@ -217,3 +217,28 @@ def test_implicit_vjps_pass_the_dot_test():
     lhs = dot(w, op(v))
     rhs = sum(float((getattr(x, k).grad.double() * getattr(v, k).double()).sum()) for k in KEYS)
     assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def test_engine_matches_reference_golden_vectors():
+  # The reference's own PrimitiveEquationsHybrid, run in float64
+  # (tests/golden/pe_hybrid_T21_L6.npz: 6 analytic levels), against the CUDA
+  # engine fed the FP32-rounded input state (that rounding alone moves the
+  # small ln p_s tendency by 1.1e-5 of its maximum, the rest by <= 4e-7).
+  import os
+  gdir = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+  g0 = np.load(os.path.join(gdir, 'pe_T21_L6.npz'))
+  g = np.load(os.path.join(gdir, 'pe_hybrid_T21_L6.npz'))
+  grid = sh.Grid.T21()
+  coords = coordinate_systems.CoordinateSystem(
+      grid, hc.HybridCoordinates(g['a_boundaries'], g['b_boundaries']))
+  eq = pe.PrimitiveEquationsHybrid(g0['ref_temps'], g0['orography'].astype(np.float32),
+                                   coords, units.SimUnits())
+  s = pe.State(*[torch.as_tensor(g0['in_' + k], device='cuda', dtype=torch.float32)
+                 for k in KEYS])
+  ref = lambda prefix: dict({k: g[f'{prefix}_{k}'] for k in KEYS}, tracers={})
+  assert_state(eq.explicit_terms(s), ref('explicit'), 1e-4)
+  assert_state(eq.implicit_terms(s), ref('implicit'), 1e-5)
+  assert_state(eq.implicit_inverse(s, 0.05), ref('inverse'), 1e-5)
+  dt = 0.175008
+  step = ti.step_with_filters(ti.imex_rk_sil3(eq, dt), [ti.exponential_step_filter(grid, dt)])
+  assert_state(step(s), ref('step1'), 1e-4)
