@@ -156,6 +156,21 @@ def main(reference_root='/root/reference'):
         **pack('implicit', impl), **pack('inverse', inv),
         **pack('step1', s1), **pack('step2', s2))
 
+  # -- hybrid level constructors (hybrid_coordinates.py:268-471) ----------
+  lv_a = hybrid_coordinates.HybridCoordinates.analytic_levels(17)
+  lv_e = hybrid_coordinates.HybridCoordinates.analytic_ecmwf_like(20)
+  lv_s = hybrid_coordinates.HybridCoordinates.from_sigma_levels(
+      sigma_coordinates.SigmaCoordinates.equidistant(8))
+  lv_c = hybrid_coordinates.HybridCoordinates.from_coefficients(
+      [0.0, 0.1, 0.05, 0.0], [0.0, 0.2, 0.6, 1.0], p0=1013.25)
+  _save('hybrid_levels.npz',
+        analytic_a=lv_a.a_boundaries, analytic_b=lv_a.b_boundaries,
+        ecmwf_like_a=lv_e.a_boundaries, ecmwf_like_b=lv_e.b_boundaries,
+        sigma_a=lv_s.a_boundaries, sigma_b=lv_s.b_boundaries,
+        coeffs_a=lv_c.a_boundaries, coeffs_b=lv_c.b_boundaries,
+        analytic_thickness_at_900=np.asarray(lv_a.layer_thickness(900.0)),
+        analytic_centers_at_900=np.asarray(lv_a.pressure_centers(900.0)))
+
   # -- hybrid sigma-pressure levels (primitive_equations.py:1961-2533) -----
   # The same input state on 6 analytic hybrid levels (a in hPa).
   hyb_levels = hybrid_coordinates.HybridCoordinates.analytic_levels(layers)

@@ -304,3 +304,23 @@ def test_moist_hybrid_terms_match_reference(pe_setup):
                  ('tracer', ghm['explicit_tracer'])):
     scale = np.abs(ref).max()
     close(out['tracers'][k] / scale, ref / scale, atol=1e-8)
+
+
+def test_package_hybrid_levels_match_reference():
+  """dinosaur_b200.hybrid_coordinates' constructors and pressure helpers
+  give the reference's levels (hybrid_levels.npz)."""
+  from dinosaur_b200 import hybrid_coordinates as hc
+  from dinosaur_b200 import sigma_coordinates as sc
+  g = load('hybrid_levels.npz')
+  cases = {'analytic': hc.HybridCoordinates.analytic_levels(17),
+           'ecmwf_like': hc.HybridCoordinates.analytic_ecmwf_like(20),
+           'sigma': hc.HybridCoordinates.from_sigma_levels(
+               sc.SigmaCoordinates.equidistant(8)),
+           'coeffs': hc.HybridCoordinates.from_coefficients(
+               [0.0, 0.1, 0.05, 0.0], [0.0, 0.2, 0.6, 1.0], p0=1013.25)}
+  for name, lev in cases.items():
+    close(lev.a_boundaries, g[f'{name}_a'], rtol=1e-15, atol=0)
+    close(lev.b_boundaries, g[f'{name}_b'], rtol=1e-15, atol=0)
+  lev = cases['analytic']
+  close(lev.layer_thickness(900.0), g['analytic_thickness_at_900'], rtol=1e-15, atol=1e-13)
+  close(lev.pressure_centers(900.0), g['analytic_centers_at_900'], rtol=1e-15, atol=1e-13)
