@@ -7,7 +7,9 @@ that the reference's own tests give it (primitive_equations_test.py:739-905):
 * implicit_inverse inverts (1 - eta implicit_terms) to atol 1e-5
   (test_implicit_inverse_sigma_like, :850-896), here also on analytic
   (non-sigma) levels;
-* the package's HybridCoordinates constructors give the oracle's levels.
+* the package's HybridCoordinates constructors give the oracle's levels;
+* the package's PrimitiveEquationsHybrid host checks (level scaling and
+  refusals) run without a GPU.
 """
 
 import numpy as np
@@ -111,3 +113,40 @@ def test_package_hybrid_matrices_match_oracle(levels):
                              rtol=1e-12, atol=1e-12)
   np.testing.assert_allclose(pe.pgf_lps_coefficient_hybrid(tref, psr, nd, R),
                              oh.pgf_coefficient(tref, psr, olev, R), rtol=1e-12, atol=0)
+
+
+def test_package_hybrid_equations_host_checks():
+  """Construction of PrimitiveEquationsHybrid is host logic: it accepts
+  hybrid levels, scales a_boundaries from hPa to nondimensional pressure,
+  and refuses sigma levels, a non-positive reference surface pressure and
+  Held-Suarez forcing (defined on sigma levels only) before any GPU work."""
+  from dinosaur_b200 import coordinate_systems
+  from dinosaur_b200 import held_suarez
+  from dinosaur_b200 import hybrid_coordinates as hc
+  from dinosaur_b200 import primitive_equations as pe
+  from dinosaur_b200 import sigma_coordinates as sc
+  from dinosaur_b200 import spherical_harmonic as sh
+  from dinosaur_b200 import time_integration
+  from dinosaur_b200 import units
+  g = sh.Grid.T21()
+  k = 6
+  lev = hc.HybridCoordinates.analytic_levels(k)
+  coords = coordinate_systems.CoordinateSystem(g, lev)
+  tref = np.full((k, 1, 1), 288.0)
+  orog = np.zeros(g.nodal_shape, np.float32)
+  eq = pe.PrimitiveEquationsHybrid(tref, orog, coords, units.SimUnits())
+  assert eq.p_s_ref == pytest.approx(units.nondim_pressure(101325.0))
+  np.testing.assert_allclose(
+      eq.nondim_levels.a_boundaries,
+      units.nondim_pressure(np.asarray(lev.a_boundaries, np.float64) * 100.0))
+  np.testing.assert_array_equal(eq.nondim_levels.b_boundaries, lev.b_boundaries)
+  with pytest.raises(ValueError):
+    pe.PrimitiveEquationsHybrid(tref, orog, coords, units.SimUnits(),
+                                reference_surface_pressure=0.0)
+  sigma_coords = coordinate_systems.CoordinateSystem(
+      g, sc.SigmaCoordinates.equidistant(k))
+  with pytest.raises(TypeError):
+    pe.PrimitiveEquationsHybrid(tref, orog, sigma_coords, units.SimUnits())
+  hs = held_suarez.HeldSuarezForcingSigma(sigma_coords, units.SimUnits(), tref)
+  with pytest.raises(NotImplementedError):
+    time_integration.compose_equations([eq, hs])
