@@ -11,9 +11,11 @@ orography, horizontal advection, virtual temperature) come from
 
 Parity pins: ``tests/golden/pe_hybrid_T21_L6.npz`` holds the reference's own
 PrimitiveEquationsHybrid outputs (explicit, implicit, implicit inverse, one
-filtered SIL3 step on 6 analytic levels; moist explicit terms with a tracer
-in ``pe_hybrid_moist_T21_L6.npz``), written by
-``tests/golden/make_golden.py``), checked in ``tests/test_oracle_golden.py``;
+filtered SIL3 step on 6 analytic levels; the same on 6 ECMWF-like levels
+whose top two layers are pure pressure in
+``pe_hybrid_ecmwf_like_T21_L6.npz``; moist explicit terms with a tracer in
+``pe_hybrid_moist_T21_L6.npz``), written by
+``tests/golden/make_golden.py`` and checked in ``tests/test_oracle_golden.py``;
 the reference test suite's sigma-like equivalence and implicit-inverse
 identity are checked in ``tests/test_hybrid_oracle.py``.
 """

@@ -187,6 +187,22 @@ def main(reference_root='/root/reference'):
         **pack('implicit', hyb_eq.implicit_terms(state)),
         **pack('inverse', hyb_eq.implicit_inverse(state, 0.05)),
         **pack('step1', hyb_step(state)))
+  # The same state on 6 ECMWF-like levels: the top two layers are pure
+  # pressure (b = 0 at both of their boundaries).
+  ecm_levels = hybrid_coordinates.HybridCoordinates.analytic_ecmwf_like(layers)
+  ecm_eq = primitive_equations.PrimitiveEquationsHybrid(
+      ref_temps, orography,
+      coordinate_systems.CoordinateSystem(horizontal=grid, vertical=ecm_levels),
+      physics_specs)
+  ecm_step = time_integration.step_with_filters(
+      time_integration.imex_rk_sil3(ecm_eq, dt),
+      [time_integration.exponential_step_filter(grid, dt)])
+  _save('pe_hybrid_ecmwf_like_T21_L6.npz',
+        a_boundaries=ecm_levels.a_boundaries, b_boundaries=ecm_levels.b_boundaries,
+        **pack('explicit', ecm_eq.explicit_terms(state)),
+        **pack('implicit', ecm_eq.implicit_terms(state)),
+        **pack('inverse', ecm_eq.implicit_inverse(state, 0.05)),
+        **pack('step1', ecm_step(state)))
 
   # -- digital filter initialisation (time_integration.py:645-712) ---------
   dfi_dt = dt

@@ -262,15 +262,19 @@ def test_digital_filter_initialization_matches_reference(pe_setup):
   assert_state_close(dfi(s), unpack(d, 'dfi'), atol=1e-10)
 
 
-def test_hybrid_terms_and_step_match_reference(pe_setup):
-  """PrimitiveEquationsHybrid on 6 analytic hybrid levels, same input state
-  (pe_hybrid_T21_L6.npz).  The reference differences its float32 reference
-  temperatures in float32 (get_temperature_implicit_weights_hybrid's
-  np.diff), 1.1e-7 of the implicit temperature term; hence 1e-6 for the
-  implicit terms, 1e-8 elsewhere (the step measures 1e-9)."""
+@pytest.mark.parametrize('fixture', ['pe_hybrid_T21_L6.npz',
+                                     'pe_hybrid_ecmwf_like_T21_L6.npz'])
+def test_hybrid_terms_and_step_match_reference(pe_setup, fixture):
+  """PrimitiveEquationsHybrid on 6 hybrid levels, same input state: the
+  analytic levels (pe_hybrid_T21_L6.npz) and ECMWF-like levels whose top two
+  layers are pure pressure, b = 0 (pe_hybrid_ecmwf_like_T21_L6.npz).  The
+  reference differences its float32 reference temperatures in float32
+  (get_temperature_implicit_weights_hybrid's np.diff), 1.1e-7 of the
+  implicit temperature term; hence 1e-6 for the implicit terms, 1e-8
+  elsewhere (the step measures 1e-9)."""
   from oracle import hybrid
   g0, grid, _, _ = pe_setup
-  g = load('pe_hybrid_T21_L6.npz')
+  g = load(fixture)
   eq = hybrid.PrimitiveEquationsHybrid(
       g0['ref_temps'], g0['orography'], grid,
       hybrid.HybridCoordinates(g['a_boundaries'], g['b_boundaries']), dycore.SimUnits())
