@@ -149,23 +149,22 @@ class ClockSampler:
 # CPU arms (oracle port of the reference's Real SHT)
 # ---------------------------------------------------------------------------
 
-def cpu_sht_sample(fields, seconds=10.0):
-  """Times the reference's einsum SHT pair (FP32 NumPy) on `fields` fields."""
+def cpu_sht_pair_fn(fields, seed=1):
+  """The reference's Real SHT pair in FP32 on the host: the oracle's
+  restatement of spherical_harmonic.py:262-280 in the reference's contraction
+  shape (one GEMM per m with the fields as N, the Fourier sums as one GEMM),
+  on all host threads.  Returns (pair, x)."""
   from oracle import sht as osht  # CPU baseline only
-  og = osht.Grid.TL255()
-  f, p, w = og.basis
-  f, p, w = f.astype(np.float32), p.astype(np.float32), w.astype(np.float32)
-  x = modal_input(fields, seed=1)
-  ft = np.ascontiguousarray(f.T)
-  pt = np.ascontiguousarray(np.swapaxes(p, -1, -2))
+  og = osht.Grid.TL255(compute_dtype=np.float32)
+  og._gemm_basis  # tables built outside the timed region
+  x = modal_input(fields, seed=seed)
+  return (lambda xx: og.to_modal(og.to_nodal(xx))), x
 
-  def pair(xx):
-    px = np.matmul(p, xx[..., None])[..., 0]            # 'mjl,...ml->...mj'
-    nodal = np.matmul(f, px)                            # 'im,...mj->...ij'
-    fwx = np.matmul(ft, w * nodal)                      # 'im,...ij->...mj'
-    return np.matmul(pt, fwx[..., None])[..., 0]        # 'mjl,...mj->...ml'
 
-  pair(x[:1])
+def cpu_sht_sample(fields=FIELDS, seconds=10.0):
+  """Median seconds per pair over `seconds` of repeated pairs (at least 2)."""
+  pair, x = cpu_sht_pair_fn(fields)
+  pair(x)
   times = []
   t_end = time.perf_counter() + seconds
   while time.perf_counter() < t_end or len(times) < 2:
@@ -175,42 +174,85 @@ def cpu_sht_sample(fields, seconds=10.0):
   return statistics.median(times), len(times)
 
 
-def cpu_baseline_entry(fields=4, seconds=10.0):
-  t, reps = cpu_sht_sample(fields, seconds)
-  return {'value': sht_flops(fields) / t / 1e12, 'unit': 'TFLOP/s',
-          'cores': os.cpu_count(), 'kind': 'port',
-          'sample': f'{fields} of {FIELDS} TL255 fields per pair, FP32 NumPy '
-                    f'einsums of the reference Real SHT, median of {reps} pairs'}
+def cpu_threads():
+  """Host threads the NumPy BLAS may use (the process's CPU affinity)."""
+  try:
+    return len(os.sched_getaffinity(0))
+  except AttributeError:
+    return os.cpu_count()
+
+
+def cpu_baseline_entry(seconds=10.0):
+  t, reps = cpu_sht_sample(FIELDS, seconds)
+  return {'value': sht_flops(FIELDS) / t / 1e12, 'unit': 'TFLOP/s',
+          'cores': cpu_threads(), 'kind': 'port', 'ms_per_pair': t * 1e3,
+          'sample': f'all {FIELDS} TL255 fields per pair; FP32 NumPy restatement of the '
+                    'reference Real SHT in its contraction shape (per-m GEMMs over all '
+                    f'fields, DFT as a GEMM); median of {reps} pairs (~{seconds:.0f} s)'}
+
+
+def cpu_pe_baseline(seconds=20.0):
+  """Primitive-equation steps/s of the FP64 NumPy restatement of the
+  reference's filtered imex_rk_sil3 step (time_integration.py:375-405 over
+  primitive_equations.py:1126-1458) on the host: T21 / 12 levels (the
+  one-day configuration, timed over its first steps) and one TL255 / 32-level
+  dry step."""
+  from oracle import dycore as od, sht as osht, states as ost  # CPU baseline only
+  out = {}
+  for name, grid_name, layers, dt_min, budget in (('T21_L12', 'T21', 12, 20, seconds / 2),
+                                                   ('TL255_L32_dry', 'TL255', 32, 6,
+                                                    seconds / 2)):
+    og = getattr(osht.Grid, grid_name)()
+    st, tref, orog, vert = ost.baroclinic_config(og, layers)
+    eq = od.PrimitiveEquationsSigma(tref, orog, og, vert, od.SimUnits())
+    dt = od.nondim_time(dt_min * 60.0)
+    step = od.step_with_filters(od.imex_rk_sil3(eq, dt),
+                                [od.exponential_step_filter(og, dt)])
+    # Warm-up outside the timed region: the tables and the implicit factors
+    # of the three SIL3 stages (the tableau's diagonal).
+    og._gemm_basis
+    a_im = od.SIL3['a_im']
+    for i in range(1, len(a_im) + 1):
+      eq.implicit_inverse(st, dt * a_im[i - 1][i])
+    n, t0 = 0, time.perf_counter()
+    while n < 1 or (time.perf_counter() - t0 < budget and n < 72):
+      st = step(st)
+      n += 1
+    sec = (time.perf_counter() - t0) / n
+    out[name] = {'steps_per_s': 1.0 / sec, 'ms_per_step': sec * 1e3, 'steps_timed': n,
+                 'cores': cpu_threads(), 'kind': 'port',
+                 'dtype': 'f64 (the oracle; the reference\'s float32 JAX path is not '
+                          'installed)'}
+  return out
 
 
 def run_reference(args):
   rank = int(os.environ.get('RANK', '0'))
   if rank != 0:
     return
-  fields = 8
+  pair, x = cpu_sht_pair_fn(FIELDS)
   for _ in range(args.warmup):
-    cpu_sht_sample(fields, seconds=0.0)
-  times = []
+    pair(x)
+  t0 = time.perf_counter()
   for _ in range(args.steps):
-    t, _ = cpu_sht_sample(fields, seconds=0.0)
-    times.append(t)
-  t = statistics.median(times)
-  value = sht_flops(fields) / t / 1e12
+    pair(x)
+  t = (time.perf_counter() - t0) / args.steps
+  value = sht_flops(FIELDS) / t / 1e12
   line = {
       'metric': 'SHT TFLOP/s (TL255 fwd+inv pair, 128 fields)',
       'value': value, 'unit': 'TFLOP/s', 'n_gpus': args.gpus,
       'steps': args.steps, 'warmup': args.warmup,
-      'ms_per_step': t * 1e3 * FIELDS / fields,
+      'ms_per_step': t * 1e3,
       'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
       'dtype': 'f32', 'data': 'synthetic',
-      'config': {'workload': 'SHT pair TL255 x 128 fields (CPU sample)',
-                 'grid': 'TL255', 'fields': FIELDS, 'sample_fields': fields},
+      'config': {'workload': 'SHT pair TL255 x 128 fields', 'grid': 'TL255',
+                 'fields': FIELDS},
       'impl': 'reference',
       'cpu_baseline': {'value': value, 'unit': 'TFLOP/s',
-                       'cores': os.cpu_count(), 'kind': 'port',
-                       'sample': f'{fields} fields per pair; NumPy FP32 '
-                                 'restatement of the reference Real SHT '
-                                 '(JAX is not installed)'},
+                       'cores': cpu_threads(), 'kind': 'port',
+                       'sample': f'all {FIELDS} fields per pair, {args.steps} timed pairs; '
+                                 'FP32 NumPy restatement of the reference Real SHT in '
+                                 'its contraction shape (JAX is not installed)'},
       'e2e': {'value': value, 'unit': 'TFLOP/s', 'h2d_bytes_per_step': 0,
               'd2h_bytes_per_step': 0},
   }
@@ -370,18 +412,14 @@ def time_phases(torch, plan, x, name, reps):
   return phase_ms
 
 
-def compute_peaks(torch, measured):
-  """Compute-roofline denominators measured on this device: the FP32 FMA rate
-  (the library's microbenchmark; the SIMT Legendre's bound) and a cuBLAS TF32
-  GEMM (the split-TF32 form's), best of three; BF16 and HBM from the
-  measured-peaks file."""
-  from dinosaur_b200 import _lib
-  import ctypes
-  fma = []
-  for _ in range(3):
-    v = ctypes.c_double(0.0)
-    _lib.check(_lib.lib().dino_measure_fp32_fma_peak(1 << 14, ctypes.byref(v)))
-    fma.append(v.value)
+def compute_peaks(torch, measured, sm_mhz=None):
+  """Compute-roofline denominators: the nominal FP32 FMA rate at the SM clock
+  (148 SMs x 128 lanes x 2 flops; the SIMT Legendre's bound), a cuBLAS TF32
+  GEMM measured here (the split-TF32 form's), best of three; BF16 and HBM
+  from the measured-peaks file."""
+  prop = torch.cuda.get_device_properties(torch.cuda.current_device())
+  mhz = sm_mhz or measured.get('sm_max_mhz') or 1965.0
+  fp32 = prop.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
   n = 8192
   a = torch.randn(n, n, device='cuda')
   b = torch.randn(n, n, device='cuda')
@@ -403,10 +441,10 @@ def compute_peaks(torch, measured):
   finally:
     torch.backends.cuda.matmul.allow_tf32 = old
   del a, b, c
-  return {'fp32_fma_tflops': max(fma), 'tf32_gemm_tflops': max(tf32),
+  return {'fp32_fma_tflops': fp32, 'tf32_gemm_tflops': max(tf32),
           'bf16_gemm_tflops': measured.get('bf16_tflops'),
           'hbm_gbs': measured.get('hbm_gbs'),
-          'how': 'fp32: dino_measure_fp32_fma_peak (2048 threads x 8 FMA chains per SM); '
+          'how': f'fp32: nominal, SMs x 128 lanes x 2 x {mhz:.0f} MHz; '
                  'tf32: cuBLAS 8192^3 GEMM via torch, allow_tf32; bf16 / hbm: '
                  'MEASURED_PEAKS.json'}
 
@@ -615,7 +653,7 @@ def run_ours(args):
   if not args.no_extra and world == 1:
     # Every Legendre form at TL255 and T85 with its rooflines; the other
     # forms' TL255 pairs are also listed as sht_<form>.
-    extra['peaks'] = compute_peaks(torch, peaks)
+    extra['peaks'] = compute_peaks(torch, peaks, clocks.get('sm_mhz'))
     extra['legendre_forms'] = legendre_forms(torch, args, extra['peaks'])
     for other in [f for f in FORMS if f != args.precision]:
       e = extra['legendre_forms']['TL255'][other]
@@ -658,6 +696,8 @@ def run_ours(args):
     }
     if world == 1 and not args.no_cpu_baseline:
       line['cpu_baseline'] = cpu_baseline_entry()
+      if extra:
+        extra['cpu_pe'] = cpu_pe_baseline()
     if extra:
       line['extra'] = extra
     print(json.dumps(line), flush=True)
@@ -869,6 +909,68 @@ def small_and_gradient_cases(torch):
   return out
 
 
+def run_pe_profile(args):
+  """Eager (no CUDA graph) filtered SIL3 steps of the primitive equations, so
+  that a kernel profiler sees every launch: seeded small random states on
+  the chosen grid, levels and members.  Prints the mean step time."""
+  import torch
+  from dinosaur_b200 import coordinate_systems, held_suarez, hybrid_coordinates
+  from dinosaur_b200 import primitive_equations as pe
+  from dinosaur_b200 import sigma_coordinates, spherical_harmonic as sh
+  from dinosaur_b200 import time_integration as ti, units
+  impl = functools.partial(sh.CudaSphericalHarmonics, precision=args.precision)
+  g = getattr(sh.Grid, args.pe_grid)(spherical_harmonics_impl=impl)
+  layers, members = args.pe_layers, args.pe_members
+  vert = (hybrid_coordinates.HybridCoordinates.analytic_levels(layers) if args.pe_hybrid
+          else sigma_coordinates.SigmaCoordinates.equidistant(layers))
+  coords = coordinate_systems.CoordinateSystem(g, vert)
+  ps = units.SimUnits()
+  hs = args.pe_held_suarez
+  tref = np.full(layers, 285.0) if hs else np.linspace(220.0, 288.0, layers)
+  eq_cls = pe.PrimitiveEquationsHybrid if args.pe_hybrid else pe.PrimitiveEquationsSigma
+  eq = eq_cls(tref, np.zeros(g.modal_shape, np.float32), coords, ps,
+              humidity_key='specific_humidity' if args.pe_moist else None)
+  if hs:
+    eq = ti.compose_equations([eq, held_suarez.HeldSuarezForcingSigma(coords, ps, tref)])
+  dt = units.nondim_time(args.pe_dt_minutes * 60.0)
+  flt = (ti.exponential_step_filter(g, dt, tau=0.0087504, order=1.5, cutoff=0.8) if hs
+         else ti.exponential_step_filter(g, dt))
+  step = ti.step_with_filters(ti.imex_rk_sil3(eq, dt), [flt])
+  rng = np.random.default_rng(0)
+  lead = (members,) if members > 1 else ()
+  _, l = g.modal_mesh
+  scale = g.mask / (l + 1.0) ** 2
+  dev = lambda a: torch.as_tensor(np.asarray(a, np.float32), device='cuda')
+  noise = lambda shp, a=1e-4: dev(a * rng.standard_normal(shp) * scale)
+  shape = lead + (layers,) + g.modal_shape
+  tracers = {}
+  if args.pe_moist:
+    const = np.zeros(shape, np.float32)
+    const[..., 0, 0] = 2.0 * np.sqrt(np.pi)  # the constant field 1
+    tracers = {'specific_humidity': dev(5e-3 * const) + noise(shape, 1e-6),
+               'tracer_a': dev(const) + noise(shape), 'tracer_b': dev(const) + noise(shape)}
+  lnps = noise(lead + (1,) + g.modal_shape)
+  if args.pe_hybrid:
+    # A physical surface pressure (1e5 Pa) as the l = 0 term.
+    lnps[..., 0, 0] += float(np.log(units.nondim_pressure(1e5)) * 2.0 * np.sqrt(np.pi))
+  state = pe.State(noise(shape), noise(shape), noise(shape), lnps, tracers=tracers)
+  eng = eq.engine(state)
+  buf = eng.pack(state)
+  eng.step_(buf, dt, step.filter_scaling, max(1, args.warmup), graph=False)
+  torch.cuda.synchronize()
+  e0 = torch.cuda.Event(enable_timing=True)
+  e1 = torch.cuda.Event(enable_timing=True)
+  e0.record()
+  eng.step_(buf, dt, step.filter_scaling, args.steps, graph=False)
+  e1.record()
+  torch.cuda.synchronize()
+  print(json.dumps({'pe_profile': {
+      'grid': args.pe_grid, 'layers': layers, 'members': members, 'held_suarez': hs,
+      'moist': args.pe_moist, 'hybrid': args.pe_hybrid, 'precision': args.precision,
+      'us_per_step_eager': e0.elapsed_time(e1) / args.steps * 1e3,
+      'finite': bool(torch.isfinite(buf).all())}}), flush=True)
+
+
 def main():
   ap = argparse.ArgumentParser()
   ap.add_argument('--gpus', type=int, default=1)
@@ -885,7 +987,21 @@ def main():
                   choices=['legendre_inverse', 'fourier_inverse', 'fourier_forward',
                            'legendre_forward'],
                   help='only one transform phase over all fields (for ncu captures)')
+  pe_grp = ap.add_argument_group(
+      'primitive-equation step profiling (eager launches, for a kernel profiler)')
+  pe_grp.add_argument('--pe-grid', default=None, help='e.g. T42 or TL255')
+  pe_grp.add_argument('--pe-layers', type=int, default=24)
+  pe_grp.add_argument('--pe-members', type=int, default=1)
+  pe_grp.add_argument('--pe-held-suarez', action='store_true')
+  pe_grp.add_argument('--pe-moist', action='store_true',
+                      help='specific humidity and two passive tracers')
+  pe_grp.add_argument('--pe-hybrid', action='store_true',
+                      help='analytic hybrid sigma-pressure levels')
+  pe_grp.add_argument('--pe-dt-minutes', type=float, default=15.0)
   args = ap.parse_args()
+  if args.pe_grid:
+    run_pe_profile(args)
+    return
   if args.warmup < 3:
     args.warmup = 3
   if args.impl == 'reference':

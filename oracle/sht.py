@@ -162,6 +162,9 @@ class Grid:
   latitude_nodes: int = 0
   latitude_spacing: str = 'gauss'
   radius: float = 1.0
+  # Arithmetic type of the transforms (float64 for the oracle; the CPU
+  # baseline times the same contractions in float32).
+  compute_dtype: type = np.float64
 
   @classmethod
   def construct(cls, max_wavenumber: int, gaussian_nodes: int, **kw) -> Grid:
@@ -256,20 +259,50 @@ class Grid:
     p = np.repeat(p, 2, axis=0)[1:]
     return f, p, wf * wp
 
+  @functools.cached_property
+  def _gemm_basis(self):
+    """The basis in the compute dtype, laid out for the per-m GEMMs."""
+    f, p, w = self.basis
+    dt = self.compute_dtype
+    if dt != np.float64:
+      # XLA's CPU backend flushes subnormals to zero; the Legendre values
+      # near the poles at large m would otherwise be subnormal in float32
+      # and slow every product that touches them.
+      p = np.where(np.abs(p) < np.finfo(dt).tiny, 0.0, p)
+    return (np.ascontiguousarray(f, dt), np.ascontiguousarray(f.T, dt),
+            np.ascontiguousarray(p, dt),
+            np.ascontiguousarray(np.swapaxes(p, -1, -2), dt), w.astype(dt))
+
   # -- transforms -------------------------------------------------------
+  # The reference contracts with einsum over all leading (field) axes at
+  # once, which XLA lowers to one GEMM per m with the fields as the GEMM's N
+  # dimension.  The same shape here: fields are moved to the last axis, so
+  # each contraction is a batched matmul over m of (J x L) @ (L x F) and the
+  # Fourier sums one (I x M) @ (M x J F) product.
   def to_nodal(self, x):
     """Inverse transform (spherical_harmonic.py:262-269)."""
-    f, p, _ = self.basis
-    x = np.asarray(x, dtype=np.float64)
-    px = np.matmul(p, x[..., None])[..., 0]          # 'mjl,...ml->...mj'
-    return np.matmul(f, px)                          # 'im,...mj->...ij'
+    f, _, p, _, _ = self._gemm_basis
+    x = np.asarray(x, dtype=self.compute_dtype)
+    lead = x.shape[:-2]
+    m_, l_ = x.shape[-2:]
+    xf = x.reshape((-1, m_, l_)).transpose(1, 2, 0)          # (M, L, F)
+    px = np.matmul(p, xf)                                    # 'mjl,...ml->...mj'
+    if self.compute_dtype != np.float64:
+      px[np.abs(px) < np.finfo(px.dtype).tiny] = 0.0         # flush subnormals
+    j_ = px.shape[1]
+    z = (f @ px.reshape(m_, -1)).reshape(f.shape[0], j_, -1)  # 'im,...mj->...ij'
+    return np.moveaxis(z, -1, 0).reshape(lead + z.shape[:2])
 
   def to_modal(self, z):
     """Forward transform (spherical_harmonic.py:271-280)."""
-    f, p, w = self.basis
-    z = np.asarray(z, dtype=np.float64)
-    fwx = np.matmul(f.T, w * z)                      # 'im,...ij->...mj'
-    return np.matmul(np.swapaxes(p, -1, -2), fwx[..., None])[..., 0]
+    _, ft, _, pt, w = self._gemm_basis
+    z = np.asarray(z, dtype=self.compute_dtype)
+    lead = z.shape[:-2]
+    i_, j_ = z.shape[-2:]
+    zf = (w * z).reshape((-1, i_, j_)).transpose(1, 2, 0)     # (I, J, F)
+    fwx = (ft @ zf.reshape(i_, -1)).reshape(ft.shape[0], j_, -1)  # 'im,...ij->...mj'
+    out = np.matmul(pt, fwx)                                 # 'mjl,...mj->...ml'
+    return np.moveaxis(out, -1, 0).reshape(lead + out.shape[:2])
 
   # -- operators --------------------------------------------------------
   def laplacian(self, x):
