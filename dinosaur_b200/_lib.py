@@ -153,7 +153,6 @@ SIGNATURES = {
                                                     ctypes.c_double, _vp]),
     'dino_pe_step_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double,
                                         _DP, _vp]),
-    'dino_measure_fp32_fma_peak': (ctypes.c_int, [_i32, _DP]),
 }
 
 

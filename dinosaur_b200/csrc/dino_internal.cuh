@@ -6,6 +6,7 @@
 
 #include <cstdio>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -49,6 +50,30 @@ struct Status {
 
 // Checks the launch status of the last kernel (does not synchronize).
 int check_launch(const char* what);
+
+// Runs a set-up step (returning a status) once per device and process, with
+// that device current.  Kernel attributes such as the dynamic shared-memory
+// limit belong to the device's context, so every device that launches the
+// kernel needs its own call.  Safe to call from several host threads.
+class PerDeviceOnce {
+ public:
+  template <class F>
+  int run(F&& fn) {
+    int dev = 0;
+    DINO_CHECK_CUDA(cudaGetDevice(&dev));
+    DINO_REQUIRE(dev >= 0 && dev < 64, DINO_ERR_ARG, "device index out of range");
+    const uint64_t bit = 1ull << dev;
+    std::lock_guard<std::mutex> lock(mu_);
+    if (done_ & bit) return DINO_OK;
+    DINO_TRY(fn());
+    done_ |= bit;
+    return DINO_OK;
+  }
+
+ private:
+  std::mutex mu_;
+  uint64_t done_ = 0;
+};
 
 // ---------------------------------------------------------------------------
 // Field segments: a batch of fields gathered from up to kMaxSegs contiguous

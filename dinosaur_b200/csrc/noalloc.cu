@@ -29,10 +29,15 @@ std::mutex g_scratch_mutex;
 float* g_scratch_ptr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
-int scratch_for_current_device(float** out) {
+// per device, with that device current).  The plan's tables live on the
+// plan's device, so that device must be the current one.
+int scratch_for_current_device(const dino_plan* p, float** out) {
   int dev = 0;
   DINO_CHECK_CUDA(cudaGetDevice(&dev));
+  DINO_REQUIRE(dev == p->device, DINO_ERR_ARG,
+               "dino_sht_inverse_noalloc: the plan belongs to device " +
+                   std::to_string(p->device) + " but device " + std::to_string(dev) +
+                   " is current");
   DINO_REQUIRE(dev >= 0 && dev < kMaxDevices, DINO_ERR_UNSUPPORTED,
                "dino_sht_inverse_noalloc: device index out of range");
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
@@ -58,9 +63,11 @@ using namespace dino;
 extern "C" int dino_sht_inverse_noalloc(dino_plan* p, const float* modal,
                                         float* nodal, int32_t nf,
                                         void* stream) {
-  DINO_REQUIRE(p && modal && nodal, DINO_ERR_ARG,
-               "dino_sht_inverse_noalloc: null argument");
+  DINO_REQUIRE(p, DINO_ERR_ARG, "dino_sht_inverse_noalloc: null plan");
   DINO_REQUIRE(nf >= 0, DINO_ERR_SHAPE, "nfields must be >= 0");
+  if (nf == 0) return DINO_OK;  // an empty batch is a no-op; buffers may be NULL
+  DINO_REQUIRE(modal && nodal, DINO_ERR_ARG,
+               "dino_sht_inverse_noalloc: null buffer");
   const long long need = (long long)nf * p->M * p->J;
   if (need > (long long)DINO_NOALLOC_SCRATCH_FLOATS) {
     set_error("dino_sht_inverse_noalloc: nfields * M * J = " +
@@ -72,9 +79,8 @@ extern "C" int dino_sht_inverse_noalloc(dino_plan* p, const float* modal,
               " fields per call");
     return DINO_ERR_SHAPE;
   }
-  if (nf == 0) return DINO_OK;
   float* scratch = nullptr;
-  DINO_TRY(scratch_for_current_device(&scratch));
+  DINO_TRY(scratch_for_current_device(p, &scratch));
   cudaStream_t st = (cudaStream_t)stream;
   DINO_TRY(legendre_inverse_fp32(p, one_seg(modal, nf), scratch, nf, st));
   return fourier_inverse(p, scratch, nodal, nf, false, st);

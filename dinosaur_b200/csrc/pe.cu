@@ -1892,22 +1892,22 @@ static int apply_attr() {
   return DINO_OK;
 }
 
-// Sets the shared-memory attribute of every instantiation once (kept out of
-// graph capture).
+// Sets the shared-memory attribute of every instantiation once per device
+// (kept out of graph capture).
 static int prepare_apply() {
-  static bool done = false;
-  if (done) return DINO_OK;
-  DINO_TRY(apply_attr<1>());
-  DINO_TRY(apply_attr<2>());
-  DINO_TRY(apply_attr<3>());
-  DINO_TRY(apply_attr<4>());
-  DINO_TRY(apply_attr<5>());
-  DINO_TRY(apply_attr<6>());
-  DINO_TRY(apply_attr<7>());
-  DINO_TRY(apply_attr<8>());
-  DINO_TRY(apply_attr<9>());
-  done = true;
-  return DINO_OK;
+  static PerDeviceOnce once;
+  return once.run([] {
+    DINO_TRY(apply_attr<1>());
+    DINO_TRY(apply_attr<2>());
+    DINO_TRY(apply_attr<3>());
+    DINO_TRY(apply_attr<4>());
+    DINO_TRY(apply_attr<5>());
+    DINO_TRY(apply_attr<6>());
+    DINO_TRY(apply_attr<7>());
+    DINO_TRY(apply_attr<8>());
+    DINO_TRY(apply_attr<9>());
+    return DINO_OK;
+  });
 }
 
 template <int TR>

@@ -801,16 +801,17 @@ __global__ void dft_forward_kernel(const float* __restrict__ x,
 
 template <int N>
 static int configure_rfft() {
-  // Kernel attributes are set once per process, outside any stream capture.
-  static bool configured = false;
-  if (configured) return DINO_OK;
-  const int smem = (int)fft_smem_bytes<N>();
-  DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_inverse_kernel<N>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_forward_kernel<N>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  configured = true;
-  return DINO_OK;
+  // Kernel attributes are set once per device, outside any stream capture
+  // (sht_prepare runs this at plan creation on the plan's device).
+  static PerDeviceOnce once;
+  return once.run([] {
+    const int smem = (int)fft_smem_bytes<N>();
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_inverse_kernel<N>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    DINO_CHECK_CUDA(cudaFuncSetAttribute(rfft_forward_kernel<N>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return DINO_OK;
+  });
 }
 
 template <int N>

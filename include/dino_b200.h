@@ -131,7 +131,9 @@ DINO_API int dino_plan_status(dino_plan* plan);
  * It is meant for callers that may not allocate device memory at call time,
  * for example a handler inside a framework that owns the GPU's memory pool,
  * or a loop that cannot afford cudaMalloc's implicit device synchronization.
- * The plan must already exist (its tables are read, not written).  Limits and
+ * The plan must already exist (its tables are read, not written) and its
+ * device must be the current one (otherwise DINO_ERR_ARG).  nfields = 0 is a
+ * no-op with NULL buffers allowed.  Limits and
  * rules: nfields * M * J <= DINO_NOALLOC_SCRATCH_FLOATS, otherwise
  * DINO_ERR_SHAPE; the Legendre contraction always runs in FP32; the first
  * call on a device looks the array up (cudaGetSymbolAddress) and sets kernel
@@ -305,13 +307,6 @@ DINO_API int dino_pe_implicit_inverse_vjp(dino_pe* pe, const float* d_out_ct,
 DINO_API int dino_pe_step_vjp(dino_pe* pe, const float* d_state,
                               const float* d_out_ct, float* d_in_ct, double dt,
                               const double* host_filter, void* stream);
-
-/* Measures the device's peak FP32 FMA rate, the compute roofline of the
- * plain FP32 Legendre contraction: every SM runs 2048 threads of 8
- * independent FMA chains for `iters` iterations, timed with CUDA events
- * after one warm-up launch; *tflops = 2 x FMAs / time.  Synchronizes the
- * device.  No counterpart in the reference. */
-DINO_API int dino_measure_fp32_fma_peak(int32_t iters, double* tflops);
 
 #ifdef __cplusplus
 }

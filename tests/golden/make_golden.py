@@ -1,9 +1,9 @@
 """Generates the golden fixtures in this directory from the reference itself.
 
-Run in a container where neuralgcm/dinosaur 1.3.6 is checked out (default
-``/root/reference``)::
+Run where neuralgcm/dinosaur 1.3.6 is checked out, naming its root as the
+argument or in the ``DINOSAUR_REFERENCE_ROOT`` environment variable::
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 ``jax``, ``tree_math`` and ``pint`` are not installed there, so
 ``_standins.py`` provides NumPy stand-ins; the reference modules then run
@@ -31,7 +31,11 @@ def _save(name, **arrays):
   print(f'wrote {name} ({size / 1024:.1f} KiB)')
 
 
-def main(reference_root='/root/reference'):
+def main(reference_root=None):
+  reference_root = reference_root or os.environ.get('DINOSAUR_REFERENCE_ROOT')
+  if not reference_root:
+    raise SystemExit('usage: make_golden.py REFERENCE_ROOT '
+                     '(or set DINOSAUR_REFERENCE_ROOT)')
   _standins.install(reference_root)
   from dinosaur import associated_legendre
   from dinosaur import coordinate_systems

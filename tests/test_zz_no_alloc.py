@@ -56,3 +56,13 @@ def test_noalloc_rejects_batches_beyond_the_fixed_scratch():
   rc = _noalloc(plan, x, out)
   assert rc == _lib.DINO_ERR_SHAPE
   assert 'exceeds the fixed scratch' in _lib.last_error()
+
+
+def test_noalloc_empty_batch_is_a_no_op_with_null_buffers():
+  plan = sh.Grid.T21().plan
+  rc = _lib.lib().dino_sht_inverse_noalloc(plan.handle, None, None, 0,
+                                           sh.stream_handle())
+  assert rc == _lib.DINO_OK
+  rc = _lib.lib().dino_sht_inverse_noalloc(plan.handle, None, None, 1,
+                                           sh.stream_handle())
+  assert rc == _lib.DINO_ERR_ARG
