@@ -122,7 +122,10 @@ class HybridCoordinates:
     return len(self.a_boundaries) - 1
 
   def _expand(self, x, surface_pressure):
-    nd = np.ndim(surface_pressure)
+    # One trailing axis per non-singleton axis of the surface pressure, as the
+    # reference does (hybrid_coordinates.py:443-462): a (1, lon, lat) surface
+    # pressure gives (levels, lon, lat) results.
+    nd = sum(1 for s in np.shape(surface_pressure) if s > 1)
     return np.reshape(x, x.shape + (1,) * nd)
 
   def pressure_boundaries(self, surface_pressure):

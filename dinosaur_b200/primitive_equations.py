@@ -104,51 +104,72 @@ def validate_state_shape(state: State,
 
 
 def get_sigma_ratios(coordinates: sigma_coordinates.SigmaCoordinates):
-  """primitive_equations.py:283-303."""
-  alpha = np.diff(np.log(coordinates.centers), append=0) / 2
-  alpha[-1] = -np.log(coordinates.centers[-1])
+  """Half log-sigma increments between level centres (primitive_equations.py:283-303).
+
+  alpha_k = (ln sigma_{k+1} - ln sigma_k) / 2 for k < K - 1 and
+  alpha_{K-1} = -ln sigma_{K-1}.  As in the reference, the logarithms are
+  taken in the level centres' dtype (float32 for equidistant levels) and
+  differenced in float64.
+  """
+  log_sigma = np.log(coordinates.centers)
+  alpha = np.empty(log_sigma.shape, np.float64)
+  alpha[:-1] = 0.5 * (log_sigma[1:].astype(np.float64) - log_sigma[:-1])
+  alpha[-1] = -log_sigma[-1]
   return alpha
 
 
 def get_geopotential_weights_sigma(coordinates, ideal_gas_constant):
-  """G (primitive_equations.py:306-338)."""
+  """G of the hydrostatic geopotential, Phi = Phi_s + G T (primitive_equations.py:306-338).
+
+  Integrating d Phi = -R T d ln sigma upwards from the surface with
+  midpoint weights gives, for level r and temperature level c:
+    G[r, c] = R alpha_r                  (c = r)
+    G[r, c] = R (alpha_c + alpha_{c-1})  (c > r, the levels below r)
+    G[r, c] = 0                          (c < r).
+  """
   alpha = get_sigma_ratios(coordinates)
   k = coordinates.layers
-  weights = np.zeros([k, k])
-  for j in range(k):
-    weights[j, j] = alpha[j]
-    for kk in range(j + 1, k):
-      weights[j, kk] = alpha[kk] + alpha[kk - 1]
+  r, c = np.indices((k, k))
+  pair = alpha[c] + alpha[np.maximum(c - 1, 0)]
+  weights = np.where(c == r, alpha[c], np.where(c > r, pair, 0.0))
   return ideal_gas_constant * weights
 
 
 def get_temperature_implicit_weights_sigma(coordinates, reference_temperature,
                                            kappa):
-  """H (primitive_equations.py:419-502)."""
-  reference_temperature = np.asarray(reference_temperature)
-  if (reference_temperature.ndim != 1
-      or reference_temperature.shape[-1] != coordinates.layers):
+  """H of the linearised temperature tendency, dT/dt = -H div (primitive_equations.py:419-502).
+
+  Durran (2010) section 8.6.5: with the lower-triangular indicator
+  [c <= r], the interface sigma_{r+1/2} = sum_{i <= r} dsigma_i and the
+  centred reference-temperature gradient g_r = (T_{r+1} - T_r) /
+  (dsigma_r + dsigma_{r+1}) (g_{K-1} = 0), entry (r, c) is dsigma_c times
+    kappa T_r / dsigma_r (alpha_r [c <= r] + alpha_{r-1} [c <= r - 1])
+    - g_r ([c <= r] - sigma_{r+1/2}) - g_{r-1} ([c <= r - 1] - sigma_{r-1/2}),
+  the terms with index r - 1 absent on the top level.  The interface sums
+  and the thickness pairs are formed in the thicknesses' dtype, as the
+  reference does.
+  """
+  t_ref = np.asarray(reference_temperature)
+  k = coordinates.layers
+  if t_ref.ndim != 1 or t_ref.shape[-1] != k:
     raise ValueError(
         '`reference_temp` must be a vector of length `coordinates.layers`; '
-        f'got shape {reference_temperature.shape} and '
-        f'{coordinates.layers} layers.')
-  k = coordinates.layers
-  p = np.tril(np.ones([k, k]))
-  alpha = get_sigma_ratios(coordinates)[..., None]
-  p_alpha = p * alpha
-  p_alpha_shifted = np.roll(p_alpha, 1, axis=0)
-  p_alpha_shifted[0] = 0
-  h0 = (kappa * reference_temperature[..., None] * (p_alpha + p_alpha_shifted)
-        / coordinates.layer_thickness[..., None])
-  temp_diff = np.diff(reference_temperature)
-  thickness_sum = coordinates.layer_thickness[:-1] + coordinates.layer_thickness[1:]
-  k0 = np.concatenate((temp_diff / thickness_sum, [0]), axis=0)[..., None]
-  thickness_cumulative = np.cumsum(coordinates.layer_thickness)[..., None]
-  k1 = p - thickness_cumulative
-  kk = k0 * k1
-  k_shifted = np.roll(kk, 1, axis=0)
-  k_shifted[0] = 0
-  return (h0 - kk - k_shifted) * coordinates.layer_thickness
+        f'got shape {t_ref.shape} and {k} layers.')
+  dsigma = coordinates.layer_thickness
+  alpha = get_sigma_ratios(coordinates)
+  interface = np.cumsum(dsigma)                   # sigma_{r+1/2}
+  grad = np.zeros(k)
+  grad[:-1] = np.diff(t_ref) / (dsigma[:-1] + dsigma[1:])
+  r, c = np.indices((k, k))
+  on = (c <= r).astype(np.float64)                # [c <= r]
+  has_above = r >= 1
+  ra = np.maximum(r - 1, 0)                       # index of the level above
+  on_above = np.where(has_above, (c <= r - 1), 0.0)
+  adiabatic = kappa * t_ref[r] * (alpha[r] * on + np.where(has_above, alpha[ra], 0.0)
+                                  * on_above) / dsigma[r]
+  advection = (grad[r] * (on - interface[r])
+               + np.where(has_above, grad[ra] * (on_above - interface[ra]), 0.0))
+  return (adiabatic - advection) * dsigma[c]
 
 
 def truncated_modal_orography(orography, coords, wavenumbers_to_clip: int = 1):

@@ -82,6 +82,23 @@ def test_package_levels_match_oracle():
     hc.HybridCoordinates(np.zeros(3), np.zeros(4))
 
 
+def test_package_level_pressures_broadcast_like_the_reference():
+  # hybrid_coordinates.py:443-462: one new axis per non-singleton axis of the
+  # surface pressure, so a (1, lon, lat) surface pressure gives
+  # (levels, lon, lat) boundaries, centres and thicknesses.
+  from dinosaur_b200 import hybrid_coordinates as hc
+  lev = hc.HybridCoordinates.analytic_levels(6)
+  ps = np.random.default_rng(3).uniform(90.0, 110.0, (1, 8, 4))
+  bounds = lev.pressure_boundaries(ps)
+  assert bounds.shape == (7, 8, 4)
+  np.testing.assert_allclose(
+      bounds, lev.a_boundaries[:, None, None] + lev.b_boundaries[:, None, None] * ps[0])
+  assert lev.pressure_centers(ps).shape == (6, 8, 4)
+  np.testing.assert_allclose(lev.layer_thickness(ps), np.diff(bounds, axis=0))
+  assert lev.pressure_boundaries(100.0).shape == (7,)
+  assert lev.layer_thickness(ps[0]).shape == (6, 8, 4)
+
+
 @pytest.mark.parametrize('levels', ['analytic', 'sigma_like', 'ecmwf_like'])
 def test_package_hybrid_matrices_match_oracle(levels):
   """The FP64 host matrices that the CUDA engine's implicit operators are
