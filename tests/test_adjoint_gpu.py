@@ -16,10 +16,6 @@ dino_pe_implicit_inverse_vjp) via the torch.autograd wrappers.  Tolerances:
   the test).
 """
 
-import concurrent.futures
-import multiprocessing
-import os
-
 import numpy as np
 import pytest
 import torch
@@ -28,6 +24,7 @@ from oracle import dycore as od
 from oracle import sht as osht
 from oracle import states as ost
 
+import config_cases
 import oracle_fd
 
 pytestmark = pytest.mark.gpu
@@ -198,9 +195,7 @@ def test_rollout_gradient_t42_l20_24_steps():
     v = random_tree(og, st0, rng)
     norm = np.sqrt(tree_dot(v, v))
     dirs.append(od.tree_map(lambda x, n=norm: x / n, v))
-  ctx = multiprocessing.get_context('spawn')
-  workers = max(1, min(8, os.cpu_count() or 1))
-  with concurrent.futures.ProcessPoolExecutor(workers, mp_context=ctx) as pool:
+  with config_cases.oracle_pool(8) as pool:
     futs = [pool.submit(oracle_fd.rollout_jvp_fd, grid_name, layers, dt,
                         n_steps, st0, target, v, eps) for v in dirs]
     # GPU gradient while the oracle runs.
