@@ -37,6 +37,12 @@ class DinoError(RuntimeError):
     self.code = code
 
 
+class DinoNonFiniteError(DinoError, AssertionError):
+  """DINO_ERR_NAN: a non-finite or singular implicit operator.  Also an
+  AssertionError, the exception the reference raises there
+  (primitive_equations.py:1296 asserts that the inverse has no NaN)."""
+
+
 class GridDesc(ctypes.Structure):
   _fields_ = [
       ('longitude_wavenumbers', ctypes.c_int32),
@@ -119,6 +125,7 @@ SIGNATURES = {
     'dino_plan_nodes': (ctypes.c_int, [_vp, _DP, _DP]),
     'dino_plan_legendre_column': (ctypes.c_int, [_vp, _i32, _i32, _DP]),
     'dino_plan_status': (ctypes.c_int, [_vp]),
+    'dino_plan_check_wait_timeout': (ctypes.c_int, [_vp, ctypes.c_int64, _vp]),
     'dino_sht_inverse': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_inverse_noalloc': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
     'dino_sht_forward': (ctypes.c_int, [_vp, _vp, _vp, _i32, _vp]),
@@ -151,6 +158,8 @@ SIGNATURES = {
     'dino_pe_implicit_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     'dino_pe_implicit_inverse_vjp': (ctypes.c_int, [_vp, _vp, _vp,
                                                     ctypes.c_double, _vp]),
+    'dino_pe_trajectory': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32, _i32,
+                                          _i32, _vp, _vp]),
     'dino_pe_step_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double,
                                         _DP, _vp]),
 }
@@ -190,6 +199,8 @@ def check(status: int, what: str = ''):
     raise ValueError(msg)
   if status == DINO_ERR_UNSUPPORTED:
     raise NotImplementedError(msg)
+  if status == DINO_ERR_NAN:
+    raise DinoNonFiniteError(status, msg)
   raise DinoError(status, msg)
 
 

@@ -202,15 +202,17 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for the phase with the given parity; gives up after kWaitLimitNs,
-// records `code` in *err and returns false.
+// Waits for the phase with the given parity; gives up after limit_ns
+// (kWaitLimitNs in the contraction kernels), records `code` in *err and
+// returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
-                                          int* err, int code) {
+                                          int* err, int code,
+                                          unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (true) {
     if (mbar_test(bar, parity)) return true;
-    if (global_ns() - t0 > kWaitLimitNs) {
+    if (global_ns() - t0 > limit_ns) {
       atomicCAS(err, 0, code);
       return false;
     }
@@ -1255,15 +1257,32 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
   return check_launch("legendre_tc_forward");
 }
 
+// Reads (and clears) the plan's device error flag.
 int tc_status(dino_plan* p) {
   if (!p->tc) return DINO_OK;
   int err = 0;
   DINO_CHECK_CUDA(cudaMemcpy(&err, p->tc->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
+    DINO_CHECK_CUDA(cudaMemset(p->tc->d_err, 0, sizeof(int)));
     set_error("a tensor-core wait gave up (code " + std::to_string(err) + ")");
     return DINO_ERR_TIMEOUT;
   }
   return DINO_OK;
+}
+
+// One CTA whose thread 0 waits, through the contraction kernels' bounded
+// wait, on an mbarrier that nothing ever completes: the wait gives up after
+// limit_ns and records kWaitCheckCode in *err.  The failure path of a
+// stalled pipeline, exercised without a fault.
+constexpr int kWaitCheckCode = 5;
+
+__global__ void tc_wait_check_kernel(int* err, unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_wait(&bar, 0, err, kWaitCheckCode, limit_ns);
+  }
 }
 
 }  // namespace dino
@@ -1283,6 +1302,17 @@ extern "C" int dino_plan_describe(dino_plan* p, char* buf, size_t len) {
   if (!tc.empty()) s += "; " + tc;
   snprintf(buf, len, "%s", s.c_str());
   return DINO_OK;
+}
+
+extern "C" int dino_plan_check_wait_timeout(dino_plan* p, int64_t limit_ns, void* stream) {
+  DINO_REQUIRE(p, DINO_ERR_ARG, "dino_plan_check_wait_timeout: null argument");
+  DINO_REQUIRE(p->tc, DINO_ERR_UNSUPPORTED,
+               "dino_plan_check_wait_timeout: the plan has no tensor-core kernels");
+  DINO_REQUIRE(limit_ns >= 1000000 && limit_ns <= 10000000000LL, DINO_ERR_ARG,
+               "dino_plan_check_wait_timeout: limit must be 1 ms .. 10 s");
+  dino::tc_wait_check_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(
+      p->tc->d_err, (unsigned long long)limit_ns);
+  return dino::check_launch("tc_wait_check");
 }
 
 extern "C" int dino_plan_status(dino_plan* p) {

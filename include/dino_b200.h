@@ -120,8 +120,20 @@ DINO_API int dino_plan_legendre_column(const dino_plan* plan, int32_t m, int32_t
 DINO_API int dino_plan_describe(dino_plan* plan, char* buf, size_t len);
 
 /* Synchronizes the device and reports whether any bounded device-side wait
- * of this plan's kernels gave up (DINO_ERR_TIMEOUT); DINO_OK otherwise. */
+ * of this plan's kernels gave up (DINO_ERR_TIMEOUT, after which the flag is
+ * cleared); DINO_OK otherwise.  Replaces the reference's reliance on XLA
+ * raising at dispatch; no direct counterpart. */
 DINO_API int dino_plan_status(dino_plan* plan);
+
+/* Diagnostic of the failure path (no counterpart in the reference): launches
+ * one CTA on `stream` whose bounded wait, the routine every tensor-core
+ * pipeline wait uses, waits on an mbarrier that nothing completes; after
+ * limit_ns (1 ms .. 10 s) it gives up and records a code in the plan's device
+ * error flag, so that the next dino_plan_status returns DINO_ERR_TIMEOUT.
+ * The context stays usable.  Tensor-core plans only (else
+ * DINO_ERR_UNSUPPORTED). */
+DINO_API int dino_plan_check_wait_timeout(dino_plan* plan, int64_t limit_ns,
+                                          void* stream);
 
 /* Allocation-free inverse transform (no counterpart in the reference).
  * Same result as dino_sht_inverse on an FP32 plan, but the intermediate
@@ -240,6 +252,19 @@ DINO_API int dino_pe_step(dino_pe* pe, float* d_state, double dt,
 DINO_API int dino_pe_step_graph(dino_pe* pe, float* d_state, double dt,
                        const double* host_filter, int32_t n_steps,
                        void* stream);
+/* trajectory_from_step(step, outer_steps, inner_steps, start_with_input)
+ * (dinosaur/time_integration.py:523-564) for the filtered SIL3 step: advances
+ * d_state in place by outer_steps x inner_steps steps and writes outer_steps
+ * frames of the packed state (dino_pe_state_size floats each) to d_frames:
+ * the state after each block of inner_steps steps, or before it when
+ * start_with_input is nonzero.  The steps replay the captured step graph and
+ * each frame is a device-to-device copy on the same stream, so the host
+ * issues the whole rollout without waiting.  d_frames must not overlap
+ * d_state. */
+DINO_API int dino_pe_trajectory(dino_pe* pe, float* d_state, double dt,
+                                const double* host_filter, int32_t outer_steps,
+                                int32_t inner_steps, int32_t start_with_input,
+                                float* d_frames, void* stream);
 
 /* Converts modal arrays between the Real layout ([M = 2 lw - 1][L], rows
  * m = 0, 1, -1, ...) and the FastSphericalHarmonics layout ([2 lw][L], rows
