@@ -3057,6 +3057,34 @@ int dino_pe_step_graph(dino_pe* pe, float* state, double dt,
   return DINO_OK;
 }
 
+int dino_pe_trajectory(dino_pe* pe, float* state, double dt, const double* host_filter,
+                       int32_t outer_steps, int32_t inner_steps, int32_t start_with_input,
+                       float* frames, void* stream) {
+  DINO_REQUIRE(pe && state, DINO_ERR_ARG, "dino_pe_trajectory: null argument");
+  DINO_REQUIRE(outer_steps >= 0 && inner_steps >= 1, DINO_ERR_ARG,
+               "dino_pe_trajectory: need outer_steps >= 0 and inner_steps >= 1");
+  if (outer_steps == 0) return DINO_OK;
+  const size_t n = (size_t)pe->n_state * pe->ML;
+  DINO_REQUIRE(frames, DINO_ERR_ARG, "dino_pe_trajectory: null frames");
+  DINO_REQUIRE(frames + n * outer_steps <= state || state + n <= frames, DINO_ERR_ARG,
+               "dino_pe_trajectory: frames must not overlap the state");
+  cudaStream_t st = (cudaStream_t)stream;
+  // Every frame: the captured step graph replayed inner_steps times and one
+  // device-to-device copy of the packed state into its slot, all queued on
+  // the stream; the host never waits.
+  for (int f = 0; f < outer_steps; ++f) {
+    float* slot = frames + (size_t)f * n;
+    if (start_with_input)
+      DINO_CHECK_CUDA(cudaMemcpyAsync(slot, state, n * sizeof(float),
+                                      cudaMemcpyDeviceToDevice, st));
+    DINO_TRY(dino_pe_step_graph(pe, state, dt, host_filter, inner_steps, stream));
+    if (!start_with_input)
+      DINO_CHECK_CUDA(cudaMemcpyAsync(slot, state, n * sizeof(float),
+                                      cudaMemcpyDeviceToDevice, st));
+  }
+  return DINO_OK;
+}
+
 int dino_pe_explicit_vjp(dino_pe* pe, const float* state, const float* tend_ct,
                          float* state_ct, void* stream) {
   DINO_REQUIRE(pe && state && tend_ct && state_ct, DINO_ERR_ARG,

@@ -374,6 +374,36 @@ class _Engine:
       raise ValueError(f'filter scaling must have shape ({self.L},)')
     return _lib.dptr(self._filt)
 
+  def trajectory_(self, buf, dt, filt, outer_steps, inner_steps, start_with_input):
+    """Advances buf in place by outer_steps x inner_steps filtered steps and
+    returns the (outer_steps, size) frames (dino_pe_trajectory)."""
+    fptr = self._filter_ptr(filt)
+    frames = torch.empty((outer_steps, self.size), device='cuda', dtype=torch.float32)
+    _lib.check(_lib.lib().dino_pe_trajectory(
+        self.handle, sh.ptr(buf), float(dt), fptr, int(outer_steps), int(inner_steps),
+        int(bool(start_with_input)), sh.ptr(frames) if outer_steps else None,
+        sh.stream_handle()), 'trajectory')
+    return frames
+
+  def unpack_frames(self, frames: torch.Tensor, like: State, sim_times=None) -> State:
+    """The (frames, size) buffer as one State whose leaves lead with the frame
+    axis."""
+    n = frames.shape[0]
+    per = [self.unpack(frames[i], like) for i in range(n)] if n else []
+    stack = lambda xs, like_leaf: (torch.stack(xs) if xs else
+                                   torch.empty((0,) + tuple(like_leaf.shape),
+                                               device='cuda'))
+    return State(
+        vorticity=stack([p.vorticity for p in per], like.vorticity),
+        divergence=stack([p.divergence for p in per], like.divergence),
+        temperature_variation=stack([p.temperature_variation for p in per],
+                                    like.temperature_variation),
+        log_surface_pressure=stack([p.log_surface_pressure for p in per],
+                                   like.log_surface_pressure),
+        tracers={k: stack([p.tracers[k] for p in per], like.tracers[k])
+                 for k in like.tracers},
+        sim_time=sim_times)
+
   def step_(self, buf, dt, filt, n_steps, graph=False):
     fptr = self._filter_ptr(filt)
     fn = (_lib.lib().dino_pe_step_graph if graph else _lib.lib().dino_pe_step)

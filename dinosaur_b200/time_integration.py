@@ -313,16 +313,58 @@ def _stack(frames):
           np.stack(xs) if isinstance(xs[0], np.ndarray) else xs[-1]), *frames)
 
 
+def _identity(x):
+  return x
+
+
 def trajectory_from_step(step_fn, outer_steps: int, inner_steps: int, *,
                          start_with_input: bool = False,
-                         post_process_fn=lambda x: x, outer_scan_fn=None,
+                         post_process_fn=_identity, outer_scan_fn=None,
                          inner_scan_fn=None):
-  """time_integration.py:523-564: returns x -> (final, stacked frames)."""
+  """time_integration.py:523-564: returns x -> (final, stacked frames).
+
+  For the fused primitive-equation step the whole rollout runs natively
+  (dino_pe_trajectory): the step graph is replayed and each frame is copied
+  on the device into one frame buffer, with no host round trip per frame;
+  post_process_fn then maps each frame.  A differentiable rollout, or any
+  other step function, runs frame by frame.
+  """
   del outer_scan_fn, inner_scan_fn
   if inner_steps != 1:
     step_fn = repeated(step_fn, inner_steps)
 
+  if isinstance(step_fn, FusedSIL3Step):
+    fused = step_fn
+
+    def native(x):
+      eng = fused.equation.engine(x)
+      buf = eng.pack(x)
+      if torch.is_grad_enabled() and buf.requires_grad:
+        return None
+      frames = eng.trajectory_(buf, fused.dt, fused.filter_scaling, outer_steps,
+                               fused.n_steps, start_with_input)
+      t0 = x.sim_time
+      final_time = None if t0 is None else t0 + fused.dt * fused.n_steps * outer_steps
+      times = None
+      if t0 is not None:
+        first = 0 if start_with_input else 1
+        times = torch.as_tensor([t0 + fused.dt * fused.n_steps * (i + first)
+                                 for i in range(outer_steps)])
+      final = eng.unpack(buf, x, final_time)
+      if post_process_fn is _identity:
+        return final, eng.unpack_frames(frames, x, times)
+      per = [post_process_fn(eng.unpack(frames[i], x,
+                                        None if times is None else times[i]))
+             for i in range(outer_steps)]
+      return final, _stack(per)
+  else:
+    native = None
+
   def multistep(x):
+    if native is not None:
+      out = native(x)
+      if out is not None:
+        return out
     frames = []
     for _ in range(outer_steps):
       x_next = step_fn(x)

@@ -128,6 +128,47 @@ def test_graph_replay_equals_eager():
     assert torch.equal(getattr(eager, k), getattr(graph, k)), k
 
 
+@pytest.mark.parametrize('start_with_input', [False, True])
+def test_trajectory_frames_equal_repeated_steps(start_with_input):
+  """trajectory_from_step (time_integration.py:523-564) on the fused step:
+  the native rollout's frames equal the states of repeated graph steps
+  bit for bit; sim_time advances per frame; post_process_fn maps frames."""
+  og, oeq, st, g, eq = make(tracers=_tracers, humidity='specific_humidity')
+  dt = 0.175008
+  step = ti.step_with_filters(ti.imex_rk_sil3(eq, dt),
+                              [ti.exponential_step_filter(g, dt)])
+  outer, inner = 3, 2
+  x = to_state(st)
+  x = pe.State(x.vorticity, x.divergence, x.temperature_variation,
+               x.log_surface_pressure, tracers=x.tracers, sim_time=1.5)
+  final, frames = ti.trajectory_from_step(
+      step, outer, inner, start_with_input=start_with_input)(x)
+  assert frames.vorticity.shape == (outer,) + tuple(x.vorticity.shape)
+  assert frames.tracers['tracer_a'].shape[0] == outer
+  ref = x
+  expected = []
+  for _ in range(outer):
+    nxt = ti.repeated(step, inner)(ref)
+    expected.append(ref if start_with_input else nxt)
+    ref = nxt
+  for i, e in enumerate(expected):
+    for k in KEYS:
+      assert torch.equal(getattr(frames, k)[i], getattr(e, k)), (i, k)
+    assert torch.equal(frames.tracers['specific_humidity'][i],
+                       e.tracers['specific_humidity'])
+  for k in KEYS:
+    assert torch.equal(getattr(final, k), getattr(ref, k)), k
+  first = 0 if start_with_input else 1
+  np.testing.assert_allclose(
+      frames.sim_time.numpy(), 1.5 + dt * inner * (np.arange(outer) + first))
+  assert final.sim_time == pytest.approx(1.5 + dt * inner * outer)
+  _, vort = ti.trajectory_from_step(step, outer, inner,
+                                    post_process_fn=lambda s: s.vorticity)(x)
+  assert torch.equal(vort, frames.vorticity if not start_with_input else
+                     torch.stack([e.vorticity for e in expected[1:]] +
+                                 [final.vorticity]))
+
+
 def test_members_batch_equals_single_runs():
   og, oeq, st, g, eq = make()
   st2 = dict(st)
@@ -217,6 +258,45 @@ def test_held_suarez_composed_step_matches_oracle():
   ref = od.step_with_filters(od.imex_rk_sil3(ocomp, dt), [oflt])(st)
   out = ti.step_with_filters(ti.imex_rk_sil3(comp, dt), [flt])(to_state(st))
   assert_state(out, ref, 2e-5)
+
+
+def test_held_suarez_forcing_standalone_matches_oracle():
+  """HeldSuarezForcingSigma evaluated on its own (held_suarez.py:105-167):
+  kt, equilibrium_temperature and explicit_terms against the oracle, and the
+  fused composition equal to the primitive equations' tendencies plus the
+  standalone forcing."""
+  og = osht.Grid.T21()
+  layers = 6
+  ost_, tref, orog, vert = ost.held_suarez_config(og, layers, member=2)
+  ops = od.SimUnits()
+  ohs = od.HeldSuarezForcingSigma(og, vert, ops, tref)
+  g = sh.Grid.T21()
+  coords = coordinate_systems.CoordinateSystem(
+      g, sigma_coordinates.SigmaCoordinates.equidistant(layers))
+  hs = held_suarez.HeldSuarezForcingSigma(coords, units.SimUnits(), tref)
+  np.testing.assert_allclose(hs.kv(), ohs.kv(), rtol=1e-12)
+  np.testing.assert_allclose(hs.kt(), ohs.kt(), rtol=1e-12)
+  ps = np.exp(og.to_nodal(ost_['log_surface_pressure']))
+  np.testing.assert_allclose(hs.equilibrium_temperature(ps),
+                             ohs.equilibrium_temperature(ps), rtol=1e-12)
+  t_dev = hs.equilibrium_temperature(torch.as_tensor(ps, device='cuda',
+                                                     dtype=torch.float32))
+  np.testing.assert_allclose(t_dev.cpu().numpy(), ohs.equilibrium_temperature(ps),
+                             rtol=2e-6)
+  st = od.tree_map(lambda x: np.asarray(x, np.float32).astype(np.float64), ost_)
+  rng = np.random.default_rng(6)
+  noise = rng.standard_normal((layers,) + og.modal_shape) * og.mask / 1e3
+  st['vorticity'] = (st['vorticity'] + noise).astype(np.float32).astype(np.float64)
+  st['divergence'] = (st['divergence'] + noise[::-1]).astype(np.float32).astype(np.float64)
+  got = hs.explicit_terms(to_state(st))
+  assert_state(got, ohs.explicit_terms(st), 2e-5)
+  peq = pe.PrimitiveEquationsSigma(tref, orog, coords, units.SimUnits())
+  fused = ti.compose_equations([peq, hs]).explicit_terms(to_state(st))
+  dyn = peq.explicit_terms(to_state(st))
+  for k in KEYS:
+    a = getattr(fused, k).double()
+    b = getattr(dyn, k).double() + getattr(got, k).double()
+    assert float((a - b).abs().max() / b.abs().max()) < 2e-5, k
 
 
 def test_config0_t21_day_matches_fp64_oracle():
