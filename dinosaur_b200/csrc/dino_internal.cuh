@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <cstdio>
@@ -50,6 +51,17 @@ struct Status {
 
 // Checks the launch status of the last kernel (does not synchronize).
 int check_launch(const char* what);
+
+// An NVTX range over the enclosing scope, so that profilers group the
+// kernels a phase launches under the reference's names for its phases
+// (inv_legendre, inv_fourier, fwd_fourier, fwd_legendre: the named calls of
+// spherical_harmonic.py:265-279).  Costs nothing without an attached tool.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Runs a set-up step (returning a status) once per device and process, with
 // that device current.  Kernel attributes such as the dynamic shared-memory

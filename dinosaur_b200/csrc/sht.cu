@@ -336,6 +336,7 @@ legendre_forward_simt(const float* __restrict__ G, float* __restrict__ out,
 // The FP32 SIMT inverse contraction regardless of the plan's precision.
 int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
                           cudaStream_t st) {
+  NvtxRange range("inv_legendre");
   dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
       in, out, nf, p->M, p->L, p->J, p->Jh, p->d_ptab, p->d_ptab_off);
@@ -344,6 +345,7 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 
 int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
                      cudaStream_t st) {
+  NvtxRange range("inv_legendre");
   if (p->precision != DINO_PREC_FP32)
     return tc_legendre_inverse(p, in, out, nf, st);
   dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
@@ -354,6 +356,7 @@ int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
 
 int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
                      cudaStream_t st) {
+  NvtxRange range("fwd_legendre");
   if (p->precision != DINO_PREC_FP32)
     return tc_legendre_forward(p, G, out, nf, st);
   if (p->L > 64) {
@@ -859,6 +862,7 @@ int sht_prepare(dino_plan* p) {
 
 int fourier_inverse(dino_plan* p, const float* F, float* nodal, int nf,
                     bool weighted_adjoint, cudaStream_t st) {
+  NvtxRange range("inv_fourier");
   const float* wq = weighted_adjoint ? p->d_wq : nullptr;
   if (p->fft_pow2) return rfft_dispatch(p, F, nodal, nf, true, wq, st);
   dim3 grid(ceil_div(p->J, 32), ceil_div(p->I, 8), nf);
@@ -869,6 +873,7 @@ int fourier_inverse(dino_plan* p, const float* F, float* nodal, int nf,
 
 int fourier_forward(dino_plan* p, const float* nodal, float* F, int nf,
                     bool weighted, cudaStream_t st) {
+  NvtxRange range("fwd_fourier");
   const float* wq = weighted ? p->d_wq : nullptr;
   if (p->fft_pow2) return rfft_dispatch(p, nodal, F, nf, false, wq, st);
   dim3 grid(ceil_div(p->J, 32), ceil_div(p->M, 8), nf);
