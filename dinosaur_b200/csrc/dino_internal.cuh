@@ -213,6 +213,12 @@ int sht_prepare(dino_plan* p);
 std::string tc_describe(dino_plan* p);  // legendre_tc.cu
 int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
                           cudaStream_t st);
+// FP32 SIMT forward Legendre contraction for any plan.
+int legendre_forward_fp32(dino_plan* p, const float* fourier, float* out, int nf,
+                          cudaStream_t st);
+// Whether a tensor-core plan's autotuner found the FP32 SIMT contraction of
+// this direction faster at its chunk size (legendre_tc.cu).
+bool tc_use_simt(const dino_plan* p, bool forward);
 
 // legendre_tc.cu
 int tc_tables_build(dino_plan* p);

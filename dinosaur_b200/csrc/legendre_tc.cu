@@ -29,6 +29,7 @@
 #include <cuda_bf16.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -55,6 +56,11 @@ struct TcTables {
   // Autotuning record: candidates tried and the chosen launch time.
   int tuned_fields = 0, tried_inv = 0, tried_fwd = 0;
   float us_inv = 0.f, us_fwd = 0.f;
+  // The FP32 SIMT contraction, timed beside the tensor-core shapes; a
+  // direction whose SIMT launch is faster at the tuned size runs SIMT (more
+  // accurate than either split form, so the precision contract holds).
+  float us_simt_inv = 0.f, us_simt_fwd = 0.f;
+  int simt_inv = 0, simt_fwd = 0;
 };
 
 __host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m - 1) / m * m; }
@@ -1129,8 +1135,34 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
     }
     return DINO_OK;
   };
+  // The FP32 SIMT contraction on the same sizes (3 timed launches after one
+  // warm-up, like the tensor-core shapes).
+  auto time_simt = [&](bool forward, float* us) -> int {
+    constexpr int kReps = 3;
+    for (int r = 0; r <= kReps; ++r) {
+      if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
+      if (forward)
+        DINO_TRY(legendre_forward_fp32(p, p->d_work, modal, nf, 0));
+      else
+        DINO_TRY(legendre_inverse_fp32(p, one_seg(modal, nf), p->d_work, nf, 0));
+    }
+    DINO_CHECK_CUDA(cudaEventRecord(e1, 0));
+    DINO_CHECK_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    DINO_CHECK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *us = 1e3f * ms / kReps;
+    return DINO_OK;
+  };
   int rc = tune(false);
   if (rc == DINO_OK) rc = tune(true);
+  if (rc == DINO_OK) rc = time_simt(false, &t->us_simt_inv);
+  if (rc == DINO_OK) rc = time_simt(true, &t->us_simt_fwd);
+  // DINO_B200_TENSOR_CORES_ONLY=1 keeps the tensor-core form whatever the
+  // timings (the tests of the tensor-core kernels on small grids use it).
+  const char* only = std::getenv("DINO_B200_TENSOR_CORES_ONLY");
+  const bool tc_only = only && only[0] == '1';
+  t->simt_inv = !tc_only && t->us_simt_inv < t->us_inv ? 1 : 0;
+  t->simt_fwd = !tc_only && t->us_simt_fwd < t->us_fwd ? 1 : 0;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(modal);
@@ -1138,16 +1170,23 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
   return tc_status(p);
 }
 
+bool tc_use_simt(const dino_plan* p, bool forward) {
+  const TcTables* t = p->tc;
+  return t && (forward ? t->simt_fwd : t->simt_inv);
+}
+
 std::string tc_describe(dino_plan* p) {
   TcTables* t = p->tc;
   if (!t) return "";
-  char buf[512];
+  char buf[768];
   snprintf(buf, sizeof(buf),
            "tcgen05 %s Legendre autotuned on %d fields: inverse %d N ranges of "
-           "%d rows, %d stages (%.1f us, %d shapes tried); forward %d N ranges of %d rows, "
-           "%d stages (%.1f us, %d shapes tried)",
-           t->tf32 ? "split-TF32" : "split-BF16", t->tuned_fields, t->nsplit_inv, t->Nsub_inv, t->stages_inv, t->us_inv,
-           t->tried_inv, t->nsplit_fwd, t->Nsub_fwd, t->stages_fwd, t->us_fwd, t->tried_fwd);
+           "%d rows, %d stages (%.1f us, %d shapes tried; FP32 SIMT %.1f us%s); forward %d N "
+           "ranges of %d rows, %d stages (%.1f us, %d shapes tried; FP32 SIMT %.1f us%s)",
+           t->tf32 ? "split-TF32" : "split-BF16", t->tuned_fields, t->nsplit_inv, t->Nsub_inv,
+           t->stages_inv, t->us_inv, t->tried_inv, t->us_simt_inv,
+           t->simt_inv ? ", faster: used" : "", t->nsplit_fwd, t->Nsub_fwd, t->stages_fwd,
+           t->us_fwd, t->tried_fwd, t->us_simt_fwd, t->simt_fwd ? ", faster: used" : "");
   return buf;
 }
 

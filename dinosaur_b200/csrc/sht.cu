@@ -346,7 +346,7 @@ int legendre_inverse_fp32(dino_plan* p, const Segs& in, float* out, int nf,
 int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
                      cudaStream_t st) {
   NvtxRange range("inv_legendre");
-  if (p->precision != DINO_PREC_FP32)
+  if (p->precision != DINO_PREC_FP32 && !tc_use_simt(p, false))
     return tc_legendre_inverse(p, in, out, nf, st);
   dim3 grid(ceil_div(p->Jh, kLegTN), ceil_div(2 * nf, kLegTB), p->lw);
   legendre_inverse_simt<<<grid, kLegThreads, 0, st>>>(
@@ -357,8 +357,14 @@ int legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
 int legendre_forward(dino_plan* p, const float* G, float* out, int nf,
                      cudaStream_t st) {
   NvtxRange range("fwd_legendre");
-  if (p->precision != DINO_PREC_FP32)
+  if (p->precision != DINO_PREC_FP32 && !tc_use_simt(p, true))
     return tc_legendre_forward(p, G, out, nf, st);
+  return legendre_forward_fp32(p, G, out, nf, st);
+}
+
+// The FP32 SIMT forward contraction regardless of the plan's precision.
+int legendre_forward_fp32(dino_plan* p, const float* G, float* out, int nf,
+                          cudaStream_t st) {
   if (p->L > 64) {
     dim3 grid(ceil_div(p->L, 64), ceil_div(2 * nf, kLegTB), p->lw);
     legendre_forward_simt<64><<<grid, kLegThreads, 0, st>>>(

@@ -20,6 +20,13 @@ from oracle import states as ost
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def _tensor_cores_only(monkeypatch):
+  # These tests exercise the tensor-core kernels themselves: keep them even
+  # on grids where the plan's autotuner would pick the FP32 SIMT contraction.
+  monkeypatch.setenv('DINO_B200_TENSOR_CORES_ONLY', '1')
+
 from dinosaur_b200 import _lib  # noqa: E402
 from dinosaur_b200 import spherical_harmonic as sh  # noqa: E402
 

@@ -35,6 +35,13 @@ from oracle import states as ost  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def _tensor_cores_only(monkeypatch):
+  # These tests exercise the tensor-core kernels themselves: keep them even
+  # on grids where the plan's autotuner would pick the FP32 SIMT contraction.
+  monkeypatch.setenv('DINO_B200_TENSOR_CORES_ONLY', '1')
+
 FORMS = ['fp32', 'bf16x3', 'tf32x3']
 BOUNDS = {'fp32': (2e-6, 1e-5), 'bf16x3': (1e-5, 5e-5), 'tf32x3': (2e-6, 1e-5)}
 FIELDS = 128

@@ -17,6 +17,13 @@ from oracle import states as ost
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def _tensor_cores_only(monkeypatch):
+  # These tests exercise the tensor-core kernels themselves: keep them even
+  # on grids where the plan's autotuner would pick the FP32 SIMT contraction.
+  monkeypatch.setenv('DINO_B200_TENSOR_CORES_ONLY', '1')
+
 from dinosaur_b200 import _lib  # noqa: E402
 from dinosaur_b200 import spherical_harmonic as sh  # noqa: E402
 
@@ -156,3 +163,22 @@ def test_autotuner_records_its_choice(precision, form):
   assert 'autotuned' in d and 'shapes tried' in d, d
   assert form in d
   assert 'FP32 (SIMT)' in sh.Grid.T21().plan.describe()
+
+
+def test_autotuner_may_pick_fp32_simt_and_stays_accurate(monkeypatch):
+  """Without the override the plan times the FP32 SIMT contraction beside
+  the tensor-core shapes and runs whichever is faster per direction (on
+  small grids often SIMT); either way the result meets the split form's
+  bound."""
+  monkeypatch.delenv('DINO_B200_TENSOR_CORES_ONLY', raising=False)
+  g = tc_grid('T42', 'bf16x3')
+  desc = g.plan.describe()
+  assert 'FP32 SIMT' in desc, desc
+  og = osht.Grid.T42()
+  x = ost.sht_modal_input(og, 8, seed=5)
+  nodal = g.to_nodal(torch.as_tensor(x, device='cuda'))
+  ref = og.to_nodal(x.astype(np.float64))
+  assert l2(nodal, ref) < TOL['bf16x3'][0]
+  modal = g.to_modal(nodal)
+  refm = og.to_modal(ref)
+  assert l2(modal, refm) < TOL['bf16x3'][0]
