@@ -307,6 +307,14 @@ class on_gpu_numa_node:
     return False
 
 
+def _measured_peaks():
+  try:
+    with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+      return json.load(fh)
+  except OSError:
+    return {}
+
+
 def replica_seed(rank):
   """Each replica transforms its own seeded batch."""
   return 1000 + rank
@@ -466,7 +474,13 @@ def legendre_forms(torch, args, peaks):
     x = torch.as_tensor(modal_input(FIELDS, 0, name), device='cuda')
     for form in FORMS:
       impl = functools.partial(sh.CudaSphericalHarmonics, precision=form)
-      plan = getattr(sh.Grid, name)(spherical_harmonics_impl=impl).plan
+      # Each form as such: the plans keep their tensor-core contraction even
+      # where the autotuner would choose the FP32 SIMT one.
+      os.environ['DINO_B200_TENSOR_CORES_ONLY'] = '1'
+      try:
+        plan = getattr(sh.Grid, name)(spherical_harmonics_impl=impl).plan
+      finally:
+        os.environ.pop('DINO_B200_TENSOR_CORES_ONLY', None)
       for _ in range(args.warmup):
         y = plan.forward(plan.inverse(x))
       torch.cuda.synchronize()
@@ -597,28 +611,35 @@ def run_ours(args):
   ev_out = [torch.cuda.Event() for _ in range(2)]
   for e in ev_out:
     e.record(s_out)
+
+  def e2e_steps(n):
+    s_in.wait_stream(stream)
+    for i in range(n):
+      b = i % 2
+      with torch.cuda.stream(s_in):
+        s_in.wait_event(ev_done[b])  # the transforms finished reading xs[b]
+        xs[b].copy_(x_host, non_blocking=True)
+        ev_in[b].record(s_in)
+      stream.wait_event(ev_in[b])
+      stream.wait_event(ev_out[b])   # ys[b] has been copied out
+      yd = grid.to_modal(grid.to_nodal(xs[b]))
+      ys[b].copy_(yd)
+      ev_done[b].record(stream)
+      with torch.cuda.stream(s_out):
+        s_out.wait_event(ev_done[b])
+        out_host.copy_(ys[b], non_blocking=True)
+        ev_out[b].record(s_out)
+    stream.wait_stream(s_out)
+
+  # Untimed warm-up of the pipelined loop (allocator, streams), then the
+  # timed steps.
+  e2e_steps(args.warmup)
   barrier()
   torch.cuda.synchronize()
   e2 = torch.cuda.Event(enable_timing=True)
   e3 = torch.cuda.Event(enable_timing=True)
   e2.record(stream)
-  s_in.wait_stream(stream)
-  for i in range(args.steps):
-    b = i % 2
-    with torch.cuda.stream(s_in):
-      s_in.wait_event(ev_done[b])  # the transforms finished reading xs[b]
-      xs[b].copy_(x_host, non_blocking=True)
-      ev_in[b].record(s_in)
-    stream.wait_event(ev_in[b])
-    stream.wait_event(ev_out[b])   # ys[b] has been copied out
-    yd = grid.to_modal(grid.to_nodal(xs[b]))
-    ys[b].copy_(yd)
-    ev_done[b].record(stream)
-    with torch.cuda.stream(s_out):
-      s_out.wait_event(ev_done[b])
-      out_host.copy_(ys[b], non_blocking=True)
-      ev_out[b].record(s_out)
-  stream.wait_stream(s_out)
+  e2e_steps(args.steps)
   e3.record(stream)
   torch.cuda.synchronize()
   barrier()
@@ -705,6 +726,47 @@ def run_ours(args):
     dist.destroy_process_group()
 
 
+def pe_step_bytes(eng, grid_name):
+  """Algorithmic HBM bytes of one filtered SIL3 step of the unfused phase
+  sequence: every phase reads its inputs and writes its outputs once.
+
+  Per explicit evaluation (3 per step): the modal pre-pass (state in,
+  auxiliary planes out), the inverse transform (n_inv modal in, n_inv nodal
+  out, Legendre table), the nodal column kernel (n_inv in, n_fwd out), the
+  forward transform (n_fwd nodal in, n_fwd modal out, table) and the modal
+  post-pass (n_fwd modal and the state in, a tendency out).  The Fourier
+  intermediates are not counted (chunks are sized to stay in L2).  Implicit
+  part: the four operator products read their n_impl implicit planes and
+  write n_impl (2 n_impl for the stage that also forms G Y2); the three
+  combines read y0 and 1, 2, 3 explicit tendencies plus 1, 1, 2 implicit
+  ones and write a state."""
+  import ctypes
+  from dinosaur_b200 import _lib
+  counts = (ctypes.c_int32 * 5)()
+  _lib.check(_lib.lib().dino_pe_counts(eng.handle, counts), 'dino_pe_counts')
+  n_state, n_aux, n_inv, n_fwd, n_impl = list(counts)
+  lw, L, I, J, M, _ = workload_dims_any(grid_name)
+  ml, ij = M * L * 4, I * J * 4
+  table = 4 * ((J + 1) // 2) * sum(L - m for m in range(lw))
+  explicit = ((n_state + n_aux) + n_inv + 2 * n_fwd + n_state) * ml + \
+      (2 * n_inv + 2 * n_fwd) * ij + 2 * table
+  implicit = 9 * n_impl * ml + (3 * n_state + 4 * n_state + 5 * n_state) * ml + \
+      (1 + 1 + 2) * n_impl * ml
+  return 3 * explicit + implicit
+
+
+def workload_dims_any(name):
+  """(lw, L, I, J, M, N_tri) of a standard Grid by name (T / TL)."""
+  if name in GRIDS:
+    return workload_dims(name)
+  linear = name.startswith('TL')
+  tmax = int(name[2:] if linear else name[1:])
+  gaussian = {21: 16, 31: 24, 42: 32, 85: 64, 63: 32, 127: 64, 255: 128}[tmax]
+  lw, L, I, J = tmax + 1, tmax + 2, 4 * gaussian, 2 * gaussian
+  M = 2 * lw - 1
+  return lw, L, I, J, M, L + 2 * sum(L - m for m in range(1, lw))
+
+
 def pe_extras(torch):
   """Primitive-equation steps/s on the benchmark grids (CUDA-graph replay).
 
@@ -783,9 +845,13 @@ def pe_extras(torch):
     a1.record()
     torch.cuda.synchronize()
     ms = a0.elapsed_time(a1) / n
+    nbytes = pe_step_bytes(eng, grid_name)
+    hbm = _measured_peaks().get('hbm_gbs', 6650.0)
     out[name] = {'ms_per_step': ms, 'steps_per_s': 1e3 / ms,
                  'member_steps_per_s': members * 1e3 / ms,
-                 'precision': precision,
+                 'precision': precision, 'plan': g.plan.describe(),
+                 'algorithmic_bytes_per_step': nbytes,
+                 'hbm_frac': nbytes / (ms * 1e-3) / 1e9 / hbm,
                  'finite': bool(torch.isfinite(buf).all())}
     del eng, buf, state, eq
     torch.cuda.empty_cache()

@@ -158,6 +158,7 @@ SIGNATURES = {
     'dino_pe_implicit_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     'dino_pe_implicit_inverse_vjp': (ctypes.c_int, [_vp, _vp, _vp,
                                                     ctypes.c_double, _vp]),
+    'dino_pe_counts': (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     'dino_pe_trajectory': (ctypes.c_int, [_vp, _vp, ctypes.c_double, _DP, _i32, _i32,
                                           _i32, _vp, _vp]),
     'dino_pe_step_vjp': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double,

@@ -2961,6 +2961,16 @@ int dino_pe_destroy(dino_pe* pe) {
   return DINO_OK;
 }
 
+int dino_pe_counts(const dino_pe* pe, int32_t* counts) {
+  DINO_REQUIRE(pe && counts, DINO_ERR_ARG, "dino_pe_counts: null argument");
+  counts[0] = pe->n_state;
+  counts[1] = pe->n_aux;
+  counts[2] = pe->n_inv;
+  counts[3] = pe->n_fwd;
+  counts[4] = pe->mem * (2 * pe->K + 1);
+  return DINO_OK;
+}
+
 int64_t dino_pe_state_size(const dino_pe* pe) {
   if (!pe) return -1;
   return (int64_t)pe->n_state * (int64_t)pe->ML;

@@ -236,6 +236,12 @@ DINO_API int dino_pe_create(dino_plan* plan, const dino_pe_desc* desc, dino_pe**
 DINO_API int dino_pe_destroy(dino_pe* pe);
 /* Size in floats of one packed state. */
 DINO_API int64_t dino_pe_state_size(const dino_pe* pe);
+/* Plane counts of the engine's work, for traffic accounting (no counterpart
+ * in the reference): counts[0] state planes, [1] modal auxiliary planes made
+ * by the pre-pass, [2] fields of the inverse transform, [3] fields of the
+ * forward transform, [4] implicit planes (members x (2K + 1)); each plane
+ * is one [M][L] (modal) or [I][J] (nodal) array. */
+DINO_API int dino_pe_counts(const dino_pe* pe, int32_t* counts);
 DINO_API int dino_pe_explicit(dino_pe* pe, const float* d_state, float* d_tendency,
                      void* stream);
 DINO_API int dino_pe_implicit(dino_pe* pe, const float* d_state, float* d_out,
