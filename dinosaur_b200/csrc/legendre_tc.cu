@@ -47,15 +47,26 @@ struct TcTables {
   int Kj = 0;   // forward K extent (latitudes), multiple of the K block
   int Nf = 0;   // forward N (l'), multiple of 16
   void *Bih = nullptr, *Bil = nullptr, *Bfh = nullptr, *Bfl = nullptr;
-  CUtensorMap tBih, tBil, tBfh, tBfl;
   int* d_err = nullptr;
-  int stages_inv = 0, stages_fwd = 0;
-  size_t smem_inv = 0, smem_fwd = 0;
-  // N sub-ranges per (m, row tile) CTA and their width (B tile rows).
-  int nsplit_inv = 1, nsplit_fwd = 1, Nsub_inv = 0, Nsub_fwd = 0;
-  // Autotuning record: candidates tried and the chosen launch time.
-  int tuned_fields = 0, tried_inv = 0, tried_fwd = 0;
+  // Launch shape of each m group of each direction, chosen by the
+  // autotuner: N sub-ranges per (m, row tile) CTA and their width (B tile
+  // rows), pipeline depth, and the B tensor maps for that width.
+  struct Shape {
+    int m0 = 0, m1 = 0;
+    int nsplit = 1, Nsub = 0, stages = 0;
+    size_t smem = 0;
+    float us = 0.f;
+    int tried = 0;
+    CUtensorMap bh, bl;
+  };
+  static constexpr int kMaxGroups = 2;
+  Shape inv[kMaxGroups], fwd[kMaxGroups];
+  int ngroups_inv = 1, ngroups_fwd = 1;
+  // Autotuning record: the chunk size and each direction's total time.
+  int tuned_fields = 0;
   float us_inv = 0.f, us_fwd = 0.f;
+  // Total time of the two-group arrangement (0 when not tried).
+  float us_inv_split = 0.f, us_fwd_split = 0.f;
   // The FP32 SIMT contraction, timed beside the tensor-core shapes; a
   // direction whose SIMT launch is faster at the tuned size runs SIMT (more
   // accurate than either split form, so the precision contract holds).
@@ -455,6 +466,7 @@ struct TcArgs {
   const float* G;  // forward: weighted Fourier coefficients [nf][M][J]
   float* out;    // inverse: Fourier [nf][M][J]; forward: modal [nf][M][L]
   int* err;
+  int m0;        // first zonal wavenumber of the launch (blockIdx.y = m - m0)
 };
 
 // Pipeline order of the (K block, parity) stages: block k's parity 0, then
@@ -623,7 +635,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
   __shared__ __align__(8) uint64_t done_bar;
   __shared__ uint32_t tmem_slot;
 
-  const int m = blockIdx.y;
+  const int m = a.m0 + blockIdx.y;
   const int tile = blockIdx.x;
   const int rows = (m == 0) ? a.nf : 2 * a.nf;
   if (tile * 128 >= rows) return;  // uniform for the CTA
@@ -1020,11 +1032,16 @@ static TcArgs tc_args(const dino_plan* p, const TcTables* t, bool forward, int n
   a.J = p->J;
   a.Jh = p->Jh;
   a.Nrows = forward ? t->Nf : t->Np;
-  a.Nsub = forward ? t->Nsub_fwd : t->Nsub_inv;
-  a.stages = forward ? t->stages_fwd : t->stages_inv;
-  a.tmem_cols = tmem_cols_for(tc_accumulators(t->tf32) * a.Nsub);
   a.err = t->d_err;
   return a;
+}
+
+// A launch's shape fields in the kernel arguments.
+static void tc_set_shape(const TcTables* t, int m0, int nsub, int stages, TcArgs* a) {
+  a->m0 = m0;
+  a->Nsub = nsub;
+  a->stages = stages;
+  a->tmem_cols = tmem_cols_for(tc_accumulators(t->tf32) * nsub);
 }
 
 // One launch of the contraction in the plan's operand format.
@@ -1039,7 +1056,7 @@ static void tc_launch(const TcTables* t, dim3 grid, size_t smem, cudaStream_t st
 }
 
 template <bool kForward>
-static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
+static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int m0, int m1, int nf,
                          const float* src, float* out, cudaEvent_t e0, cudaEvent_t e1,
                          float* us) {
   const size_t lw2 = (size_t)p->lw * 2;
@@ -1052,9 +1069,7 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
     DINO_TRY(make_map(&bl, t->Bfl, t->tf32, t->Kj, (long long)lw2 * t->Nf, c.Nsub));
   }
   TcArgs a = tc_args(p, t, kForward, nf);
-  a.Nsub = c.Nsub;
-  a.stages = c.stages;
-  a.tmem_cols = tmem_cols_for(tc_accumulators(t->tf32) * c.Nsub);
+  tc_set_shape(t, m0, c.Nsub, c.stages, &a);
   a.out = out;
   CUtensorMap o2, o1;
   memset(&o2, 0, sizeof(o2));
@@ -1066,7 +1081,7 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int nf,
     a.vec = tc_vec_input(p, a.in);
     tc_out_maps(p, &a, out, nf, &o2, &o1);
   }
-  dim3 grid(ceil_div(2 * nf, 128), p->lw, c.nsplit);
+  dim3 grid(ceil_div(2 * nf, 128), m1 - m0, c.nsplit);
   constexpr int kReps = 3;
   for (int r = 0; r <= kReps; ++r) {
     if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
@@ -1097,42 +1112,77 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
   cudaEvent_t e0, e1;
   DINO_CHECK_CUDA(cudaEventCreate(&e0));
   DINO_CHECK_CUDA(cudaEventCreate(&e1));
-  auto tune = [&](bool forward) -> int {
-    std::vector<TcShape> cands;
-    tc_candidates(forward ? t->Nf : t->Np, tc_accumulators(t->tf32), &cands);
-    float best = 1e30f;
-    TcShape pick = cands.front();
-    for (const TcShape& c : cands) {
-      float us = 0.f;
-      const int rc = forward
-                         ? tc_time_shape<true>(p, t, c, nf, p->d_work, modal, e0, e1, &us)
-                         : tc_time_shape<false>(p, t, c, nf, modal, p->d_work, e0, e1, &us);
-      if (rc != DINO_OK) return rc;
-      if (us < best) {
-        best = us;
-        pick = c;
+  // Launch shapes are tuned for the whole m range in one launch and for two
+  // m groups (low and high zonal wavenumbers: the triangle's short high-m
+  // rows, with few l' for the forward and few K steps for the inverse,
+  // favour other splits and depths than the long low-m rows), each group in
+  // a launch of its own; per direction the faster arrangement is kept.
+  auto tune_groups = [&](bool forward, int ngroups, TcTables::Shape* out,
+                         float* total) -> int {
+    const size_t lw2 = (size_t)p->lw * 2;
+    *total = 0.f;
+    for (int gi = 0; gi < ngroups; ++gi) {
+      TcTables::Shape& sh = out[gi];
+      sh.m0 = gi * p->lw / ngroups;
+      sh.m1 = (gi + 1) * p->lw / ngroups;
+      // The group's widest N range: l' of its lowest m (forward), or the
+      // latitudes (inverse).
+      const int nfull = forward ? round_up((p->L - sh.m0 + 1) / 2, 16) : t->Np;
+      std::vector<TcShape> cands;
+      tc_candidates(nfull, tc_accumulators(t->tf32), &cands);
+      float best = 1e30f;
+      TcShape pick = cands.front();
+      for (const TcShape& c : cands) {
+        float us = 0.f;
+        const int rc =
+            forward ? tc_time_shape<true>(p, t, c, sh.m0, sh.m1, nf, p->d_work, modal, e0, e1, &us)
+                    : tc_time_shape<false>(p, t, c, sh.m0, sh.m1, nf, modal, p->d_work, e0, e1,
+                                           &us);
+        if (rc != DINO_OK) return rc;
+        if (us < best) {
+          best = us;
+          pick = c;
+        }
+      }
+      sh.nsplit = pick.nsplit;
+      sh.Nsub = pick.Nsub;
+      sh.stages = pick.stages;
+      sh.smem = pick.smem;
+      sh.us = best;
+      sh.tried = (int)cands.size();
+      *total += best;
+      if (forward) {
+        DINO_TRY(make_map(&sh.bh, t->Bfh, t->tf32, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
+        DINO_TRY(make_map(&sh.bl, t->Bfl, t->tf32, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
+      } else {
+        DINO_TRY(make_map(&sh.bh, t->Bih, t->tf32, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
+        DINO_TRY(make_map(&sh.bl, t->Bil, t->tf32, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
       }
     }
-    const size_t lw2 = (size_t)p->lw * 2;
-    if (forward) {
-      t->nsplit_fwd = pick.nsplit;
-      t->Nsub_fwd = pick.Nsub;
-      t->stages_fwd = pick.stages;
-      t->smem_fwd = pick.smem;
-      t->us_fwd = best;
-      t->tried_fwd = (int)cands.size();
-      DINO_TRY(make_map(&t->tBfh, t->Bfh, t->tf32, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
-      DINO_TRY(make_map(&t->tBfl, t->Bfl, t->tf32, t->Kj, (long long)lw2 * t->Nf, pick.Nsub));
-    } else {
-      t->nsplit_inv = pick.nsplit;
-      t->Nsub_inv = pick.Nsub;
-      t->stages_inv = pick.stages;
-      t->smem_inv = pick.smem;
-      t->us_inv = best;
-      t->tried_inv = (int)cands.size();
-      DINO_TRY(make_map(&t->tBih, t->Bih, t->tf32, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
-      DINO_TRY(make_map(&t->tBil, t->Bil, t->tf32, t->Kp, (long long)lw2 * t->Np, pick.Nsub));
+    return DINO_OK;
+  };
+  auto tune = [&](bool forward) -> int {
+    TcTables::Shape* dst = forward ? t->fwd : t->inv;
+    float one = 0.f;
+    DINO_TRY(tune_groups(forward, 1, dst, &one));
+    int ngroups = 1;
+    float best = one;
+    // DINO_B200_TC_M_GROUPS=1 or 2 forces the arrangement (tests of both).
+    const char* force = std::getenv("DINO_B200_TC_M_GROUPS");
+    const int forced = force ? std::atoi(force) : 0;
+    if (p->lw >= 32 && forced != 1) {
+      TcTables::Shape two[TcTables::kMaxGroups];
+      float t2 = 0.f;
+      DINO_TRY(tune_groups(forward, 2, two, &t2));
+      if (t2 < one || forced == 2) {
+        for (int gi = 0; gi < 2; ++gi) dst[gi] = two[gi];
+        ngroups = 2;
+        best = t2;
+      }
+      (forward ? t->us_fwd_split : t->us_inv_split) = t2;
     }
+    (forward ? t->ngroups_fwd : t->ngroups_inv) = ngroups;
+    (forward ? t->us_fwd : t->us_inv) = best;
     return DINO_OK;
   };
   // The FP32 SIMT contraction on the same sizes (3 timed launches after one
@@ -1178,16 +1228,30 @@ bool tc_use_simt(const dino_plan* p, bool forward) {
 std::string tc_describe(dino_plan* p) {
   TcTables* t = p->tc;
   if (!t) return "";
-  char buf[768];
-  snprintf(buf, sizeof(buf),
-           "tcgen05 %s Legendre autotuned on %d fields: inverse %d N ranges of "
-           "%d rows, %d stages (%.1f us, %d shapes tried; FP32 SIMT %.1f us%s); forward %d N "
-           "ranges of %d rows, %d stages (%.1f us, %d shapes tried; FP32 SIMT %.1f us%s)",
-           t->tf32 ? "split-TF32" : "split-BF16", t->tuned_fields, t->nsplit_inv, t->Nsub_inv,
-           t->stages_inv, t->us_inv, t->tried_inv, t->us_simt_inv,
-           t->simt_inv ? ", faster: used" : "", t->nsplit_fwd, t->Nsub_fwd, t->stages_fwd,
-           t->us_fwd, t->tried_fwd, t->us_simt_fwd, t->simt_fwd ? ", faster: used" : "");
-  return buf;
+  auto dir = [&](const char* name, const TcTables::Shape* g, int ng, float us, float split,
+                 float simt, int used) {
+    std::string out = name;
+    for (int gi = 0; gi < ng; ++gi) {
+      char b[160];
+      snprintf(b, sizeof(b), "%s m %d-%d: %d N ranges of %d rows, %d stages (%.1f us, %d shapes)",
+               gi ? ";" : "", g[gi].m0, g[gi].m1 - 1, g[gi].nsplit, g[gi].Nsub, g[gi].stages,
+               g[gi].us, g[gi].tried);
+      out += b;
+    }
+    char b[160];
+    snprintf(b, sizeof(b), "; %.1f us (two m groups: %.1f us), FP32 SIMT %.1f us%s", us, split,
+             simt, used ? ", faster: used" : "");
+    return out + b;
+  };
+  char head[128];
+  snprintf(head, sizeof(head), "tcgen05 %s Legendre autotuned on %d fields (shapes tried per m range): ",
+           t->tf32 ? "split-TF32" : "split-BF16", t->tuned_fields);
+  return std::string(head) +
+         dir("inverse", t->inv, t->ngroups_inv, t->us_inv, t->us_inv_split, t->us_simt_inv,
+             t->simt_inv) +
+         " | " +
+         dir("forward", t->fwd, t->ngroups_fwd, t->us_fwd, t->us_fwd_split, t->us_simt_fwd,
+             t->simt_fwd);
 }
 
 int tc_tables_build(dino_plan* p) {
@@ -1203,6 +1267,7 @@ int tc_tables_build(dino_plan* p) {
   const int half_l = (p->L + 1) / 2;
   t->Kp = round_up(half_l, kb);
   t->Np = round_up(p->Jh, 16);
+
   t->Kj = round_up(p->Jh, kb);
   t->Nf = round_up(half_l, 16);
   const size_t lw2 = (size_t)p->lw * 2;
@@ -1276,9 +1341,14 @@ int tc_legendre_inverse(dino_plan* p, const Segs& in, float* out, int nf,
   a.out = out;
   CUtensorMap o2, o1;
   tc_out_maps(p, &a, out, nf, &o2, &o1);
-  dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_inv);
-  tc_launch<false>(t, grid, t->smem_inv, st, t->tBih, t->tBil, o2, o1, a);
-  return check_launch("legendre_tc_inverse");
+  for (int gi = 0; gi < t->ngroups_inv; ++gi) {
+    const TcTables::Shape& sh = t->inv[gi];
+    tc_set_shape(t, sh.m0, sh.Nsub, sh.stages, &a);
+    dim3 grid(ceil_div(2 * nf, 128), sh.m1 - sh.m0, sh.nsplit);
+    tc_launch<false>(t, grid, sh.smem, st, sh.bh, sh.bl, o2, o1, a);
+    DINO_TRY(check_launch("legendre_tc_inverse"));
+  }
+  return DINO_OK;
 }
 
 int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
@@ -1291,9 +1361,14 @@ int tc_legendre_forward(dino_plan* p, const float* G, float* out, int nf,
   a.out = out;
   CUtensorMap unused;  // the forward epilogue uses row stores
   memset(&unused, 0, sizeof(unused));
-  dim3 grid(ceil_div(2 * nf, 128), p->lw, t->nsplit_fwd);
-  tc_launch<true>(t, grid, t->smem_fwd, st, t->tBfh, t->tBfl, unused, unused, a);
-  return check_launch("legendre_tc_forward");
+  for (int gi = 0; gi < t->ngroups_fwd; ++gi) {
+    const TcTables::Shape& sh = t->fwd[gi];
+    tc_set_shape(t, sh.m0, sh.Nsub, sh.stages, &a);
+    dim3 grid(ceil_div(2 * nf, 128), sh.m1 - sh.m0, sh.nsplit);
+    tc_launch<true>(t, grid, sh.smem, st, sh.bh, sh.bl, unused, unused, a);
+    DINO_TRY(check_launch("legendre_tc_forward"));
+  }
+  return DINO_OK;
 }
 
 // Reads (and clears) the plan's device error flag.

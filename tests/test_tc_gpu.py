@@ -160,7 +160,7 @@ def test_autotuner_records_its_choice(precision, form):
   keeps the fastest; the choice and its time are reported."""
   g = tc_grid('TL255', precision)
   d = g.plan.describe()
-  assert 'autotuned' in d and 'shapes tried' in d, d
+  assert 'autotuned' in d and 'shapes tried per m range' in d, d
   assert form in d
   assert 'FP32 (SIMT)' in sh.Grid.T21().plan.describe()
 
@@ -182,3 +182,23 @@ def test_autotuner_may_pick_fp32_simt_and_stays_accurate(monkeypatch):
   modal = g.to_modal(nodal)
   refm = og.to_modal(ref)
   assert l2(modal, refm) < TOL['bf16x3'][0]
+
+
+@pytest.mark.parametrize('precision', FORMS)
+@pytest.mark.parametrize('name', ['T85', 'TL255'])
+def test_two_m_group_launches_match_fp64_oracle(name, precision, monkeypatch):
+  """The per-m-range arrangement (low and high zonal wavenumbers launched
+  with shapes of their own) gives the same accuracy as one launch."""
+  monkeypatch.setenv('DINO_B200_TC_M_GROUPS', '2')
+  g = tc_grid(name, precision)
+  assert g.plan.describe().count(' m ') >= 4  # two groups in each direction
+  tl2, tmax = TOL[precision]
+  og = getattr(osht.Grid, name)()
+  x = ost.sht_modal_input(og, 5, seed=8)
+  nodal = g.to_nodal(torch.as_tensor(x, device='cuda'))
+  _lib.check(_lib.lib().dino_plan_status(g.plan.handle))
+  ref = og.to_nodal(x.astype(np.float64))
+  assert l2(nodal, ref) < tl2 and maxrel(nodal, ref) < tmax
+  modal = g.to_modal(nodal)
+  refm = og.to_modal(ref)
+  assert l2(modal, refm) < tl2 and maxrel(modal, refm) < tmax
