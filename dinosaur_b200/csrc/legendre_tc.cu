@@ -409,6 +409,31 @@ __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
   }
 }
 
+// Forward epilogue: stores one staged chunk (32 interleaved l = lbase + lane
+// of the rows row0 .. row0 + 31, stage[r][36]) of the modal output.  Rows are
+// (field, cos / sin of m) pairs for m > 0 (row0 even), fields for m = 0, so
+// each row's address follows from the previous one by a fixed step.
+__device__ __forceinline__ void fwd_store_chunk(float* out, int M, int L, int m, int rows,
+                                                int row0, const float* stage, int lbase,
+                                                bool keep, int lane) {
+  const int l = lbase + lane;
+  if (!keep || l >= L) return;
+  const size_t ML = (size_t)M * L;
+  const int rmax = min(32, rows - row0);
+  if (m == 0) {
+    float* o = out + (size_t)row0 * ML + l;
+#pragma unroll 4
+    for (int r = 0; r < rmax; ++r, o += ML) *o = stage[r * 36 + lane];
+  } else {
+    float* o = out + (size_t)(row0 >> 1) * ML + (size_t)(2 * m - 1) * L + l;
+#pragma unroll 4
+    for (int r = 0; r < rmax; r += 2, o += ML) {
+      o[0] = stage[r * 36 + lane];
+      if (r + 1 < rmax) o[L] = stage[(r + 1) * 36 + lane];
+    }
+  }
+}
+
 // Byte offset of 16-byte chunk c of row r in a 128-row K-major tile of
 // 128-byte rows with the 128-byte swizzle: the layout that TMA writes for
 // CU_TENSOR_MAP_SWIZZLE_128B and the UMMA descriptor (umma_desc_sw128) reads.
@@ -888,19 +913,10 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
           stage[lane * kStride + 2 * t + 1] = od[t];
         }
         __syncwarp();
-        const int lbase = m + 2 * (lo + 16 * c);
-        for (int r = 0; r < 32; ++r) {
-          const int rr = row0 + r;
-          if (rr >= rows) break;
-          const int l = lbase + lane;
-          const int lp = lo + 16 * c + (lane >> 1);
-          const bool keep = (lane & 1) ? (lp < n_par[1]) : (lp < n_par[0]);
-          if (keep && l < a.L) {
-            int b, row;
-            tc_row_map(m, rr, b, row);
-            a.out[((size_t)b * a.M + row) * a.L + l] = stage[r * kStride + lane];
-          }
-        }
+        const int lp = lo + 16 * c + (lane >> 1);
+        const bool keep = (lane & 1) ? (lp < n_par[1]) : (lp < n_par[0]);
+        fwd_store_chunk(a.out, a.M, a.L, m, rows, row0, stage, m + 2 * (lo + 16 * c), keep,
+                        lane);
         __syncwarp();
       }
     }
