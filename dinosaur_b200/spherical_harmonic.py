@@ -33,55 +33,85 @@ Array = Any
 
 
 def _legendre_host(n_m: int, n_l: int, x: np.ndarray) -> np.ndarray:
-  """p[m, j, l] with the normalised recurrence (associated_legendre.py:23-101)."""
+  """p[m, j, l]: associated Legendre functions normalised to unit L2 norm on
+  [-1, 1] (associated_legendre.py:23-101), entries with l < m zero.
+
+  Every order advances together: the sectoral values P_m^m come from one
+  cumulative product over m, and each step in l applies the normalised
+  three-term recurrence to all orders m < l at once (O(n_l) vector steps).
+  """
   x = np.asarray(x, np.float64)
-  y = np.sqrt(1 - x * x)
+  m = np.arange(n_m, dtype=np.float64)[:, None]
+  s = np.sqrt(1 - x * x)[None, :]
+  scale = np.concatenate([[1 / np.sqrt(2)], -np.sqrt(1 + 1 / (2 * m[1:, 0]))])
+  sectoral = np.cumprod(scale[:, None] * np.where(m > 0, s, 1.0), axis=0)
   out = np.zeros((n_m, len(x), n_l))
-  diag = np.full(len(x), 1 / np.sqrt(2))
-  for m in range(n_m):
-    if m:
-      diag = -np.sqrt(1 + 1 / (2 * m)) * y * diag
-    p2, p1 = np.zeros(len(x)), diag
-    out[m, :, m] = diag
-    for k in range(1, n_l - m):
-      mk2, mkp2 = (m + k) ** 2, (m + k - 1) ** 2
-      cur = np.sqrt((4 * mk2 - 1) / (mk2 - m * m)) * (
-          x * p1 - np.sqrt((mkp2 - m * m) / (4 * mkp2 - 1)) * p2)
-      out[m, :, m + k] = cur
-      p2, p1 = p1, cur
+  prev = np.zeros((n_m, len(x)))   # P_{l-2}^m
+  cur = np.zeros((n_m, len(x)))    # P_{l-1}^m
+  for l in range(n_l):
+    nxt = np.zeros_like(cur)
+    lower = m[:, 0] < l
+    if l > 0:
+      mm = m[lower]
+      a = np.sqrt((4.0 * l * l - 1) / (l * l - mm * mm))
+      b = np.sqrt(((l - 1.0) ** 2 - mm * mm) / (4.0 * (l - 1.0) ** 2 - 1))
+      nxt[lower] = a * (x[None, :] * cur[lower] - b * prev[lower])
+    if l < n_m:
+      nxt[l] = sectoral[l]
+    out[:, :, l] = nxt
+    prev, cur = cur, nxt
   return out
 
 
-def _weights_for(x: np.ndarray) -> np.ndarray:
-  """Quadrature weights exact for P_k, k < len(x) (associated_legendre.py:160-175)."""
-  legendre = _legendre_host(1, x.shape[0], x)[0].T
-  z = np.zeros_like(x)
-  z[0] = 1
-  w = np.linalg.solve(legendre, z)
-  return w / w.sum() * 2
+def _interpolatory_weights(n: int, with_poles: bool) -> np.ndarray:
+  """Weights of the n-point interpolatory rule on equiangular nodes, in the
+  order of ascending sin(latitude).
+
+  The reference solves sum_j w_j P_k(x_j) = delta_k0 for k < n
+  (associated_legendre.py:160-175): the unique n-point rule exact for
+  polynomials of degree < n.  On equiangular nodes that rule has a closed
+  form in the colatitudes phi: Fejer's first rule on the cell centres
+  phi_k = (k + 1/2) pi / n, and the Clenshaw-Curtis rule on
+  phi_k = k pi / (n - 1) with the poles (Waldvogel, BIT 46 (2006) 195-202).
+  Both node sets are symmetric, so the colatitude order needs no reversal.
+  """
+  if with_poles:
+    big_n = n - 1
+    phi = np.arange(n) * np.pi / big_n
+    j = np.arange(1, big_n // 2 + 1)
+    b = np.where(2 * j == big_n, 1.0, 2.0)
+    c = np.full(n, 2.0)
+    c[0] = c[-1] = 1.0
+    series = (b / (4.0 * j * j - 1))[None, :] * np.cos(2 * np.outer(phi, j))
+    return c / big_n * (1 - series.sum(axis=1))
+  phi = (np.arange(n) + 0.5) * np.pi / n
+  j = np.arange(1, n // 2 + 1)
+  series = np.cos(2 * np.outer(phi, j)) / (4.0 * j * j - 1)
+  return 2.0 / n * (1 - 2 * series.sum(axis=1))
 
 
 def _equiangular(n: int, with_poles: bool):
+  """Equiangular latitudes (associated_legendre.py:117-157) and their weights."""
   if with_poles:
     theta = np.linspace(-np.pi / 2, np.pi / 2, n)
   else:
     s = np.pi / n
     theta = np.linspace(-np.pi / 2 + s / 2, np.pi / 2 - s / 2, n)
-  x = np.sin(theta)
-  return x, _weights_for(x)
+  return np.sin(theta), _interpolatory_weights(n, with_poles)
 
 
 def _real_basis(wavenumbers: int, nodes: int) -> np.ndarray:
-  """Real Fourier basis (fourier.py:24-60)."""
+  """Real Fourier basis (fourier.py:24-60): columns 1/sqrt(2 pi), then
+  cos(k lambda)/sqrt(pi) and sin(k lambda)/sqrt(pi) interleaved for k >= 1."""
   if nodes < wavenumbers:
     raise ValueError('`real_basis` requires nodes >= wavenumbers; '
                      f'got m = {nodes} and n = {wavenumbers}.')
   lam = 2 * np.pi * np.arange(nodes) / nodes
+  k = np.arange(1, wavenumbers)
   f = np.empty((nodes, 2 * wavenumbers - 1))
   f[:, 0] = 1 / np.sqrt(2 * np.pi)
-  j = np.arange(1, wavenumbers)
-  f[:, 1::2] = np.cos(np.outer(lam, j)) / np.sqrt(np.pi)
-  f[:, 2::2] = np.sin(np.outer(lam, j)) / np.sqrt(np.pi)
+  f[:, 1::2] = np.cos(np.outer(lam, k)) / np.sqrt(np.pi)
+  f[:, 2::2] = np.sin(np.outer(lam, k)) / np.sqrt(np.pi)
   return f
 
 
