@@ -568,6 +568,72 @@ __device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int t
   }
 }
 
+// Inverse, rows at any alignment (L not a multiple of 4, or a segment that
+// starts off a 16-byte boundary): the same tasks, each read as W / 4 float4 of
+// the 16-byte-aligned window that holds its 2C entries, R = the entries'
+// misalignment (0..3, per task), and shifted into place with two rounds of
+// selects; a task whose window would cross the end of its row reads its
+// entries one by one.  The window ends inside the row, and it starts on the
+// 16-byte boundary at or before the task's first entry: inside the caller's
+// allocation, which starts on a 256-byte boundary (device allocations do).
+template <class Op>
+__device__ __forceinline__ void tc_produce_inverse_any(const TcArgs& a, int m, int tile,
+                                                       int rows, int k, uint8_t* t0,
+                                                       uint8_t* t1, int pt) {
+  constexpr uint32_t kTile = 128u * 128u;
+  constexpr int C = Op::kChunk, W = 2 * C + 4, U = Op::kUnroll;
+  for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
+    float w[U][W];
+    int sh[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = q0 + u * kTcProducers;
+#pragma unroll
+      for (int e = 0; e < W; ++e) w[u][e] = 0.f;
+      sh[u] = 0;
+      if (q >= kTcTasks) continue;
+      const int r = q >> 3, c = q & 7;
+      const int rr = tile * 128 + r;
+      if (rr >= rows) continue;
+      int b, row;
+      tc_row_map(m, rr, b, row);
+      const int l0 = 2 * Op::kKB * k + 2 * C * c;  // relative to l = m
+      const int lim = (a.L - m) - l0;             // valid entries from l0
+      const float* src = seg_field(a.in, b, (size_t)a.M * a.L) + (size_t)row * a.L + m + l0;
+      const int R = (int)((reinterpret_cast<uintptr_t>(src) >> 2) & 3);
+      if (lim >= W - R) {
+        const float4* w4 = reinterpret_cast<const float4*>(src - R);
+#pragma unroll
+        for (int i = 0; i < W / 4; ++i) {
+          const float4 t = __ldg(w4 + i);
+          w[u][4 * i] = t.x;
+          w[u][4 * i + 1] = t.y;
+          w[u][4 * i + 2] = t.z;
+          w[u][4 * i + 3] = t.w;
+        }
+        sh[u] = R;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 2 * C; ++e) w[u][e] = (e < lim) ? __ldg(src + e) : 0.f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = q0 + u * kTcProducers;
+      if (q >= kTcTasks) continue;
+      // o[e] = w[sh + e]: shift by 1, then by 2.
+      float y[2 * C + 2], o[2 * C];
+#pragma unroll
+      for (int i = 0; i < 2 * C + 2; ++i) y[i] = (sh[u] & 1) ? w[u][i + 1] : w[u][i];
+#pragma unroll
+      for (int e = 0; e < 2 * C; ++e) o[e] = (sh[u] & 2) ? y[e + 2] : y[e];
+      const uint32_t off = sw128_off(q >> 3, q & 7);
+      put_split<Op>(o, 0, 2, t0, t0 + kTile, off);
+      if (t1) put_split<Op>(o, 1, 2, t1, t1 + kTile, off);
+    }
+  }
+}
+
 // Forward: a task covers the C latitudes j0 .. j0 + C - 1 and their mirrors.
 template <class Op>
 __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int tile, int rows,
@@ -634,6 +700,8 @@ __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int
                                            uint8_t* t0, uint8_t* t1, int pt) {
   if (kForward) {
     tc_produce_forward<Op>(a, m, tile, rows, k, t0, t1, pt);
+  } else if (!a.vec) {
+    tc_produce_inverse_any<Op>(a, m, tile, rows, k, t0, t1, pt);
   } else {
     switch (m & 3) {
       case 0: tc_produce_inverse<Op, 0>(a, m, tile, rows, k, t0, t1, pt); break;
