@@ -399,6 +399,13 @@ __device__ __forceinline__ void tc_ld_acc(uint32_t base, int ncol, int c, bool o
 }
 
 
+// v[q] for a q known only at run time, by selects (no local-memory copy).
+__device__ __forceinline__ float4 pick4(const float4 (&v)[4], int q) {
+  const float4 a = (q & 1) ? v[1] : v[0];
+  const float4 b = (q & 1) ? v[3] : v[2];
+  return (q & 2) ? b : a;
+}
+
 __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
   if (m == 0) {
     b = r;
@@ -410,12 +417,12 @@ __device__ __forceinline__ void tc_row_map(int m, int r, int& b, int& row) {
 }
 
 // Forward epilogue: stores one staged chunk (32 interleaved l = lbase + lane
-// of the rows row0 .. row0 + 31, stage[r][36]) of the modal output.  Rows are
+// of the rows row0 .. row0 + 31, stage[r][stride]) of the modal output.  Rows are
 // (field, cos / sin of m) pairs for m > 0 (row0 even), fields for m = 0, so
 // each row's address follows from the previous one by a fixed step.
 __device__ __forceinline__ void fwd_store_chunk(float* out, int M, int L, int m, int rows,
-                                                int row0, const float* stage, int lbase,
-                                                bool keep, int lane) {
+                                                int row0, const float* stage, int stride,
+                                                int lbase, bool keep, int lane) {
   const int l = lbase + lane;
   if (!keep || l >= L) return;
   const size_t ML = (size_t)M * L;
@@ -423,13 +430,13 @@ __device__ __forceinline__ void fwd_store_chunk(float* out, int M, int L, int m,
   if (m == 0) {
     float* o = out + (size_t)row0 * ML + l;
 #pragma unroll 4
-    for (int r = 0; r < rmax; ++r, o += ML) *o = stage[r * 36 + lane];
+    for (int r = 0; r < rmax; ++r, o += ML) *o = stage[r * stride + lane];
   } else {
     float* o = out + (size_t)(row0 >> 1) * ML + (size_t)(2 * m - 1) * L + l;
 #pragma unroll 4
     for (int r = 0; r < rmax; r += 2, o += ML) {
-      o[0] = stage[r * 36 + lane];
-      if (r + 1 < rmax) o[L] = stage[(r + 1) * 36 + lane];
+      o[0] = stage[r * stride + lane];
+      if (r + 1 < rmax) o[L] = stage[(r + 1) * stride + lane];
     }
   }
 }
@@ -516,6 +523,12 @@ __device__ __forceinline__ void tc_seq(int i, int kb1, int& k, int& p) {
 // before converting any, so that enough bytes are in flight to cover the
 // latency.
 constexpr int kTcTasks = 128 * 8;
+// Tasks per producer thread in flight in the inverse: for split-BF16 all of
+// a K block's (1024 / 192 -> 6), so each K block costs one round trip to
+// memory (TL255 x 64 fields: first K block 4.2 -> 3.5 us after the CTA's
+// set-up); split-TF32 keeps its unroll.
+template <class Op>
+constexpr int kInvUnroll = Op::kFmt == OpBf16::kFmt ? 6 : Op::kUnroll;
 
 // Inverse: a task covers the 2C consecutive l = m + l0 .. m + l0 + 2C - 1
 // (both parities).  S = m mod 4 places them at entries S .. S + 2C - 1 of a
@@ -524,7 +537,7 @@ template <class Op, int S>
 __device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int tile, int rows,
                                                    int k, uint8_t* t0, uint8_t* t1, int pt) {
   constexpr uint32_t kTile = 128u * 128u;
-  constexpr int C = Op::kChunk, W = 2 * C + 4, U = Op::kUnroll;
+  constexpr int C = Op::kChunk, W = 2 * C + 4, U = kInvUnroll<Op>;
   for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
     float w[U][W];
 #pragma unroll
@@ -581,7 +594,7 @@ __device__ __forceinline__ void tc_produce_inverse_any(const TcArgs& a, int m, i
                                                        int rows, int k, uint8_t* t0,
                                                        uint8_t* t1, int pt) {
   constexpr uint32_t kTile = 128u * 128u;
-  constexpr int C = Op::kChunk, W = 2 * C + 4, U = Op::kUnroll;
+  constexpr int C = Op::kChunk, W = 2 * C + 4, U = kInvUnroll<Op>;
   for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
     float w[U][W];
     int sh[U];
@@ -716,8 +729,11 @@ __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int
 // and its lane 0 issues the MMAs, warps 2-7 produce the A tiles; all eight
 // warps drain TMEM in the epilogue (warp w reads lane quarter w mod 4 and
 // every other 16-column chunk).
+// The split-BF16 inverse keeps a K block's loads in flight in registers (one
+// CTA per SM, as its shapes with more than one pipeline stage have anyway);
+// the other kernels keep room for two CTAs per SM.
 template <bool kForward, class Op>
-__global__ void __launch_bounds__(kTcThreads, 2)
+__global__ void __launch_bounds__(kTcThreads, (!kForward && Op::kFmt == OpBf16::kFmt) ? 1 : 2)
 legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
                    const __grid_constant__ CUtensorMap tBl,
                    const __grid_constant__ CUtensorMap tO2,
@@ -863,6 +879,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
     // it back with row-contiguous, coalesced stores; the two warps of a lane
     // quarter take alternate 16-column chunks.
     constexpr int kStride = 36;  // floats per staged row (16-byte multiple)
+    constexpr int kFwdStride = 34;  // forward: floats per staged row (8-byte multiple)
     const int quarter = warp & 3, half = warp >> 2;
     // Each warp owns 8 KB of the drained pipeline buffers: two TMA-store
     // buffers (a direct and a mirrored 32 x 16 block each, the box layout of
@@ -888,12 +905,22 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
           __syncwarp();
           float4* d4 = reinterpret_cast<float4*>(sd + lane * 16);
           float4* m4 = reinterpret_cast<float4*>(sm + lane * 16);
+          float4 dv[4], mv[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            d4[i] = make_float4(e[4 * i] + od[4 * i], e[4 * i + 1] + od[4 * i + 1],
+            dv[i] = make_float4(e[4 * i] + od[4 * i], e[4 * i + 1] + od[4 * i + 1],
                                 e[4 * i + 2] + od[4 * i + 2], e[4 * i + 3] + od[4 * i + 3]);
-            m4[i] = make_float4(e[15 - 4 * i] - od[15 - 4 * i], e[14 - 4 * i] - od[14 - 4 * i],
+            mv[i] = make_float4(e[15 - 4 * i] - od[15 - 4 * i], e[14 - 4 * i] - od[14 - 4 * i],
                                 e[13 - 4 * i] - od[13 - 4 * i], e[12 - 4 * i] - od[12 - 4 * i]);
+          }
+          // A staged row is 64 bytes: at store i lane L writes its float4
+          // (i + L / 2) mod 4, so each 8-lane phase covers all 32 banks once.
+          const int rot = (lane >> 1) & 3;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int q = (i + rot) & 3;
+            d4[q] = pick4(dv, q);
+            m4[q] = pick4(mv, q);
           }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           __syncwarp();
@@ -957,8 +984,9 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
         }
         __syncwarp();
       }
-      // The stores have completed before the CTA (and its shared memory) ends.
-      if (lane == 0 && nb > 0) bulk_wait_all();
+      // The stores have read their shared-memory source before the CTA (and
+      // its shared memory) ends; their global writes complete with the grid.
+      if (lane == 0 && nb > 0) bulk_wait_read<0>();
       __syncwarp();
     } else {
       // Structural zeros l < m (first N range only), alternate rows.
@@ -974,17 +1002,16 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       for (int c = half; c < nchunks; c += 2) {
         float e[16], od[16];
         tc_ld_acc<Op>(lane_base, acc_cols, c, cnt[1] > 0, e, od);
-        // Interleave parities: l = m + 32c + 2t + p.
+        // Interleave parities: l = m + 32c + 2t + p.  Rows kFwdStride = 34
+        // floats apart: each half-warp's 8-byte stores cover all 32 banks.
 #pragma unroll
-        for (int t = 0; t < 16; ++t) {
-          stage[lane * kStride + 2 * t] = e[t];
-          stage[lane * kStride + 2 * t + 1] = od[t];
-        }
+        for (int t = 0; t < 16; ++t)
+          *reinterpret_cast<float2*>(stage + lane * kFwdStride + 2 * t) = make_float2(e[t], od[t]);
         __syncwarp();
         const int lp = lo + 16 * c + (lane >> 1);
         const bool keep = (lane & 1) ? (lp < n_par[1]) : (lp < n_par[0]);
-        fwd_store_chunk(a.out, a.M, a.L, m, rows, row0, stage, m + 2 * (lo + 16 * c), keep,
-                        lane);
+        fwd_store_chunk(a.out, a.M, a.L, m, rows, row0, stage, kFwdStride, m + 2 * (lo + 16 * c),
+                        keep, lane);
         __syncwarp();
       }
     }
@@ -1223,6 +1250,9 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
                     : tc_time_shape<false>(p, t, c, sh.m0, sh.m1, nf, modal, p->d_work, e0, e1,
                                            &us);
         if (rc != DINO_OK) return rc;
+        if (std::getenv("DINO_B200_TC_DEBUG"))
+          std::fprintf(stderr, "tc tune %s m %d-%d nsplit %d nsub %d stages %d smem %zu: %.1f us\n",
+                       forward ? "fwd" : "inv", sh.m0, sh.m1, c.nsplit, c.Nsub, c.stages, c.smem, us);
         if (us < best) {
           best = us;
           pick = c;
@@ -1518,3 +1548,4 @@ extern "C" int dino_plan_status(dino_plan* p) {
   DINO_CHECK_CUDA(cudaDeviceSynchronize());
   return dino::tc_status(p);
 }
+
