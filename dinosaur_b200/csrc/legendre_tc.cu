@@ -5,9 +5,10 @@
 // in the operand format (bf16: 8 significant bits, tf32: 11); each product is
 // formed as hi*hi + hi*lo + lo*hi (the lo*lo term, ~2^-16 relative for bf16
 // and ~2^-22 for tf32, is dropped) and accumulated in FP32 in tensor memory.
-// The Legendre tables are split from their FP64 values.  Both forms share
-// every tile shape: a 128-byte swizzled row holds one K block (64 bf16 or 32
-// tf32 entries) and one MMA instruction consumes 32 bytes of K (16 or 8).
+// The Legendre tables are split from their FP64 values.  A tile row holds
+// one K block of 32 entries, swizzled over its width (64 bytes of bf16, 128
+// bytes of tf32), and one MMA instruction consumes 32 bytes of K (16 or 8
+// entries).
 //
 // Per zonal wavenumber m the contraction is a GEMM
 //   inverse:  D[r, j]  = sum_{l'} X_p[r, l'] P_p[j, l']   (K = l', N = j)
@@ -15,7 +16,7 @@
 // with r = (field, cos/sin) rows, p the parity of l - m (the N/S fold),
 // l = m + 2 l' + p, and G_0 / G_1 the symmetric / antisymmetric latitude
 // folds.  The tables P_p are K-major split operands in HBM, loaded by TMA (no
-// multicast) into 128-byte-swizzled shared memory tiles; the A operand is
+// multicast) into swizzled shared memory tiles; the A operand is
 // produced in the same layout by six warps of the CTA straight from the FP32
 // modal coefficients (inverse) or Fourier coefficients (forward): one read of
 // the source gives both parities, folded and split.  One thread issues
@@ -28,6 +29,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -76,7 +78,7 @@ struct TcTables {
 
 __host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-// Operand formats.  kKB: K entries per 128-byte swizzled row (one K block per
+// Operand formats.  kKB: K entries per swizzled tile row (one K block per
 // pipeline stage); kStep: K entries per MMA instruction (32 bytes); kChunk: K
 // entries per 16-byte chunk of a row; kFmt: the instruction descriptor's A / B
 // format code; kUnroll: producer tasks loaded before any is converted;
@@ -89,18 +91,31 @@ __host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m -
 // term), so there these roundings dominate: the separate accumulators leave
 // one per K step on the large sums instead of three.  The bf16 split (~4e-6,
 // its dropped lo*lo term) dominates the roundings, so one accumulator serves.
+//
+// kRowBytes: bytes of one tile row (one K block), swizzled over its own
+// width (64 or 128 bytes); kLayout: the UMMA descriptor's code for that
+// swizzle.  Split-BF16 K blocks are 32 entries (64-byte rows), which halves a
+// pipeline stage against 128-byte rows, so that two CTAs share an SM at the
+// widest N range that fits TMEM twice (128 columns per accumulator).
 struct OpBf16 {
   typedef bf16 T;
-  static constexpr int kKB = 64, kStep = 16, kChunk = 8, kUnroll = 3;
+  static constexpr int kKB = 32, kStep = 16, kChunk = 8, kUnroll = 3;
+  static constexpr int kRowBytes = 64;
+  static constexpr uint64_t kLayout = 4;  // SWIZZLE_64B
   static constexpr uint32_t kFmt = 1;  // BF16
   static constexpr bool kSepAcc = false;
 };
 struct OpTf32 {
   typedef float T;  // tf32 in an FP32 container (low 13 mantissa bits zero)
   static constexpr int kKB = 32, kStep = 8, kChunk = 4, kUnroll = 6;
+  static constexpr int kRowBytes = 128;
+  static constexpr uint64_t kLayout = 2;  // SWIZZLE_128B
   static constexpr uint32_t kFmt = 2;  // TF32
   static constexpr bool kSepAcc = true;
 };
+
+// Row bytes of a plan's operand format (host side).
+constexpr int tc_row_bytes(int tf32) { return tf32 ? OpTf32::kRowBytes : OpBf16::kRowBytes; }
 
 // TMEM accumulators (each Nsub columns) per CTA: one per parity, twice that
 // with separate correction accumulators.
@@ -174,7 +189,7 @@ __global__ void tc_table_kernel(int lw, int L, int Jh, const double* __restrict_
 
 constexpr int kTcThreads = 256;
 constexpr int kTcProducers = 192;  // warps 2-7
-constexpr int kMaxStages = 4;
+constexpr int kMaxStages = 6;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -271,16 +286,18 @@ __device__ __forceinline__ void bulk_wait_all() {
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), leading offset unused for swizzled K-major.
-__device__ __forceinline__ uint64_t umma_desc_sw128(const void* p) {
+// Shared-memory matrix descriptor: K-major, rows of Op::kRowBytes swizzled
+// over their width, 8-row groups 8 * kRowBytes apart (SBO), leading offset
+// unused for swizzled K-major.
+template <class Op>
+__device__ __forceinline__ uint64_t umma_desc(const void* p) {
   uint64_t addr = smem_u32(p);
   uint64_t d = 0;
   d |= (addr >> 4) & 0x3FFFull;
   d |= 1ull << 16;
-  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)((8 * Op::kRowBytes) >> 4) << 32;
   d |= 1ull << 46;
-  d |= 2ull << 61;
+  d |= Op::kLayout << 61;
   return d;
 }
 
@@ -441,11 +458,17 @@ __device__ __forceinline__ void fwd_store_chunk(float* out, int M, int L, int m,
   }
 }
 
-// Byte offset of 16-byte chunk c of row r in a 128-row K-major tile of
-// 128-byte rows with the 128-byte swizzle: the layout that TMA writes for
-// CU_TENSOR_MAP_SWIZZLE_128B and the UMMA descriptor (umma_desc_sw128) reads.
-__device__ __forceinline__ uint32_t sw128_off(int r, int c) {
-  return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
+// Byte offset of 16-byte chunk c of row r in a K-major tile of
+// Op::kRowBytes rows swizzled over their width: the layout that TMA writes
+// for CU_TENSOR_MAP_SWIZZLE_128B / _64B and the UMMA descriptor (umma_desc)
+// reads.  128-byte rows: chunk c ^ (r mod 8); 64-byte rows: c ^ (r / 2 mod 4)
+// (the address bits 4-6 or 4-5 XOR bits 7-9 or 7-8).
+template <class Op>
+__device__ __forceinline__ uint32_t sw_off(int r, int c) {
+  if constexpr (Op::kRowBytes == 128)
+    return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
+  else
+    return (uint32_t)(r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
 }
 
 // hi = bf16x2(x0, x1) and lo = bf16x2 of the remainders x - hi, each rounded
@@ -522,13 +545,12 @@ __device__ __forceinline__ void tc_seq(int i, int kb1, int& k, int& p) {
 // A task is one (row, 16-byte chunk); each thread loads Op::kUnroll tasks
 // before converting any, so that enough bytes are in flight to cover the
 // latency.
-constexpr int kTcTasks = 128 * 8;
-// Tasks per producer thread in flight in the inverse: for split-BF16 all of
-// a K block's (1024 / 192 -> 6), so each K block costs one round trip to
-// memory (TL255 x 64 fields: first K block 4.2 -> 3.5 us after the CTA's
-// set-up); split-TF32 keeps its unroll.
 template <class Op>
-constexpr int kInvUnroll = Op::kFmt == OpBf16::kFmt ? 6 : Op::kUnroll;
+constexpr int kTcTasks = 128 * (Op::kRowBytes / 16);
+// Tasks per producer thread in flight in the inverse: all of a split-BF16 K
+// block's (512 / 192 -> 3), so each K block costs one round trip to memory.
+template <class Op>
+constexpr int kInvUnroll = Op::kUnroll;
 
 // Inverse: a task covers the 2C consecutive l = m + l0 .. m + l0 + 2C - 1
 // (both parities).  S = m mod 4 places them at entries S .. S + 2C - 1 of a
@@ -536,17 +558,18 @@ constexpr int kInvUnroll = Op::kFmt == OpBf16::kFmt ? 6 : Op::kUnroll;
 template <class Op, int S>
 __device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int tile, int rows,
                                                    int k, uint8_t* t0, uint8_t* t1, int pt) {
-  constexpr uint32_t kTile = 128u * 128u;
+  constexpr uint32_t kTile = 128u * Op::kRowBytes;
   constexpr int C = Op::kChunk, W = 2 * C + 4, U = kInvUnroll<Op>;
-  for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
+  for (int q0 = pt; q0 < kTcTasks<Op>; q0 += U * kTcProducers) {
     float w[U][W];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
 #pragma unroll
       for (int e = 0; e < W; ++e) w[u][e] = 0.f;
-      if (q >= kTcTasks) continue;
-      const int r = q >> 3, c = q & 7;
+      if (q >= kTcTasks<Op>) continue;
+      constexpr int CH = Op::kRowBytes / 16;  // chunks per tile row
+      const int r = q / CH, c = q % CH;
       const int rr = tile * 128 + r;
       if (rr >= rows) continue;
       int b, row;
@@ -572,8 +595,8 @@ __device__ __forceinline__ void tc_produce_inverse(const TcArgs& a, int m, int t
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
-      if (q >= kTcTasks) continue;
-      const uint32_t off = sw128_off(q >> 3, q & 7);
+      if (q >= kTcTasks<Op>) continue;
+      const uint32_t off = sw_off<Op>(q / (Op::kRowBytes / 16), q % (Op::kRowBytes / 16));
       // Entries S .. S+2C-1: even l - m are parity 0, odd ones parity 1.
       put_split<Op>(w[u], S, 2, t0, t0 + kTile, off);
       if (t1) put_split<Op>(w[u], S + 1, 2, t1, t1 + kTile, off);
@@ -593,9 +616,9 @@ template <class Op>
 __device__ __forceinline__ void tc_produce_inverse_any(const TcArgs& a, int m, int tile,
                                                        int rows, int k, uint8_t* t0,
                                                        uint8_t* t1, int pt) {
-  constexpr uint32_t kTile = 128u * 128u;
+  constexpr uint32_t kTile = 128u * Op::kRowBytes;
   constexpr int C = Op::kChunk, W = 2 * C + 4, U = kInvUnroll<Op>;
-  for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
+  for (int q0 = pt; q0 < kTcTasks<Op>; q0 += U * kTcProducers) {
     float w[U][W];
     int sh[U];
 #pragma unroll
@@ -604,8 +627,9 @@ __device__ __forceinline__ void tc_produce_inverse_any(const TcArgs& a, int m, i
 #pragma unroll
       for (int e = 0; e < W; ++e) w[u][e] = 0.f;
       sh[u] = 0;
-      if (q >= kTcTasks) continue;
-      const int r = q >> 3, c = q & 7;
+      if (q >= kTcTasks<Op>) continue;
+      constexpr int CH = Op::kRowBytes / 16;  // chunks per tile row
+      const int r = q / CH, c = q % CH;
       const int rr = tile * 128 + r;
       if (rr >= rows) continue;
       int b, row;
@@ -633,14 +657,14 @@ __device__ __forceinline__ void tc_produce_inverse_any(const TcArgs& a, int m, i
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
-      if (q >= kTcTasks) continue;
+      if (q >= kTcTasks<Op>) continue;
       // o[e] = w[sh + e]: shift by 1, then by 2.
       float y[2 * C + 2], o[2 * C];
 #pragma unroll
       for (int i = 0; i < 2 * C + 2; ++i) y[i] = (sh[u] & 1) ? w[u][i + 1] : w[u][i];
 #pragma unroll
       for (int e = 0; e < 2 * C; ++e) o[e] = (sh[u] & 2) ? y[e + 2] : y[e];
-      const uint32_t off = sw128_off(q >> 3, q & 7);
+      const uint32_t off = sw_off<Op>(q / (Op::kRowBytes / 16), q % (Op::kRowBytes / 16));
       put_split<Op>(o, 0, 2, t0, t0 + kTile, off);
       if (t1) put_split<Op>(o, 1, 2, t1, t1 + kTile, off);
     }
@@ -651,18 +675,19 @@ __device__ __forceinline__ void tc_produce_inverse_any(const TcArgs& a, int m, i
 template <class Op>
 __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int tile, int rows,
                                                    int k, uint8_t* t0, uint8_t* t1, int pt) {
-  constexpr uint32_t kTile = 128u * 128u;
+  constexpr uint32_t kTile = 128u * Op::kRowBytes;
   constexpr int C = Op::kChunk, U = Op::kUnroll;
   const bool vec = (a.J & 3) == 0;
-  for (int q0 = pt; q0 < kTcTasks; q0 += U * kTcProducers) {
+  for (int q0 = pt; q0 < kTcTasks<Op>; q0 += U * kTcProducers) {
     float d[U][C], e[U][C];  // G[j0 + t], G[J - 1 - j0 - t]
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
 #pragma unroll
       for (int t = 0; t < C; ++t) d[u][t] = e[u][t] = 0.f;
-      if (q >= kTcTasks) continue;
-      const int r = q >> 3, c = q & 7;
+      if (q >= kTcTasks<Op>) continue;
+      constexpr int CH = Op::kRowBytes / 16;  // chunks per tile row
+      const int r = q / CH, c = q % CH;
       const int rr = tile * 128 + r;
       if (rr >= rows) continue;
       int b, row;
@@ -694,8 +719,8 @@ __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int t
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int q = q0 + u * kTcProducers;
-      if (q >= kTcTasks) continue;
-      const uint32_t off = sw128_off(q >> 3, q & 7);
+      if (q >= kTcTasks<Op>) continue;
+      const uint32_t off = sw_off<Op>(q / (Op::kRowBytes / 16), q % (Op::kRowBytes / 16));
       float sv[C], dv[C];
 #pragma unroll
       for (int t = 0; t < C; ++t) {
@@ -729,11 +754,8 @@ __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int
 // and its lane 0 issues the MMAs, warps 2-7 produce the A tiles; all eight
 // warps drain TMEM in the epilogue (warp w reads lane quarter w mod 4 and
 // every other 16-column chunk).
-// The split-BF16 inverse keeps a K block's loads in flight in registers (one
-// CTA per SM, as its shapes with more than one pipeline stage have anyway);
-// the other kernels keep room for two CTAs per SM.
 template <bool kForward, class Op>
-__global__ void __launch_bounds__(kTcThreads, (!kForward && Op::kFmt == OpBf16::kFmt) ? 1 : 2)
+__global__ void __launch_bounds__(kTcThreads, 2)
 legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
                    const __grid_constant__ CUtensorMap tBl,
                    const __grid_constant__ CUtensorMap tO2,
@@ -772,8 +794,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
   if (kForward && cnt[0] == 0) return;
   if (!kForward && lo >= a.Jh) return;
   const int nblocks = kblk[0] + kblk[1];
-  const uint32_t tile_a = 128u * 128u;             // 128 rows x 128 bytes of K
-  const uint32_t tile_b = (uint32_t)a.Nsub * 128u;  // Nsub rows x 128 bytes of K
+  const uint32_t tile_a = 128u * Op::kRowBytes;             // 128 rows x one K block
+  const uint32_t tile_b = (uint32_t)a.Nsub * Op::kRowBytes;  // Nsub rows x one K block
   const uint32_t stage_bytes = 2 * tile_a + 2 * tile_b;
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
   uint8_t* base = smem_raw + pad;
@@ -828,16 +850,17 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       int k, p;
       tc_seq(i, kblk[1], k, p);
-      const int steps = min(4, (p ? ksteps[1] : ksteps[0]) - k * 4);
+      constexpr int kSPB = Op::kKB / Op::kStep;  // MMA K steps per K block
+      const int steps = min(kSPB, (p ? ksteps[1] : ksteps[0]) - k * kSPB);
       const uint32_t d = tmem + (uint32_t)(p * acc_cols);
       // Corrections: their own accumulator, or the same one.
       const uint32_t dc = Op::kSepAcc ? tmem + (uint32_t)((2 + p) * acc_cols) : d;
       const uint32_t idesc = umma_idesc<Op>(p ? ncols[1] : ncols[0]);
       uint8_t* st = base + (size_t)s * stage_bytes;
-      const uint64_t dah = umma_desc_sw128(st);
-      const uint64_t dal = umma_desc_sw128(st + tile_a);
-      const uint64_t dbh = umma_desc_sw128(st + 2 * tile_a);
-      const uint64_t dbl = umma_desc_sw128(st + 2 * tile_a + tile_b);
+      const uint64_t dah = umma_desc<Op>(st);
+      const uint64_t dal = umma_desc<Op>(st + tile_a);
+      const uint64_t dbh = umma_desc<Op>(st + 2 * tile_a);
+      const uint64_t dbl = umma_desc<Op>(st + 2 * tile_a + tile_b);
       for (int q = 0; q < steps; ++q) {
         const uint64_t off = (uint64_t)(2 * q);  // 32 bytes per K step, in 16 B units
         const uint32_t acc = (k > 0 || q > 0) ? 1u : 0u;
@@ -866,6 +889,22 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full_bar[s0]);
       if (two) mbar_arrive(&full_bar[s1]);
+    }
+    if (kForward) {
+      // The structural zeros l < m of this tile's rows, while the MMAs of
+      // the last K blocks run.  The rows are dealt out over the N ranges
+      // that have columns (the others have returned), warps 2-7 take
+      // alternate rows and lanes consecutive l.
+      const int nact = min((int)gridDim.z, (n_par[0] + a.Nsub - 1) / a.Nsub);
+      const int pw = pt >> 5;
+      for (int r = (int)blockIdx.z + nact * pw; r < 128; r += nact * (kTcProducers / 32)) {
+        const int rr = tile * 128 + r;
+        if (rr >= rows) break;
+        int b, row;
+        tc_row_map(m, rr, b, row);
+        float* o = a.out + ((size_t)b * a.M + row) * a.L;
+        for (int l = lane; l < m; l += 32) o[l] = 0.f;
+      }
     }
   }
   __syncwarp();
@@ -989,15 +1028,6 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       if (lane == 0 && nb > 0) bulk_wait_read<0>();
       __syncwarp();
     } else {
-      // Structural zeros l < m (first N range only), alternate rows.
-      for (int r = half; r < 32 && lo == 0; r += 2) {
-        const int rr = row0 + r;
-        if (rr >= rows) break;
-        int b, row;
-        tc_row_map(m, rr, b, row);
-        float* o = a.out + ((size_t)b * a.M + row) * a.L;
-        for (int l = lane; l < m; l += 32) o[l] = 0.f;
-      }
       const int nchunks = (max(cnt[0], cnt[1]) + 15) / 16;
       for (int c = half; c < nchunks; c += 2) {
         float e[16], od[16];
@@ -1043,12 +1073,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Table [rows][inner] of bf16 (tf32 = 0) or tf32-in-FP32 (tf32 = 1) entries;
-// the box is one 128-byte K block of box_rows rows, swizzled for the MMA.
+// the box is one K block (kRowBytes) of box_rows rows, swizzled for the MMA.
 static int make_map(CUtensorMap* tm, const void* ptr, int tf32, int inner, long long rows,
                     int box_rows) {
   auto fn = encode_fn();
   const int esz = tf32 ? 4 : 2;
-  const int kb = 128 / esz;
+  const int rb = tc_row_bytes(tf32);
+  const int kb = rb / esz;
   DINO_REQUIRE(fn != nullptr, DINO_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
   DINO_REQUIRE(((uintptr_t)ptr & 15) == 0, DINO_ERR_ARG, "TMA base must be 16-byte aligned");
   DINO_REQUIRE(inner % kb == 0 && box_rows >= 8 && box_rows <= 256, DINO_ERR_ARG,
@@ -1059,7 +1090,8 @@ static int make_map(CUtensorMap* tm, const void* ptr, int tf32, int inner, long 
   cuuint32_t elem[2] = {1u, 1u};
   CUresult r = fn(tm, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16,
                   2, (void*)ptr, dims, strides, box,
-                  elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  rb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -1110,16 +1142,25 @@ struct TcShape {
   size_t smem;
 };
 
-static void tc_candidates(int nfull, int accs, std::vector<TcShape>* out) {
-  int last_nsub = -1;
-  for (int nsplit : {1, 2, 4}) {
-    const int nsub = round_up((nfull + nsplit - 1) / nsplit, 16);
-    if (nsub == last_nsub || (nsplit > 1 && nsub * (nsplit - 1) >= nfull)) continue;
-    last_nsub = nsub;
-    if (tmem_cols_for(accs * nsub) > 512) continue;
-    const size_t stage = 2 * 128 * 128 + 2 * (size_t)nsub * 128;
+// N range widths: the full range split in 1, 2 or 4, and 128 and 64
+// columns (an accumulator pair of 128 columns is the widest that lets two
+// CTAs share TMEM); depths from 2 stages while the shared memory fits.  The
+// epilogue stages its output in the drained pipeline buffers, 8 KB per warp.
+static void tc_candidates(int nfull, int accs, int row_bytes, std::vector<TcShape>* out) {
+  std::vector<int> widths;
+  for (int nsplit : {1, 2, 4}) widths.push_back(round_up((nfull + nsplit - 1) / nsplit, 16));
+  for (int w : {128, 64})
+    if (w < nfull) widths.push_back(w);
+  std::vector<int> seen;
+  for (int nsub : widths) {
+    bool dup = false;
+    for (int w : seen) dup |= (w == nsub);
+    if (dup || tmem_cols_for(accs * nsub) > 512) continue;
+    seen.push_back(nsub);
+    const int nsplit = (nfull + nsub - 1) / nsub;
+    const size_t stage = 2 * 128 * (size_t)row_bytes + 2 * (size_t)nsub * row_bytes;
     for (int stages = 2; stages <= kMaxStages; ++stages) {
-      const size_t smem = stage * stages + 1024;
+      const size_t smem = std::max(stage * stages, (size_t)kTcThreads / 32 * 8192) + 1024;
       if (smem > kTcSmemLimit) break;
       out->push_back({nsplit, nsub, stages, smem});
     }
@@ -1193,7 +1234,7 @@ static int tc_time_shape(dino_plan* p, TcTables* t, const TcShape& c, int m0, in
     tc_out_maps(p, &a, out, nf, &o2, &o1);
   }
   dim3 grid(ceil_div(2 * nf, 128), m1 - m0, c.nsplit);
-  constexpr int kReps = 3;
+  constexpr int kReps = 10;
   for (int r = 0; r <= kReps; ++r) {
     if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
     tc_launch<kForward>(t, grid, c.smem, 0, bh, bl, o2, o1, a);
@@ -1240,7 +1281,7 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
       // latitudes (inverse).
       const int nfull = forward ? round_up((p->L - sh.m0 + 1) / 2, 16) : t->Np;
       std::vector<TcShape> cands;
-      tc_candidates(nfull, tc_accumulators(t->tf32), &cands);
+      tc_candidates(nfull, tc_accumulators(t->tf32), tc_row_bytes(t->tf32), &cands);
       float best = 1e30f;
       TcShape pick = cands.front();
       for (const TcShape& c : cands) {
@@ -1299,10 +1340,10 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
     (forward ? t->us_fwd : t->us_inv) = best;
     return DINO_OK;
   };
-  // The FP32 SIMT contraction on the same sizes (3 timed launches after one
+  // The FP32 SIMT contraction on the same sizes (10 timed launches after one
   // warm-up, like the tensor-core shapes).
   auto time_simt = [&](bool forward, float* us) -> int {
-    constexpr int kReps = 3;
+    constexpr int kReps = 10;
     for (int r = 0; r <= kReps; ++r) {
       if (r == 1) DINO_CHECK_CUDA(cudaEventRecord(e0, 0));
       if (forward)
