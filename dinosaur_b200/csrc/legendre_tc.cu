@@ -1282,6 +1282,19 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
       const int nfull = forward ? round_up((p->L - sh.m0 + 1) / 2, 16) : t->Np;
       std::vector<TcShape> cands;
       tc_candidates(nfull, tc_accumulators(t->tf32), tc_row_bytes(t->tf32), &cands);
+      // DINO_B200_TC_SHAPE="inv:NSUBxSTAGES,fwd:NSUBxSTAGES" keeps only the
+      // named candidates (a profiler's serialised launches make its own
+      // timings pick unrepresentative shapes).
+      if (const char* want = std::getenv("DINO_B200_TC_SHAPE")) {
+        const char* key = std::strstr(want, forward ? "fwd:" : "inv:");
+        int wn = 0, ws = 0;
+        if (key && std::sscanf(key + 4, "%dx%d", &wn, &ws) == 2) {
+          std::vector<TcShape> keep;
+          for (const TcShape& c : cands)
+            if (c.Nsub == wn && c.stages == ws) keep.push_back(c);
+          if (!keep.empty()) cands.swap(keep);
+        }
+      }
       float best = 1e30f;
       TcShape pick = cands.front();
       for (const TcShape& c : cands) {
@@ -1322,9 +1335,10 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
     DINO_TRY(tune_groups(forward, 1, dst, &one));
     int ngroups = 1;
     float best = one;
-    // DINO_B200_TC_M_GROUPS=1 or 2 forces the arrangement (tests of both).
+    // DINO_B200_TC_M_GROUPS=1 or 2 forces the arrangement (tests of both);
+    // a forced shape (DINO_B200_TC_SHAPE) is one launch.
     const char* force = std::getenv("DINO_B200_TC_M_GROUPS");
-    const int forced = force ? std::atoi(force) : 0;
+    const int forced = force ? std::atoi(force) : (std::getenv("DINO_B200_TC_SHAPE") ? 1 : 0);
     if (p->lw >= 32 && forced != 1) {
       TcTables::Shape two[TcTables::kMaxGroups];
       float t2 = 0.f;
@@ -1365,7 +1379,7 @@ static int tc_autotune(dino_plan* p, TcTables* t) {
   // DINO_B200_TENSOR_CORES_ONLY=1 keeps the tensor-core form whatever the
   // timings (the tests of the tensor-core kernels on small grids use it).
   const char* only = std::getenv("DINO_B200_TENSOR_CORES_ONLY");
-  const bool tc_only = only && only[0] == '1';
+  const bool tc_only = (only && only[0] == '1') || std::getenv("DINO_B200_TC_SHAPE");
   t->simt_inv = !tc_only && t->us_simt_inv < t->us_inv ? 1 : 0;
   t->simt_fwd = !tc_only && t->us_simt_fwd < t->us_fwd ? 1 : 0;
   cudaEventDestroy(e0);
