@@ -384,6 +384,7 @@ int legendre_forward_fp32(dino_plan* p, const float* G, float* out, int nf,
 
 constexpr int kFftJS = 16;       // latitudes (columns) per CTA
 constexpr int kFftThreads = 256;
+static_assert(kFftThreads % kFftJS == 0, "a thread keeps one FFT column in every pass");
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -712,11 +713,14 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
   __syncthreads();
   float* ob = out + (size_t)b * (2 * N) * J + j0;
   auto first = [S](int n, int c) { return S[n * kFftJS + c]; };
-  auto last = [ob, ncol, J, wq, j0](int n, int c, float2 v) {
+  // A thread's column is the same in every pass (c = tid mod kFftJS), so its
+  // weight is read once; offsets within a field fit 32 bits.
+  const int cth = tid % kFftJS;
+  const float sc = (wq && cth < ncol) ? wq[j0 + cth] : 1.f;
+  auto last = [ob, ncol, J, sc](int n, int c, float2 v) {
     if (c < ncol) {
-      const float s = wq ? wq[j0 + c] : 1.f;
-      ob[(size_t)(2 * n) * J + c] = v.x * s;
-      ob[(size_t)(2 * n + 1) * J + c] = v.y * s;
+      ob[2 * n * J + c] = v.x * sc;
+      ob[(2 * n + 1) * J + c] = v.y * sc;
     }
   };
   fft_passes<N, 1, true>(S, twn, first, last);
@@ -748,7 +752,7 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
   // a thread's loads in flight together.
   auto first = [xb, ncol, J](int n, int c) {
     if (c >= ncol) return make_float2(0.f, 0.f);
-    return make_float2(xb[(size_t)(2 * n) * J + c], xb[(size_t)(2 * n + 1) * J + c]);
+    return make_float2(xb[2 * n * J + c], xb[(2 * n + 1) * J + c]);
   };
   auto last = [S](int n, int c, float2 v) { S[n * kFftJS + c] = v; };
   fft_passes<N, -1, false>(S, twn, first, last);
@@ -756,21 +760,40 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
   float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
   const float inv_sqrt_pi = 0.5641895835477563f;
-  for (int idx = tid; idx < lw * kFftJS; idx += kFftThreads) {
-    int k = idx / kFftJS, c = idx % kFftJS;
-    if (c >= ncol) continue;
-    float2 zk = S[(k % N) * kFftJS + c];
-    float2 zc = cconj(S[((N - k) % N) * kFftJS + c]);
-    float2 s = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
-    float2 d = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
-    // X[k] = s + e^{-2 pi i k / I} * (-i d)
-    float2 xk = cadd(s, cmul(cconj(twi[k]), cmul_i<-1>(d)));
-    float w = wq ? wq[j0 + c] : 1.f;
-    if (k == 0) {
-      Fb[c] = xk.x * w * inv_sqrt_2pi;
-    } else {
-      Fb[(size_t)(2 * k - 1) * J + c] = xk.x * w * inv_sqrt_pi;
-      Fb[(size_t)(2 * k) * J + c] = -xk.y * w * inv_sqrt_pi;
+  // X[k] and X[N - k] from the same two values of Z: with
+  // s = (Z[k] + conj Z[N-k]) / 2 and d = (Z[k] - conj Z[N-k]) / 2,
+  // X[k] = s + e^{-2 pi i k / I} (-i d), and X[N-k] likewise with Z[k] and
+  // Z[N-k] exchanged.  A thread keeps one column (c = tid mod kFftJS) and
+  // takes k = tid / kFftJS + kFftJS q for k <= N / 2.
+  const int c = tid % kFftJS;
+  if (c < ncol) {
+    const float w = wq ? wq[j0 + c] : 1.f;
+    const float a0 = w * inv_sqrt_2pi, a1 = w * inv_sqrt_pi;
+    float* Fc = Fb + c;
+    for (int k = tid / kFftJS; k <= N / 2; k += kFftThreads / kFftJS) {
+      const int kn = (N - k) & (N - 1);  // N - k; 0 for k = 0
+      const float2 zk = S[k * kFftJS + c];
+      const float2 zn = S[kn * kFftJS + c];
+      if (k < lw) {
+        const float2 zc = cconj(zn);
+        const float2 s2 = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+        const float2 d2 = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));
+        const float2 xk = cadd(s2, cmul(cconj(twi[k]), cmul_i<-1>(d2)));
+        if (k == 0) {
+          Fc[0] = xk.x * a0;
+        } else {
+          Fc[(2 * k - 1) * J] = xk.x * a1;
+          Fc[2 * k * J] = -xk.y * a1;
+        }
+      }
+      if (k > 0 && k < N / 2 && kn < lw) {
+        const float2 zc = cconj(zk);
+        const float2 s2 = make_float2(0.5f * (zn.x + zc.x), 0.5f * (zn.y + zc.y));
+        const float2 d2 = make_float2(0.5f * (zn.x - zc.x), 0.5f * (zn.y - zc.y));
+        const float2 xn = cadd(s2, cmul(cconj(twi[kn]), cmul_i<-1>(d2)));
+        Fc[(2 * kn - 1) * J] = xn.x * a1;
+        Fc[2 * kn * J] = -xn.y * a1;
+      }
     }
   }
 }
