@@ -733,6 +733,37 @@ __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int t
   }
 }
 
+// L2 prefetches of the rows of K block 0 that the producers read first,
+// issued before the CTA's set-up barrier (barrier init, TMEM allocation), so
+// that the set-up overlaps their latency.  Every address lies inside its row.
+__device__ __forceinline__ void prefetch_l2(const float* p) {
+  asm volatile("prefetch.L2 [%0];" ::"l"(p));
+}
+
+template <bool kForward, class Op>
+__device__ __forceinline__ void tc_prefetch_first(const TcArgs& a, int m, int tile, int rows,
+                                                  int pt) {
+  constexpr int kPts = kForward ? 4 : 3;  // addresses per row
+  for (int q = pt; q < 128 * kPts; q += kTcProducers) {
+    const int r = q / kPts, e = q - r * kPts;
+    const int rr = tile * 128 + r;
+    if (rr >= rows) continue;
+    int b, row;
+    tc_row_map(m, rr, b, row);
+    if (kForward) {
+      const float* gr = a.G + ((size_t)b * a.M + row) * a.J;
+      const int w = min(Op::kKB, a.Jh);
+      const int j = e == 0 ? 0 : e == 1 ? w - 1 : e == 2 ? a.J - w : a.J - 1;
+      prefetch_l2(gr + j);
+    } else {
+      const float* src = seg_field(a.in, b, (size_t)a.M * a.L) + (size_t)row * a.L + m;
+      const int last = min(2 * Op::kKB, a.L - m) - 1;
+      const int off = e == 0 ? 0 : e == 1 ? min(32, last) : last;
+      prefetch_l2(src + off);
+    }
+  }
+}
+
 template <bool kForward, class Op>
 __device__ __forceinline__ void tc_produce(const TcArgs& a, int m, int tile, int rows, int k,
                                            uint8_t* t0, uint8_t* t1, int pt) {
@@ -811,6 +842,19 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
     mbar_init(&done_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    // The first stages' table tiles, before the set-up barrier (this thread
+    // initialised the barriers; every stage is free).
+    for (int i = 0; i < min(a.stages, nblocks); ++i) {
+      int k, p;
+      tc_seq(i, kblk[1], k, p);
+      uint8_t* st = base + (size_t)i * stage_bytes;
+      mbar_expect_tx(&full_bar[i], 2 * tile_b);
+      const int yb = (m * 2 + p) * a.Nrows + lo;
+      tma_load_2d(st + 2 * tile_a, &tBh, &full_bar[i], k * Op::kKB, yb);
+      tma_load_2d(st + 2 * tile_a + tile_b, &tBl, &full_bar[i], k * Op::kKB, yb);
+    }
+  } else if (warp >= 2) {
+    tc_prefetch_first<kForward, Op>(a, m, tile, rows, threadIdx.x - 64);
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -828,8 +872,8 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
   const int acc_cols = a.Nsub;
 
   if (threadIdx.x == 0) {
-    // B producer (TMA).
-    for (int i = 0; i < nblocks; ++i) {
+    // B producer (TMA); the first min(stages, nblocks) were issued above.
+    for (int i = min(a.stages, nblocks); i < nblocks; ++i) {
       const int s = i % a.stages;
       const int use = i / a.stages;
       if (use > 0 && !mbar_wait(&empty_bar[s], (use - 1) & 1, a.err, 1)) break;
