@@ -592,50 +592,54 @@ constexpr size_t fft_smem_bytes() {
 // Runs all passes on the one shared buffer S: the first pass reads via
 // `first` (in place when kFirstInS), the last writes via `last`; the passes
 // between run in place.
-template <int N, int kSign, bool kFirstInS, class First, class Last>
+// kLastInS: the last pass writes back into S (in place, so its loads finish
+// before its stores).
+template <int N, int kSign, bool kFirstInS, bool kLastInS = false, class First, class Last>
 __device__ __forceinline__ void fft_passes(float2* S, const float2* twn, First first,
                                            Last last) {
   using Rd = FftRadix<N>;
   auto s_load = [S](int n, int c) { return S[n * kFftJS + c]; };
   auto s_store = [S](int n, int c, float2 v) { S[n * kFftJS + c] = v; };
   if constexpr (Rd::r2 == 1) {
-    stockham_pass<N, Rd::r1, kSign, kFirstInS>(1, twn, first, last);
+    stockham_pass<N, Rd::r1, kSign, kFirstInS || kLastInS>(1, twn, first, last);
   } else if constexpr (Rd::r3 == 1) {
     stockham_pass<N, Rd::r1, kSign, kFirstInS>(1, twn, first, s_store);
     __syncthreads();
-    stockham_pass<N, Rd::r2, kSign, false>(Rd::r1, twn, s_load, last);
+    stockham_pass<N, Rd::r2, kSign, kLastInS>(Rd::r1, twn, s_load, last);
   } else {
     stockham_pass<N, Rd::r1, kSign, kFirstInS>(1, twn, first, s_store);
     __syncthreads();
     stockham_pass<N, Rd::r2, kSign, true>(Rd::r1, twn, s_load, s_store);
     __syncthreads();
-    stockham_pass<N, Rd::r3, kSign, false>(Rd::r1 * Rd::r2, twn, s_load, last);
+    stockham_pass<N, Rd::r3, kSign, kLastInS>(Rd::r1 * Rd::r2, twn, s_load, last);
   }
 }
 
 // Copies a rows x kFftJS tile (row stride J floats) into shared memory
-// (row stride kFftJS) with every thread's loads issued before its stores:
-// float4 loads when rows start 16-byte aligned and the tile is full, else
-// scalar loads with zero fill past ncol.
+// (row stride kFftJS): 16-byte asynchronous copies when rows start 16-byte
+// aligned and the tile is full, else scalar loads with zero fill past ncol.
 template <int kMaxRows>
 __device__ __forceinline__ void stage_tile(const float* __restrict__ src, int rows,
                                            int J, int ncol, float* dst) {
-  if ((J & 3) == 0 && ncol == kFftJS) {
+  if ((J & 3) == 0 && ncol == kFftJS && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
     constexpr int kQ = kFftJS / 4;  // float4 per row
+    // 16-byte asynchronous copies (cp.async): every copy of the thread is in
+    // flight at once and none holds a register; the caller's barrier follows
+    // the wait below.
     constexpr int kChunks = (kMaxRows * kQ + kFftThreads - 1) / kFftThreads;
-    float4 v[kChunks];
 #pragma unroll
     for (int i = 0; i < kChunks; ++i) {
       const int t = threadIdx.x + i * kFftThreads;
       const int r = t / kQ, q = t % kQ;
-      v[i] = (r < rows) ? *reinterpret_cast<const float4*>(src + (size_t)r * J + 4 * q)
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (r < rows) {
+        const float* g = src + (size_t)r * J + 4 * q;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(reinterpret_cast<float4*>(dst) + t)),
+                     "l"(g)
+                     : "memory");
+      }
     }
-#pragma unroll
-    for (int i = 0; i < kChunks; ++i) {
-      const int t = threadIdx.x + i * kFftThreads;
-      if (t / kQ < rows) reinterpret_cast<float4*>(dst)[t] = v[i];
-    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
   } else {
     for (int t = threadIdx.x; t < rows * kFftJS; t += kFftThreads) {
       const int r = t / kFftJS, c = t % kFftJS;
@@ -651,7 +655,7 @@ __device__ __forceinline__ void stage_tile(const float* __restrict__ src, int ro
 // (at most 2N - 1 rows of kFftJS floats) is staged in the shared buffer, Z is
 // formed in registers and written back over it, and the passes run in place.
 template <int N>
-__global__ void __launch_bounds__(kFftThreads)
+__global__ void __launch_bounds__(kFftThreads, N <= 256 ? 5 : 3)
 rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
                     int M, int lw, int J, const float2* __restrict__ tw_n,
                     const float2* __restrict__ tw_i,
@@ -682,48 +686,91 @@ rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
                        -src[(2 * k) * kFftJS + c] * half_inv_sqrt_pi);
   };
   // Pairs (k, N - k), k = 0..N/2; k = 0 pairs with the (zero) Nyquist term.
-  constexpr int kTotal = (N / 2 + 1) * kFftJS;
-  constexpr int kItems = (kTotal + kFftThreads - 1) / kFftThreads;
-  float2 xk[kItems], xn[kItems];
-#pragma unroll
-  for (int it = 0; it < kItems; ++it) {
-    const int item = tid + it * kFftThreads;
-    if (item < kTotal) {
-      const int k = item / kFftJS, c = item % kFftJS;
-      xk[it] = X(k, c);
-      xn[it] = (k == 0) ? make_float2(0.f, 0.f) : X(N - k, c);
+  // A thread keeps one column (c = tid mod kFftJS) and takes
+  // k = tid / kFftJS + kRowsPerPass * it.  Z[k] overwrites the staged rows
+  // 2k and 2k + 1 and Z[N - k] the rows 2(N - k) and 2(N - k) + 1, so the
+  // items run in two halves (k < kSplit, then the rest), each loading all of
+  // its X before any of its Z is written: the first half's Z rows are ones
+  // that the second half no longer reads, except row 2 kSplit - 1 of
+  // Z[kSplit - 1], which is written after the second half's loads.  Half
+  // the X values are live at a time.
+  constexpr int kRowsPerPass = kFftThreads / kFftJS;
+  constexpr int kItems = (N / 2 + 1 + kRowsPerPass - 1) / kRowsPerPass;
+  constexpr int kItA = kItems / 2;
+  constexpr int kSplit = kItA * kRowsPerPass;
+  const int cz = tid % kFftJS, k0 = tid / kFftJS;
+  auto z_pair = [&](int k, float2 xk, float2 xn, bool write_k) {
+    const float2 xnc = cconj(xn), xkc = cconj(xk);
+    const float2 zk = cadd(cadd(xk, xnc), cmul_i<1>(cmul(twi[k], csub(xk, xnc))));
+    if (write_k) S[k * kFftJS + cz] = zk;
+    if (k > 0 && k < N / 2 + (N & 1)) {
+      const int kn = N - k;
+      S[kn * kFftJS + cz] =
+          cadd(cadd(xn, xkc), cmul_i<1>(cmul(twi[kn], csub(xn, xkc))));
     }
-  }
-  __syncthreads();
+    return zk;
+  };
+  float2 held = make_float2(0.f, 0.f);  // Z[kSplit - 1], written last
+  bool hold = false;
+  if constexpr (kItA > 0) {
+    float2 xk[kItA], xn[kItA];
 #pragma unroll
-  for (int it = 0; it < kItems; ++it) {
-    const int item = tid + it * kFftThreads;
-    if (item < kTotal) {
-      const int k = item / kFftJS, c = item % kFftJS;
-      const float2 xnc = cconj(xn[it]), xkc = cconj(xk[it]);
-      S[k * kFftJS + c] =
-          cadd(cadd(xk[it], xnc), cmul_i<1>(cmul(twi[k], csub(xk[it], xnc))));
-      if (k > 0 && k < N / 2 + (N & 1)) {
-        const int kn = N - k;
-        S[kn * kFftJS + c] =
-            cadd(cadd(xn[it], xkc), cmul_i<1>(cmul(twi[kn], csub(xn[it], xkc))));
+    for (int it = 0; it < kItA; ++it) {
+      const int k = k0 + it * kRowsPerPass;
+      xk[it] = X(k, cz);
+      xn[it] = (k == 0) ? make_float2(0.f, 0.f) : X(N - k, cz);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kItA; ++it) {
+      const int k = k0 + it * kRowsPerPass;
+      const bool last_row = (k == kSplit - 1);
+      const float2 zk = z_pair(k, xk[it], xn[it], !last_row);
+      if (last_row) {
+        held = zk;
+        hold = true;
       }
     }
+  }
+  {
+    constexpr int kItB = kItems - kItA;
+    float2 xk[kItB], xn[kItB];
+#pragma unroll
+    for (int it = 0; it < kItB; ++it) {
+      const int k = kSplit + k0 + it * kRowsPerPass;
+      if (k <= N / 2) {
+        xk[it] = X(k, cz);
+        xn[it] = (k == 0) ? make_float2(0.f, 0.f) : X(N - k, cz);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kItB; ++it) {
+      const int k = kSplit + k0 + it * kRowsPerPass;
+      if (k <= N / 2) z_pair(k, xk[it], xn[it], true);
+    }
+    if (hold) S[(kSplit - 1) * kFftJS + cz] = held;
   }
   __syncthreads();
   float* ob = out + (size_t)b * (2 * N) * J + j0;
   auto first = [S](int n, int c) { return S[n * kFftJS + c]; };
-  // A thread's column is the same in every pass (c = tid mod kFftJS), so its
-  // weight is read once; offsets within a field fit 32 bits.
+  // The last pass writes z back into S; then each thread copies its column
+  // (c = tid mod kFftJS, the same in every pass) out as rows 2n (Re z[n])
+  // and 2n + 1 (Im z[n]) with its weight read once.  Keeping the global
+  // stores out of the pass keeps its register count down.
+  auto last = [S](int n, int c, float2 v) { S[n * kFftJS + c] = v; };
+  fft_passes<N, 1, true, true>(S, twn, first, last);
+  __syncthreads();
   const int cth = tid % kFftJS;
-  const float sc = (wq && cth < ncol) ? wq[j0 + cth] : 1.f;
-  auto last = [ob, ncol, J, sc](int n, int c, float2 v) {
-    if (c < ncol) {
-      ob[2 * n * J + c] = v.x * sc;
-      ob[(2 * n + 1) * J + c] = v.y * sc;
+  if (cth < ncol) {
+    const float sc = wq ? wq[j0 + cth] : 1.f;
+    float* oc = ob + cth;
+    for (int n = tid / kFftJS; n < N; n += kFftThreads / kFftJS) {
+      const float2 v = S[n * kFftJS + cth];
+      oc[2 * n * J] = v.x * sc;
+      oc[(2 * n + 1) * J] = v.y * sc;
     }
-  };
-  fft_passes<N, 1, true>(S, twn, first, last);
+  }
 }
 
 // nodal[b][i][j] -> F[b][row][j] (times wq[j] when given: the forward SHT's
