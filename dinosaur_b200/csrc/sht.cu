@@ -793,16 +793,17 @@ rfft_forward_kernel(const float* __restrict__ x, float* __restrict__ F, int M,
     twn[t] = tw_n[t];
     twi[t] = tw_i[t];
   }
-  __syncthreads();
   const float* xb = x + (size_t)b * (2 * N) * J + j0;
-  // The first pass reads the nodal tile straight from global memory, all of
-  // a thread's loads in flight together.
-  auto first = [xb, ncol, J](int n, int c) {
-    if (c >= ncol) return make_float2(0.f, 0.f);
-    return make_float2(xb[2 * n * J + c], xb[(2 * n + 1) * J + c]);
+  // The nodal tile (2N rows of kFftJS floats) is staged by asynchronous
+  // copies; the first pass reads it in place.
+  stage_tile<2 * N>(xb, 2 * N, J, ncol, reinterpret_cast<float*>(S));
+  __syncthreads();
+  const float* Sf = reinterpret_cast<const float*>(S);
+  auto first = [Sf](int n, int c) {
+    return make_float2(Sf[2 * n * kFftJS + c], Sf[(2 * n + 1) * kFftJS + c]);
   };
   auto last = [S](int n, int c, float2 v) { S[n * kFftJS + c] = v; };
-  fft_passes<N, -1, false>(S, twn, first, last);
+  fft_passes<N, -1, true>(S, twn, first, last);
   __syncthreads();
   float* Fb = F + (size_t)b * M * J + j0;
   const float inv_sqrt_2pi = 0.3989422804014327f;
