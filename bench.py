@@ -42,12 +42,12 @@ FORMS = ('fp32', 'bf16x3', 'tf32x3')
 # (profiles/sht_phase_tl255_b128_dram_traffic.md).
 PHASE_TRAFFIC = {
     ('bf16x3', 'legendre_inverse'): 75117568 + 15423744,
-    ('bf16x3', 'fourier_inverse'): 67014912 + 23471360,
-    ('bf16x3', 'fourier_forward'): 67135744 + 25449472,
+    ('bf16x3', 'fourier_inverse'): 67005440 + 22596096,
+    ('bf16x3', 'fourier_forward'): 67136000 + 24715264,
     ('bf16x3', 'legendre_forward'): 102526208 + 20786176,
     ('fp32', 'legendre_inverse'): 58467584 + 19169536,
-    ('fp32', 'fourier_inverse'): 67018752 + 23803136,
-    ('fp32', 'fourier_forward'): 67136000 + 25746688,
+    ('fp32', 'fourier_inverse'): 67005440 + 22596096,
+    ('fp32', 'fourier_forward'): 67136000 + 24715264,
     ('fp32', 'legendre_forward'): 84916224 + 27469824,
     ('tf32x3', 'legendre_inverse'): 118548480 + 34110976,
     ('tf32x3', 'legendre_forward'): 151210240 + 43932416,
