@@ -733,16 +733,18 @@ __device__ __forceinline__ void tc_produce_forward(const TcArgs& a, int m, int t
   }
 }
 
-// L2 prefetches of the rows of K block 0 that the producers read first,
-// issued before the CTA's set-up barrier (barrier init, TMEM allocation), so
-// that the set-up overlaps their latency.  Every address lies inside its row.
+// L2 prefetches of the rows of K block k: block 0's before the CTA's set-up
+// barrier (barrier init, TMEM allocation), so that the set-up overlaps their
+// latency, and block k + 1's as the producers start block k, so that its
+// memory latency overlaps block k's conversion and stage waits.  Every
+// address lies inside its row.
 __device__ __forceinline__ void prefetch_l2(const float* p) {
   asm volatile("prefetch.L2 [%0];" ::"l"(p));
 }
 
 template <bool kForward, class Op>
-__device__ __forceinline__ void tc_prefetch_first(const TcArgs& a, int m, int tile, int rows,
-                                                  int pt) {
+__device__ __forceinline__ void tc_prefetch_block(const TcArgs& a, int m, int tile, int rows,
+                                                  int k, int pt) {
   constexpr int kPts = kForward ? 4 : 3;  // addresses per row
   for (int q = pt; q < 128 * kPts; q += kTcProducers) {
     const int r = q / kPts, e = q - r * kPts;
@@ -752,12 +754,14 @@ __device__ __forceinline__ void tc_prefetch_first(const TcArgs& a, int m, int ti
     tc_row_map(m, rr, b, row);
     if (kForward) {
       const float* gr = a.G + ((size_t)b * a.M + row) * a.J;
-      const int w = min(Op::kKB, a.Jh);
-      const int j = e == 0 ? 0 : e == 1 ? w - 1 : e == 2 ? a.J - w : a.J - 1;
+      const int j0 = Op::kKB * k;
+      const int w = min(Op::kKB, a.Jh - j0);  // >= 1 for k < kblk
+      const int j = e == 0 ? j0 : e == 1 ? j0 + w - 1 : e == 2 ? a.J - j0 - w : a.J - 1 - j0;
       prefetch_l2(gr + j);
     } else {
-      const float* src = seg_field(a.in, b, (size_t)a.M * a.L) + (size_t)row * a.L + m;
-      const int last = min(2 * Op::kKB, a.L - m) - 1;
+      const int l0 = 2 * Op::kKB * k;  // relative to l = m
+      const float* src = seg_field(a.in, b, (size_t)a.M * a.L) + (size_t)row * a.L + m + l0;
+      const int last = min(2 * Op::kKB, a.L - m - l0) - 1;  // >= 0 for k < kblk
       const int off = e == 0 ? 0 : e == 1 ? min(32, last) : last;
       prefetch_l2(src + off);
     }
@@ -854,7 +858,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       tma_load_2d(st + 2 * tile_a + tile_b, &tBl, &full_bar[i], k * Op::kKB, yb);
     }
   } else if (warp >= 2) {
-    tc_prefetch_first<kForward, Op>(a, m, tile, rows, threadIdx.x - 64);
+    tc_prefetch_block<kForward, Op>(a, m, tile, rows, 0, threadIdx.x - 64);
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -928,6 +932,7 @@ legendre_tc_kernel(const __grid_constant__ CUtensorMap tBh,
       if (two && u1 > 0 && !mbar_wait(&empty_bar[s1], (u1 - 1) & 1, a.err, 4)) break;
       uint8_t* t0 = base + (size_t)s0 * stage_bytes;
       uint8_t* t1 = two ? base + (size_t)s1 * stage_bytes : nullptr;
+      if (k + 1 < kblk[0]) tc_prefetch_block<kForward, Op>(a, m, tile, rows, k + 1, pt);
       tc_produce<kForward, Op>(a, m, tile, rows, k, t0, t1, pt);
       // Make the generic-proxy stores visible to the tensor cores.
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
