@@ -38,8 +38,8 @@ FORMS = ('fp32', 'bf16x3', 'tf32x3')
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# each transform phase over the 128 TL255 fields, from one ncu capture
-# (profiles/sht_phase_tl255_b128_dram_traffic.md).
+# each transform phase over the 128 TL255 fields, from one ncu capture of
+# `bench.py --profile-phase <phase>` per phase.
 PHASE_TRAFFIC = {
     ('bf16x3', 'legendre_inverse'): 75117568 + 15423744,
     ('bf16x3', 'fourier_inverse'): 67005440 + 22596096,
