@@ -41,10 +41,10 @@ FORMS = ('fp32', 'bf16x3', 'tf32x3')
 # each transform phase over the 128 TL255 fields, from one ncu capture of
 # `bench.py --profile-phase <phase>` per phase.
 PHASE_TRAFFIC = {
-    ('bf16x3', 'legendre_inverse'): 75117568 + 15423744,
+    ('bf16x3', 'legendre_inverse'): 75098880 + 17449728,
     ('bf16x3', 'fourier_inverse'): 67005440 + 22596096,
     ('bf16x3', 'fourier_forward'): 67136000 + 24715264,
-    ('bf16x3', 'legendre_forward'): 102526208 + 20786176,
+    ('bf16x3', 'legendre_forward'): 103041024 + 21350656,
     ('fp32', 'legendre_inverse'): 58467584 + 19169536,
     ('fp32', 'fourier_inverse'): 67005440 + 22596096,
     ('fp32', 'fourier_forward'): 67136000 + 24715264,
