@@ -653,7 +653,10 @@ __device__ __forceinline__ void stage_tile(const float* __restrict__ src, int ro
 // Z[k] = (X[k] + conj X[N-k]) + i w_I^k (X[k] - conj X[N-k]), then
 // z = IDFT_N(Z) and x[2n] = Re z[n], x[2n+1] = Im z[n].  The coefficient tile
 // (at most 2N - 1 rows of kFftJS floats) is staged in the shared buffer, Z is
-// formed in registers and written back over it, and the passes run in place.
+// formed in registers in two halves and written back over it, the passes run
+// in place and a per-column copy writes the nodal rows.  Up to N = 256 the
+// kernel fits 48 registers, so five CTAs (36 KB of shared memory each) share
+// an SM.
 template <int N>
 __global__ void __launch_bounds__(kFftThreads, N <= 256 ? 5 : 3)
 rfft_inverse_kernel(const float* __restrict__ F, float* __restrict__ out,
